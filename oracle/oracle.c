@@ -1,0 +1,349 @@
+/* Test infrastructure only (the checker, never the product path).
+ *
+ * Plain-C restatement of the reference's CPU registration hot path.  The generic
+ * bodies live in oracle_core.h (pixel passes), oracle_field.h (displacement-field
+ * passes) and oracle_cdm.h (the CDM driver); this file holds the transform
+ * algebra and the two affine cost functions, then instantiates the generic
+ * bodies for uint8/float (reference-exact) and double (error reporting).
+ * Build: oracle/Makefile (gcc -O2 -ffp-contract=off).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include "oracle.h"
+
+/* rotation_matrix (numerical/transformation.hpp:143-164), scaling
+ * (transformation.hpp:196-208), affine shear (transformation.hpp:220-231) and the
+ * voxel-space composition of transformation_matrix(affine_param, ...)
+ * (transformation.hpp:636-675).  All in float, in the reference's order. */
+void orc_affine_to_matrix(const float* p, const int* fd, const float* fvs, const int* td, const float* tvs, float* T)
+{
+    const float* tr = p;
+    const float* th = p + 3;
+    const float* s = p + 6;
+    const float* a = p + 9;
+    float* m = T;
+    float sin_x = sinf(th[0]), cos_x = cosf(th[0]);
+    float sin_y = sinf(th[1]), cos_y = cosf(th[1]);
+    float sin_z = sinf(th[2]), cos_z = cosf(th[2]);
+    float cos_x_sin_z = cos_x * sin_z, cos_x_cos_z = cos_x * cos_z;
+    float sin_x_sin_z = sin_x * sin_z, sin_x_cos_z = sin_x * cos_z;
+    m[0] = cos_y * cos_z;
+    m[1] = cos_y * sin_z;
+    m[2] = -sin_y;
+    m[3] = -cos_x_sin_z + sin_x_cos_z * sin_y;
+    m[4] = cos_x_cos_z + sin_x_sin_z * sin_y;
+    m[5] = sin_x * cos_y;
+    m[6] = sin_x_sin_z + cos_x_cos_z * sin_y;
+    m[7] = -sin_x_cos_z + cos_x_sin_z * sin_y;
+    m[8] = cos_x * cos_y;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            m[3 * r + c] *= s[r];
+    m[0] += m[3] * a[0] + m[6] * a[1];
+    m[1] += m[4] * a[0] + m[7] * a[1];
+    m[2] += m[5] * a[0] + m[8] * a[1];
+    m[3] += m[6] * a[2];
+    m[4] += m[7] * a[2];
+    m[5] += m[8] * a[2];
+    float t[3] = {(float)fd[0], (float)fd[1], (float)fd[2]};
+    for (int i = 0; i < 3; ++i) {
+        t[i] *= -0.5f;
+    }
+    for (int i = 0; i < 3; ++i)
+        t[i] *= fvs[i];
+    for (int i = 0; i < 3; ++i)
+        t[i] += tr[i];
+    float* sh = T + 9;
+    sh[0] = m[0] * t[0] + m[1] * t[1] + m[2] * t[2];
+    sh[1] = m[3] * t[0] + m[4] * t[1] + m[5] * t[2];
+    sh[2] = m[6] * t[0] + m[7] * t[1] + m[8] * t[2];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            m[3 * r + c] *= fvs[c];
+    for (int r = 0; r < 3; ++r)
+        if (tvs[r] != 1.0f) {
+            m[3 * r] /= tvs[r];
+            m[3 * r + 1] /= tvs[r];
+            m[3 * r + 2] /= tvs[r];
+            sh[r] /= tvs[r];
+        }
+    for (int r = 0; r < 3; ++r)
+        sh[r] += (float)td[r] * 0.5f;
+}
+
+/* The same composition in double (the FP64 4x4 affine path). */
+void orc_affine_to_matrix_f64(const double* p, const int* fd, const double* fvs, const int* td, const double* tvs,
+                              double* T)
+{
+    const double* tr = p;
+    const double* th = p + 3;
+    const double* s = p + 6;
+    const double* a = p + 9;
+    double* m = T;
+    double sin_x = sin(th[0]), cos_x = cos(th[0]);
+    double sin_y = sin(th[1]), cos_y = cos(th[1]);
+    double sin_z = sin(th[2]), cos_z = cos(th[2]);
+    m[0] = cos_y * cos_z;
+    m[1] = cos_y * sin_z;
+    m[2] = -sin_y;
+    m[3] = -cos_x * sin_z + sin_x * cos_z * sin_y;
+    m[4] = cos_x * cos_z + sin_x * sin_z * sin_y;
+    m[5] = sin_x * cos_y;
+    m[6] = sin_x * sin_z + cos_x * cos_z * sin_y;
+    m[7] = -sin_x * cos_z + cos_x * sin_z * sin_y;
+    m[8] = cos_x * cos_y;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            m[3 * r + c] *= s[r];
+    m[0] += m[3] * a[0] + m[6] * a[1];
+    m[1] += m[4] * a[0] + m[7] * a[1];
+    m[2] += m[5] * a[0] + m[8] * a[1];
+    m[3] += m[6] * a[2];
+    m[4] += m[7] * a[2];
+    m[5] += m[8] * a[2];
+    double t[3];
+    for (int i = 0; i < 3; ++i)
+        t[i] = (double)fd[i] * -0.5 * fvs[i] + tr[i];
+    double* sh = T + 9;
+    for (int r = 0; r < 3; ++r)
+        sh[r] = m[3 * r] * t[0] + m[3 * r + 1] * t[1] + m[3 * r + 2] * t[2];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            m[3 * r + c] *= fvs[c];
+    for (int r = 0; r < 3; ++r) {
+        m[3 * r] /= tvs[r];
+        m[3 * r + 1] /= tvs[r];
+        m[3 * r + 2] /= tvs[r];
+        sh[r] /= tvs[r];
+        sh[r] += (double)td[r] * 0.5;
+    }
+}
+
+/* transformation_matrix::inverse (numerical/transformation.hpp:820-832) with the
+ * cofactor 3x3 inverse of numerical/matrix.hpp:1347-1352,1479-1505.  On a
+ * singular sr the matrix is left unchanged and 0 is returned. */
+int orc_matrix_inverse(float* T)
+{
+    const float* a = T;
+    float det = a[0] * (a[4] * a[8] - a[5] * a[7]) + a[1] * (a[5] * a[6] - a[3] * a[8]) +
+                a[2] * (a[3] * a[7] - a[4] * a[6]);
+    if (det + 1.0f == 1.0f)
+        return 0;
+    float t[9];
+    t[0] = a[4] * a[8] - a[5] * a[7];
+    t[1] = a[2] * a[7] - a[1] * a[8];
+    t[2] = a[1] * a[5] - a[2] * a[4];
+    t[3] = a[5] * a[6] - a[3] * a[8];
+    t[4] = a[0] * a[8] - a[2] * a[6];
+    t[5] = a[2] * a[3] - a[0] * a[5];
+    t[6] = a[3] * a[7] - a[4] * a[6];
+    t[7] = a[1] * a[6] - a[0] * a[7];
+    t[8] = a[0] * a[4] - a[1] * a[3];
+    for (int i = 0; i < 9; ++i)
+        t[i] = t[i] / det;
+    float s[3] = {T[9], T[10], T[11]};
+    float ns[3];
+    for (int r = 0; r < 3; ++r)
+        ns[r] = s[0] * t[3 * r] + s[1] * t[3 * r + 1] + s[2] * t[3 * r + 2];
+    for (int r = 0; r < 3; ++r)
+        T[9 + r] = -ns[r];
+    for (int i = 0; i < 9; ++i)
+        T[i] = t[i];
+    return 1;
+}
+
+/* The integer-shift test of the CPU resample fast path
+ * (numerical/resampling.hpp:1243-1258): every shift within 1e-4 of an integer
+ * and sr within 1e-4 of the identity. */
+int orc_is_integer_shift(const float* T, int* shift)
+{
+    const double eps = 1.0e-4;
+    for (int i = 0; i < 3; ++i) {
+        long s = lroundf(T[9 + i]);
+        if (fabsf(T[9 + i] - (float)s) > eps)
+            return 0;
+        shift[i] = (int)s;
+        for (int j = 0; j < 3; ++j)
+            if (fabsf(T[3 * i + j] - (float)(i == j)) > eps)
+                return 0;
+    }
+    return 1;
+}
+
+/* ---- generic instantiations ------------------------------------------------ */
+#define SFX _u8
+#define PIX uint8_t
+#define R float
+#define PIX_IS_U8 1
+#include "oracle_core.h"
+#undef SFX
+#undef PIX
+#undef R
+#undef PIX_IS_U8
+
+#define SFX _f32
+#define PIX float
+#define R float
+#define PIX_IS_U8 0
+#include "oracle_core.h"
+#undef SFX
+#undef PIX
+#undef R
+#undef PIX_IS_U8
+
+#define SFX _f64
+#define PIX double
+#define R double
+#define PIX_IS_U8 0
+#include "oracle_core.h"
+#undef SFX
+#undef PIX
+#undef R
+#undef PIX_IS_U8
+
+#define FSFX _f32
+#define R float
+#include "oracle_field.h"
+#undef FSFX
+#undef R
+
+#define FSFX _f64
+#define R double
+#include "oracle_field.h"
+#undef FSFX
+#undef R
+
+#define SFX _u8
+#define FSFX _f32
+#define PIX uint8_t
+#define R float
+#include "oracle_cdm.h"
+#undef SFX
+#undef FSFX
+#undef PIX
+#undef R
+
+#define SFX _f32
+#define FSFX _f32
+#define PIX float
+#define R float
+#include "oracle_cdm.h"
+#undef SFX
+#undef FSFX
+#undef PIX
+#undef R
+
+#define SFX _f64
+#define FSFX _f64
+#define PIX double
+#define R double
+#include "oracle_cdm.h"
+#undef SFX
+#undef FSFX
+#undef PIX
+#undef R
+
+/* ---- affine costs ---------------------------------------------------------- */
+
+/* histogram(img, hist, 0, 255, 256) (numerical/basic_op.hpp:1293-1311): bin =
+ * clamp(floor(v * (256/255)), 0, 255), which for uint8 is the value itself. */
+void orc_histogram_u8(const uint8_t* img, long long n, int32_t* hist)
+{
+    float range = 256.0f / 255.0f;
+    memset(hist, 0, 256 * sizeof(int32_t));
+    for (long long i = 0; i < n; ++i) {
+        float v = (float)img[i] * range;
+        int b = (int)floorf(v);
+        if (b < 0) b = 0;
+        if (b > 255) b = 255;
+        ++hist[b];
+    }
+}
+
+/* get_mutual_info CPU (reg/linear.hpp:138-146): for every template voxel x,
+ * H[(from[x] << 8) + to(T x)]++, where to(T x) is the uint8 trilinear sample of the
+ * moving volume (0 outside). */
+void orc_mi_hist_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T,
+                    int32_t* hist)
+{
+    memset(hist, 0, 65536 * sizeof(int32_t));
+    size_t i = 0;
+    for (int z = 0; z < fdim[2]; ++z)
+        for (int y = 0; y < fdim[1]; ++y)
+            for (int x = 0; x < fdim[0]; ++x, ++i) {
+                float p[3];
+                apply_T_u8(T, (float)x, (float)y, (float)z, p);
+                uint8_t v = 0;
+                trilinear_u8(to, tdim, p[0], p[1], p[2], &v);
+                ++hist[((uint32_t)from[i] << 8) + v];
+            }
+}
+
+/* get_mutual_info_mean CPU (reg/linear.hpp:87-104): column sums of H, then
+ * sum over non-zero bins of n*ln(n/row/col), divided by 65536; the functor
+ * returns its negative (linear.hpp:201). */
+double orc_mi_cost_from_hist(const int32_t* hist, const int32_t* from_hist)
+{
+    uint32_t to_hist[256];
+    memset(to_hist, 0, sizeof(to_hist));
+    for (int i = 0; i < 65536; ++i)
+        to_hist[i & 255] += (uint32_t)hist[i];
+    double sum = 0.0;
+    for (int i = 0; i < 65536; ++i) {
+        double mu = hist[i];
+        if (mu == 0.0f)
+            continue;
+        sum += mu * log(mu / (double)from_hist[i >> 8] / (double)to_hist[i & 255]);
+    }
+    return -(sum / (double)65536.0f);
+}
+
+double orc_mi_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T)
+{
+    int32_t* hist = (int32_t*)malloc(65536 * sizeof(int32_t));
+    int32_t fh[256];
+    orc_histogram_u8(from, (long long)fdim[0] * fdim[1] * fdim[2], fh);
+    orc_mi_hist_u8(from, fdim, to, tdim, T, hist);
+    double c = orc_mi_cost_from_hist(hist, fh);
+    free(hist);
+    return c;
+}
+
+/* correlation functor CPU (reg/linear.hpp:23-37): the smaller volume is the
+ * fixed grid (the transform is inverted when the roles swap); the other is
+ * resampled onto it with the CPU resample (integer-shift copy included) and
+ * cost = 1 - r^2, r formed in double from exact integer sums
+ * (numerical/statistics.hpp:569-580, 311-322, 257-309, 491-567) and squared in float. */
+double orc_corr_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T)
+{
+    long long nf = (long long)fdim[0] * fdim[1] * fdim[2];
+    long long nt = (long long)tdim[0] * tdim[1] * tdim[2];
+    if (nf > nt) {
+        float Ti[12];
+        memcpy(Ti, T, sizeof(Ti));
+        orc_matrix_inverse(Ti);
+        return orc_corr_cost_u8(to, tdim, from, fdim, Ti);
+    }
+    uint8_t* y = (uint8_t*)malloc((size_t)nf);
+    orc_resample_u8(to, tdim, y, fdim, T, 1);
+    long long sx = 0, sy = 0, sxx = 0, syy = 0, sxy = 0;
+    for (long long i = 0; i < nf; ++i) {
+        sx += from[i];
+        sy += y[i];
+        sxx += (long long)from[i] * from[i];
+        syy += (long long)y[i] * y[i];
+        sxy += (long long)from[i] * y[i];
+    }
+    free(y);
+    double n = (double)nf;
+    double mx = (double)sx / n, my = (double)sy / n;
+    double vx = (double)sxx / n - mx * mx, vy = (double)syy / n - my * my;
+    double sd1 = vx > 0.0 ? sqrt(vx) : 0.0, sd2 = vy > 0.0 ? sqrt(vy) : 0.0;
+    double c = 0.0;
+    if (!(sd1 == 0 || sd2 == 0))
+        c = ((double)sxy / n - mx * my) / sd1 / sd2;
+    float cf = (float)c;
+    return (double)(1.0f - cf * cf);
+}

@@ -1,0 +1,69 @@
+/* Test infrastructure only (the checker, never the product path).
+ *
+ * Plain-C restatement of the reference's CPU registration hot path, built into
+ * oracle/liboracle.so by oracle/Makefile.  Volumes are x-fastest,
+ * index = (z*h + y)*w + x; displacement fields are AoS xyz per voxel.
+ * A transform T is the reference's transformation_matrix storage:
+ * T[0..8] = sr (row-major 3x3), T[9..11] = shift (numerical/transformation.hpp:589-605).
+ *
+ * Suffixes: _u8 / _f32 are reference-exact (bit-identical to the reference's own
+ * -O2 -ffp-contract=off build); _f64 computes everything in double and exists only
+ * to report how far the FP32 paths are from exact arithmetic.
+ */
+#ifndef REGB_ORACLE_H
+#define REGB_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void orc_affine_to_matrix(const float* param, const int* from_dim, const float* from_vs, const int* to_dim,
+                          const float* to_vs, float* T);
+void orc_affine_to_matrix_f64(const double* param, const int* from_dim, const double* from_vs, const int* to_dim,
+                              const double* to_vs, double* T);
+int orc_matrix_inverse(float* T);
+int orc_is_integer_shift(const float* T, int* shift);
+
+void orc_resample_u8(const uint8_t* from, const int* fdim, uint8_t* to, const int* tdim, const float* T, int allow_crop);
+void orc_resample_f32(const float* from, const int* fdim, float* to, const int* tdim, const float* T, int allow_crop);
+
+void orc_histogram_u8(const uint8_t* img, long long n, int32_t* hist256);
+void orc_mi_hist_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T,
+                    int32_t* hist);
+double orc_mi_cost_from_hist(const int32_t* hist, const int32_t* from_hist);
+double orc_mi_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T);
+double orc_corr_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T);
+
+void orc_compose_u8(const uint8_t* Is, const int* dim, const float* dis, uint8_t* Js);
+void orc_compose_f32(const float* Is, const int* dim, const float* dis, float* Js);
+void orc_compose_f64(const double* Is, const int* dim, const double* dis, double* Js);
+float orc_cdm_gradient_u8(const uint8_t* Js, const uint8_t* It, const int* dim, float* new_d, int gradient_type);
+float orc_cdm_gradient_f32(const float* Js, const float* It, const int* dim, float* new_d, int gradient_type);
+double orc_cdm_gradient_f64(const double* Js, const double* It, const int* dim, double* new_d, int gradient_type);
+void orc_downsample_u8(const uint8_t* in, const int* dim, uint8_t* out);
+void orc_downsample_f32(const float* in, const int* dim, float* out);
+void orc_downsample_f64(const double* in, const int* dim, double* out);
+
+void orc_cdm_poisson_f32(float* new_d, const int* dim, int sweeps);
+void orc_cdm_poisson_f64(double* new_d, const int* dim, int sweeps);
+float orc_cdm_max_len_f32(const float* d, const int* dim);
+double orc_cdm_max_len_f64(const double* d, const int* dim);
+void orc_accumulate_f32(const float* cur_d, float* new_d, const int* dim);
+void orc_accumulate_f64(const double* cur_d, double* new_d, const int* dim);
+void orc_cdm_smooth_f32(const float* d, float* dd, const int* dim, float smoothing);
+void orc_cdm_smooth_f64(const double* d, double* dd, const int* dim, double smoothing);
+void orc_upsample_field_x2_f32(const float* in, const int* in_dim, float* out, const int* out_dim);
+void orc_upsample_field_x2_f64(const double* in, const int* in_dim, double* out, const int* out_dim);
+
+int orc_cdm_level_u8(const uint8_t* It, const uint8_t* Is, const int* dim, float* best_d, float resolution,
+                     float speed, float smoothing, unsigned int min_dimension, int gradient_type, int* iters_out);
+int orc_cdm_level_f32(const float* It, const float* Is, const int* dim, float* best_d, float resolution, float speed,
+                      float smoothing, unsigned int min_dimension, int gradient_type, int* iters_out);
+int orc_cdm_level_f64(const double* It, const double* Is, const int* dim, double* best_d, float resolution,
+                      float speed, float smoothing, unsigned int min_dimension, int gradient_type, int* iters_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

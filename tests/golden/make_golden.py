@@ -1,0 +1,130 @@
+"""Generate the golden fixtures in this folder from the reference's own CPU code.
+
+Run where the reference tree is present (it builds oracle/_ref/libtipl_ref.so from
+it):  python tests/golden/make_golden.py [--ref-root PATH]
+
+Every fixture stores its seeded inputs together with the reference's outputs, so
+the tests need neither the reference nor the phantom generator to replay them.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from tipl_b200 import phantom as ph  # noqa: E402
+
+
+def save(name, **arrays):
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **arrays)
+    print(f"{name}: {os.path.getsize(path)} bytes")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref-root", default=os.environ.get("TIPL_REF_ROOT", oracle.DEFAULT_REF_ROOT))
+    args = ap.parse_args()
+    oracle.build(args.ref_root, with_ref=True)
+    R = oracle.Reference()
+    R.set_threads(1)
+    rng = np.random.default_rng(ph.seed_for(0, 1))
+
+    # transformation_matrix(affine_param, ...) and its inverse
+    params, shapes, T_out, Ti_out = [], [], [], []
+    for k in range(24):
+        fs = tuple(int(v) for v in rng.integers(5, 60, 3))
+        ts = tuple(int(v) for v in rng.integers(5, 60, 3))
+        fvs = rng.uniform(0.7, 2.2, 3).astype(np.float32)
+        tvs = rng.uniform(0.7, 2.2, 3).astype(np.float32)
+        if k % 4 == 0:
+            tvs[:] = 1.0
+        p = ph.random_affine(rng, rot_deg=25, trans_vox=8, vs=fvs)
+        T = R.affine_to_matrix(p, fs, fvs, ts, tvs)
+        params.append(np.concatenate([p, fvs, tvs]))
+        shapes.append(np.array(fs + ts, np.int32))
+        T_out.append(T)
+        Ti_out.append(R.matrix_inverse(T))
+    save("transforms", params=np.array(params, np.float32), shapes=np.array(shapes), T=np.array(T_out),
+         Tinv=np.array(Ti_out))
+
+    # resample (uint8 and float), including the integer-shift copy path
+    src8 = (rng.random((23, 19, 17)) * 256).astype(np.uint8)
+    srcf = rng.random((23, 19, 17)).astype(np.float32)
+    out_shape = (20, 21, 18)
+    Ts = []
+    for k in range(6):
+        p = ph.random_affine(rng, rot_deg=20, trans_vox=4)
+        Ts.append(R.affine_to_matrix(p, out_shape, (1, 1, 1), src8.shape, (1, 1, 1)))
+    Ts.append(np.array([1, 0, 0, 0, 1, 0, 0, 0, 1, 2, -3, 1], np.float32))  # integer shift: copy path
+    Ts.append(np.array([1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0], np.float32))   # identity
+    Ts = np.array(Ts, np.float32)
+    save("resample", src8=src8, srcf=srcf, out_shape=np.array(out_shape), T=Ts,
+         out8=np.array([R.resample(src8, out_shape, T) for T in Ts]),
+         outf=np.array([R.resample(srcf, out_shape, T) for T in Ts]))
+
+    # MI joint histogram / MI cost / correlation cost on a small phantom pair
+    tmpl, mov, _ = ph.affine_pair((30, 34, 28), rng=rng)
+    f8 = ph.normalize_to_u8(tmpl)
+    m8 = ph.normalize_to_u8(mov)
+    m8b = m8[1:-2, 2:, :-3].copy()  # a moving volume of another shape
+    Ts, mi, corr, corr_swap, hists = [], [], [], [], []
+    for k in range(5):
+        p = ph.random_affine(rng, rot_deg=8, trans_vox=3) if k else np.array([0, 0, 0, 0, 0, 0, 1, 1, 1, 0, 0, 0],
+                                                                            np.float32)
+        T = R.affine_to_matrix(p, f8.shape, (1, 1, 1), m8b.shape, (1, 1, 1))
+        Ts.append(T)
+        hists.append(R.mi_hist(f8, m8b, T))
+        mi.append(R.mi_cost(f8, m8b, T))
+        corr.append(R.corr_cost(f8, m8b, T))
+        corr_swap.append(R.corr_cost(m8b, f8, T))
+    save("affine_costs", fixed=f8, moving=m8b, T=np.array(Ts), hist=np.array(hists), mi=np.array(mi),
+         corr=np.array(corr), corr_swap=np.array(corr_swap), from_hist=R.histogram(f8))
+
+    # CDM passes on odd shapes (flat-index wrap, 1- and 2-voxel axes)
+    cases = {}
+    for ci, shp in enumerate([(17, 9, 5), (6, 11, 13), (2, 7, 9), (1, 8, 8)]):
+        It = (rng.random(shp) * 256).astype(np.uint8)
+        Is = (rng.random(shp) * 256).astype(np.uint8)
+        It.flat[:: 7] = 0
+        Itf = rng.random(shp).astype(np.float32)
+        Isf = rng.random(shp).astype(np.float32)
+        d = rng.normal(0, 1.5, shp + (3,)).astype(np.float32)
+        d.reshape(-1, 3)[::4] = 0
+        cd = rng.normal(0, 1.0, shp + (3,)).astype(np.float32)
+        c = {"It": It, "Is": Is, "Itf": Itf, "Isf": Isf, "d": d, "cd": cd}
+        c["compose8"] = R.compose(Is, d)
+        c["composef"] = R.compose(Isf, d)
+        for gt in "rd":
+            c[f"grad8_{gt}"], c[f"cost8_{gt}"] = R.cdm_gradient(Is, It, gt)
+            c[f"gradf_{gt}"], c[f"costf_{gt}"] = R.cdm_gradient(Isf, Itf, gt)
+        c["poisson"] = R.cdm_poisson(d)
+        c["maxlen"] = np.float32(R.cdm_max_len(d))
+        c["accumulate"] = R.accumulate(cd, d)
+        c["smooth"] = R.cdm_smooth(d, 0.4)
+        c["down8"] = R.downsample(Is)
+        c["downf"] = R.downsample(Isf)
+        small = d[: (shp[0] + 1) // 2, : (shp[1] + 1) // 2, : (shp[2] + 1) // 2].copy()
+        c["up_in"] = small
+        c["up"] = R.upsample_field_x2(small, shp)
+        for k, v in c.items():
+            cases[f"c{ci}_{k}"] = np.asarray(v)
+    save("cdm_passes", **cases)
+
+    # CDM end to end (default parameters): uint8 and float, 32^3 blob pair
+    t, m, _ = ph.cdm_pair((32, 32, 32), rng=rng)
+    t8, m8 = ph.normalize_to_u8(t), ph.normalize_to_u8(m)
+    d8, ok8 = R.cdm(t8, m8)
+    df, okf = R.cdm(t, m)
+    save("cdm_e2e", It8=t8, Is8=m8, d8=d8, ok8=np.array(ok8), Itf=t, Isf=m, df=df, okf=np.array(okf))
+
+
+if __name__ == "__main__":
+    main()

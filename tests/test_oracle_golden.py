@@ -1,0 +1,108 @@
+"""Pins the plain-C oracle to the reference: every golden fixture (made by
+tests/golden/make_golden.py from the reference's own CPU build) must be reproduced
+bit for bit.  When the reference build is present (oracle/_ref), a few fresh seeded
+cases are also compared live."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+
+def bits(a):
+    a = np.asarray(a)
+    return a.view({1: np.uint8, 4: np.uint32, 8: np.uint64}[a.dtype.itemsize])
+
+
+def same(a, b):
+    return np.array_equal(bits(a), bits(b))
+
+
+def test_transforms(orc, golden):
+    g = golden("transforms")
+    for p, s, T, Ti in zip(g["params"], g["shapes"], g["T"], g["Tinv"]):
+        fs = (s[0], s[1], s[2])
+        ts = (s[3], s[4], s[5])
+        got = orc.affine_to_matrix(p[:12], fs, p[12:15], ts, p[15:18])
+        assert same(got, T)
+        assert same(orc.matrix_inverse(T), Ti)
+
+
+def test_resample(orc, golden):
+    g = golden("resample")
+    shape = tuple(g["out_shape"])
+    for T, o8, of in zip(g["T"], g["out8"], g["outf"]):
+        assert same(orc.resample(g["src8"], shape, T), o8)
+        assert same(orc.resample(g["srcf"], shape, T), of)
+
+
+def test_affine_costs(orc, golden):
+    g = golden("affine_costs")
+    f, m = g["fixed"], g["moving"]
+    assert same(orc.histogram(f), g["from_hist"])
+    for T, h, mi, c, cs in zip(g["T"], g["hist"], g["mi"], g["corr"], g["corr_swap"]):
+        hist = orc.mi_hist(f, m, T)
+        assert same(hist, h)
+        assert int(hist.sum()) == f.size
+        assert orc.mi_cost(f, m, T) == pytest.approx(mi, rel=1e-12)
+        assert orc.mi_cost_from_hist(h, g["from_hist"]) == pytest.approx(mi, rel=1e-12)
+        assert orc.corr_cost(f, m, T) == c  # exact integer moments: bit-exact
+        assert orc.corr_cost(m, f, T) == cs  # roles swapped, transform inverted
+
+
+@pytest.mark.parametrize("ci", range(4))
+def test_cdm_passes(orc, golden, ci):
+    g = golden("cdm_passes")
+    c = {k.split("_", 1)[1]: g[k] for k in g.files if k.startswith(f"c{ci}_")}
+    assert same(orc.compose(c["Is"], c["d"]), c["compose8"])
+    assert same(orc.compose(c["Isf"], c["d"]), c["composef"])
+    for gt in "rd":
+        nd, cost = orc.cdm_gradient(c["Is"], c["It"], gt)
+        assert same(nd, c[f"grad8_{gt}"]) and np.float32(cost) == c[f"cost8_{gt}"]
+        nd, cost = orc.cdm_gradient(c["Isf"], c["Itf"], gt)
+        assert same(nd, c[f"gradf_{gt}"]) and np.float32(cost) == c[f"costf_{gt}"]
+    assert same(orc.cdm_poisson(c["d"]), c["poisson"])
+    assert np.float32(orc.cdm_max_len(c["d"])) == c["maxlen"]
+    assert same(orc.accumulate(c["cd"], c["d"]), c["accumulate"])
+    assert same(orc.cdm_smooth(c["d"], 0.4), c["smooth"])
+    assert same(orc.downsample(c["Is"]), c["down8"])
+    assert same(orc.downsample(c["Isf"]), c["downf"])
+    assert same(orc.upsample_field_x2(c["up_in"], c["Is"].shape), c["up"])
+
+
+def test_cdm_end_to_end(orc, golden):
+    g = golden("cdm_e2e")
+    d8, ok8, _ = orc.cdm(g["It8"], g["Is8"])
+    assert ok8 == bool(g["ok8"]) and same(d8, g["d8"])
+    df, okf, _ = orc.cdm(g["Itf"], g["Isf"])
+    assert okf == bool(g["okf"]) and same(df, g["df"])
+
+
+def test_f64_oracle_close_to_f32(orc, golden):
+    """The all-double restatement agrees with the FP32 one to FP32 accuracy."""
+    g = golden("cdm_passes")
+    d = g["c1_d"]
+    p32 = orc.cdm_poisson(d)
+    p64 = orc.cdm_poisson(d.astype(np.float64))
+    assert np.abs(p32 - p64).max() <= 1e-5 * max(1.0, np.abs(p64).max())
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.REF_SO), reason="reference build not present")
+def test_live_against_reference(orc):
+    R = oracle.Reference()
+    rng = np.random.default_rng(7)
+    from tipl_b200 import phantom as ph
+
+    t, m, _ = ph.cdm_pair((24, 22, 20), rng=rng)
+    t8, m8 = ph.normalize_to_u8(t), ph.normalize_to_u8(m)
+    assert same(t8, R.normalize_to_u8(t))
+    a, oka, _ = orc.cdm(t8, m8, min_dimension=8)
+    b, okb = R.cdm(t8, m8, min_dimension=8)
+    assert oka == okb and same(a, b)
+    for k in range(3):
+        p = ph.random_affine(rng, rot_deg=15, trans_vox=3)
+        T = orc.affine_to_matrix(p, t8.shape, (1, 1, 1), m8.shape, (1, 1, 1))
+        assert same(T, R.affine_to_matrix(p, t8.shape, (1, 1, 1), m8.shape, (1, 1, 1)))
+        assert same(orc.mi_hist(t8, m8, T), R.mi_hist(t8, m8, T))
+        assert orc.corr_cost(t8, m8, T) == R.corr_cost(t8, m8, T)
