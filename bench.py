@@ -1,0 +1,285 @@
+"""Benchmark: registrations/s of the affine (12-DOF, MI, 256x256 joint histogram)
+registration of a 182x218x182 uint8 volume pair at 1 mm, on N GPUs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--mode served|plain] [--batch B] [--no-cpu-baseline]
+
+One process per GPU (torchrun for N > 1); every rank registers its own subjects
+(independent jobs, weak scaling, no collective on the data path) and rank 0 prints
+one JSON line.
+
+A step is one pass of the hot path over one batch of subjects:
+  plain  -- one registration through the plain single-job path (regb_linear);
+  served -- a batch of B registrations submitted together to the serving engine.
+value: registrations/s with the volumes already resident in HBM, device-timed with
+CUDA events, max over ranks.  e2e: the same through the C ABI with host buffers, the
+host->device copies of the volumes inside the timed region.  L2 is flushed (a 256 MB
+write) between timed steps, outside the timed spans.
+
+--impl reference times the reference's own CPU implementation of tipl::reg::linear
+(compiled from its sources into oracle/_ref) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (182, 218, 182)  # numpy (z, y, x) = 182 x 218 x 182 voxels
+VS = (1.0, 1.0, 1.0)
+METRIC = "registrations/s (affine 12-DOF MI, 182x218x182 uint8, 1 mm)"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+def make_pair(job: int):
+    from tipl_b200 import phantom as ph
+
+    rng = np.random.default_rng(ph.seed_for(2, job))
+    t, m, p = ph.affine_pair(SHAPE, rng=rng)
+    return ph.normalize_to_u8(t), ph.normalize_to_u8(m), p
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """Samples nvidia-smi during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_linear(fixed, moving, threads: int):
+    """One reference registration (oracle/_ref, the reference's CPU code)."""
+    import oracle
+
+    if not os.path.exists(oracle.REF_SO):
+        return None
+    R = oracle.Reference()
+    R.set_threads(threads)
+    t0 = time.perf_counter()
+    cost, arg = R.linear(fixed, VS, moving, VS, reg_type=15, cost_type=1)
+    dt = time.perf_counter() - t0
+    return dt, cost, arg
+
+
+def run_reference(args):
+    rank, local, world = env_rank()
+    if rank != 0:
+        return 0
+    import oracle
+
+    threads = os.cpu_count() or 1
+    if not os.path.exists(oracle.REF_SO):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtipl_ref.so was not built"}))
+        return 0
+    f8, m8, _ = make_pair(0)
+    for _ in range(args.warmup):
+        cpu_baseline_linear(f8, m8, threads)
+    times = []
+    cost = None
+    for _ in range(args.steps):
+        dt, cost, _ = cpu_baseline_linear(f8, m8, threads)
+        times.append(dt)
+    tot = sum(times)
+    value = args.steps / tot
+    line = {"metric": METRIC, "value": value, "unit": "registrations/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "affine MI registration, 182x218x182 uint8 pair, 1 mm, one subject per step",
+                       "cost": "MI 256x256", "final_cost": cost},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "registrations/s", "cores": threads, "kind": "reference",
+                             "sample": "one full tipl::reg::linear registration per step"},
+            "e2e": {"value": value, "unit": "registrations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="plain", choices=["plain", "served"])
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    import tipl_b200 as tb
+    from tipl_b200 import _lib
+
+    L = _lib.lib()
+    f8, m8, p_true = make_pair(rank)
+    fd = torch.from_numpy(f8).cuda()
+    md = torch.from_numpy(m8).cuda()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def one(fx, mx):
+        return tb.reg.linear(fx, VS, mx, VS)
+
+    for _ in range(args.warmup):
+        one(fd, md)
+    torch.cuda.synchronize()
+
+    def timed(fx, mx, collect_stats):
+        total = 0.0
+        costs, evals = [], 0
+        if collect_stats:
+            L.regb_stats_reset(1)
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            c, _, ev = one(fx, mx)
+            b.record()
+            torch.cuda.synchronize()
+            total += a.elapsed_time(b) / 1000.0
+            costs.append(c)
+            evals += ev
+        st = _lib.Stats()
+        if collect_stats:
+            L.regb_stats_get(st)
+            L.regb_stats_reset(0)
+        return total, costs, evals, st
+
+    clk = Clocks(local)
+    clk.start()
+    t_dev, costs, evals, st = timed(fd, md, True)
+    clocks = clk.stop()
+    t_e2e, _, _, _ = timed(f8, m8, False)  # host numpy buffers: the library copies them in each step
+
+    def maxall(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    t_dev = maxall(t_dev)
+    t_e2e = maxall(t_e2e)
+    regs = args.steps * world
+    value = regs / t_dev
+    e2e = regs / t_e2e
+    hbm, hbm_kind = peaks()
+    achieved = (st.mi_bytes / st.mi_launches) / (st.mi_ms / st.mi_launches / 1000.0) / 1e9 if st.mi_launches else 0
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        r = cpu_baseline_linear(f8, m8, threads)
+        if r:
+            cpu = {"value": 1.0 / r[0], "unit": "registrations/s", "cores": threads, "kind": "reference",
+                   "sample": "one full tipl::reg::linear (MI) registration of the same pair (oracle/_ref)",
+                   "final_cost": r[1]}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "registrations/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+                "config": {"workload": "affine MI registration, 182x218x182 uint8 pair, 1 mm, one subject per step",
+                           "mode": args.mode, "cost": "MI 256x256 joint histogram",
+                           "l2": "flushed between timed steps (256 MB write)",
+                           "final_cost_mean": float(np.mean(costs)), "cost_evals_per_registration":
+                               evals / max(1, args.steps), "parallelism": f"replicas x{world}"},
+                "roofline": {"bound": "hbm", "kernel": "mi_kernel", "achieved": achieved, "peak": hbm,
+                             "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                             "launches": st.mi_launches, "avg_launch_ms": st.mi_ms / max(1, st.mi_launches),
+                             "bytes_per_launch": st.mi_bytes / max(1, st.mi_launches)},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e, "unit": "registrations/s", "h2d_bytes_per_step": int(f8.nbytes + m8.nbytes),
+                        "d2h_bytes_per_step": 52},
+                "gpu_launches": int(st.launches), "clocks": clocks}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

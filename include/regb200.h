@@ -1,0 +1,182 @@
+/* regb200 -- C ABI of the B200 (sm_100a) registration hot path.
+ *
+ * Drop-in boundary for the reference's registration calls.  Each entry point below
+ * names the reference interface it replaces (file:line within the reference
+ * project).  Conventions:
+ *   - volumes are x-fastest, index = (z*h + y)*w + x (utility/basic_image.hpp:160);
+ *   - a displacement field is AoS float xyz per voxel (tipl::vector<3>);
+ *   - a transform T[12] is the reference's transformation_matrix storage:
+ *     T[0..8] = sr row-major, T[9..11] = shift; it maps a voxel of the fixed
+ *     ("from") grid to a voxel of the sampled ("to") volume
+ *     (numerical/transformation.hpp:589-605, 834-839);
+ *   - an affine parameter vector is affine_param<float,3> order:
+ *     translocation[3], rotation[3], scaling[3], affine[3]
+ *     (numerical/transformation.hpp:428-438);
+ *   - every call returns a regb_status; nothing throws across the ABI.
+ * Pointers in a regb_volume / regb_field with location REGB_DEVICE are CUDA device
+ * pointers on the current device; REGB_HOST pointers are ordinary host memory, and
+ * the call copies in and out itself.  `stream` arguments are cudaStream_t values
+ * (NULL = the legacy default stream); calls on host memory synchronise before they
+ * return.
+ */
+#ifndef REGB200_H
+#define REGB200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int regb_status;
+#define REGB_OK 0
+#define REGB_FALSE 1            /* the reference's `false` (cdm: zero cost / no result) */
+#define REGB_ERR_ARG (-1)       /* bad argument (null pointer, size, dtype, limit) */
+#define REGB_ERR_CUDA (-2)      /* a CUDA runtime error; see regb_last_error() */
+#define REGB_ERR_NOMEM (-3)     /* device allocation failed */
+#define REGB_CANCELLED (-4)     /* the caller's terminated flag was set */
+#define REGB_ERR_NOTFOUND (-5)  /* unknown job id */
+#define REGB_PENDING (-6)       /* job not finished yet (regb_poll) */
+#define REGB_ERR_BUDGET (-7)    /* job larger than the engine's device-memory budget */
+
+typedef enum { REGB_U8 = 0, REGB_F32 = 1, REGB_U16 = 2, REGB_BF16 = 3 } regb_dtype;
+typedef enum { REGB_HOST = 0, REGB_DEVICE = 1 } regb_location;
+
+typedef struct {
+    void* ptr;
+    int dim[3]; /* w, h, d */
+    int dtype;  /* regb_dtype */
+    int location;
+} regb_volume;
+
+typedef struct {
+    float* ptr; /* 3 floats per voxel */
+    int dim[3];
+    int location;
+} regb_field;
+
+/* reg/linear.hpp:255-256 */
+typedef enum { REGB_REG_TRANSLOCATION = 1, REGB_REG_ROTATION = 2, REGB_REG_RIGID_BODY = 3,
+               REGB_REG_SCALING = 4, REGB_REG_TRANSLOCATION_SCALING = 5, REGB_REG_RIGID_SCALING = 7,
+               REGB_REG_TILT = 8, REGB_REG_AFFINE = 15 } regb_reg_type;
+typedef enum { REGB_COST_CORR = 0, REGB_COST_MI = 1 } regb_cost_type;
+typedef enum { REGB_BOUND_REG = 0, REGB_BOUND_NARROW = 1, REGB_BOUND_LARGE = 2 } regb_bound;
+
+/* linear_reg_param (reg/linear.hpp:268-288); bound selects reg_bound / narrow_bound /
+ * large_bound (reg/linear.hpp:258-266). */
+typedef struct {
+    int reg_type;          /* regb_reg_type, default AFFINE */
+    int cost_type;         /* regb_cost_type, default MI */
+    int bound;             /* regb_bound, default REGB_BOUND_REG */
+    unsigned int search_count; /* default 16 */
+    int absolute_bound;    /* default 1 */
+} regb_linear_param;
+
+/* cdm_param (reg/cdm.hpp:36-44); gradient_type 'r' (local correlation) or 'd'. */
+typedef struct {
+    float resolution;      /* default 2.0 */
+    float speed;           /* default 0.3 */
+    float smoothing;       /* default 0.05 */
+    unsigned int min_dimension; /* default 16 */
+    int gradient_type;     /* default 'r' */
+} regb_cdm_param;
+
+void regb_linear_param_default(regb_linear_param* p);
+void regb_cdm_param_default(regb_cdm_param* p);
+
+/* Library status. */
+const char* regb_version(void);
+const char* regb_last_error(void);   /* thread-local text of the last failure */
+regb_status regb_device_info(int* device, int* sm_count, size_t* free_bytes, size_t* total_bytes);
+/* Release every cached device buffer of this thread's context. */
+regb_status regb_release(void);
+
+/* Launch accounting (no reference counterpart: instrumentation of this library).
+ * launches counts every kernel this library launched since the last reset; with
+ * timing on, each MI / correlation cost launch is bracketed by CUDA events on its
+ * stream and its algorithmic bytes (fixed voxels + sampled voxels + 2*256 KB of
+ * histogram for MI) are accumulated. */
+typedef struct {
+    long long launches;
+    long long mi_launches, mi_tasks;
+    double mi_voxels, mi_bytes, mi_ms;
+    long long corr_launches, corr_tasks;
+    double corr_voxels, corr_bytes, corr_ms;
+} regb_stats;
+regb_status regb_stats_reset(int timing);
+regb_status regb_stats_get(regb_stats* out);
+
+/* ---- transform algebra (host) -------------------------------------------------- */
+/* transformation_matrix(affine_param, from, from_vs, to, to_vs)
+ * (numerical/transformation.hpp:636-701), in float as the reference computes it. */
+regb_status regb_affine_to_matrix(const float param[12], const int from_dim[3], const float from_vs[3],
+                                  const int to_dim[3], const float to_vs[3], float T[12]);
+/* The same composition in double (the FP64 affine path). */
+regb_status regb_affine_to_matrix_f64(const double param[12], const int from_dim[3], const double from_vs[3],
+                                      const int to_dim[3], const double to_vs[3], double T[12]);
+/* transformation_matrix::inverse (numerical/transformation.hpp:820-832); REGB_FALSE if singular. */
+regb_status regb_matrix_inverse(float T[12]);
+
+/* ---- resample ------------------------------------------------------------------- */
+/* tipl::resample<linear>(from, to, trans) (numerical/resampling.hpp:1239-1298):
+ * to(x) = trilinear(from, T x), 0 outside; uint8 results truncate like the
+ * reference.  allow_shift_copy != 0 takes the CPU path's integer-shift copy
+ * (resampling.hpp:1243-1262) when T qualifies. from/to must share dtype (U8 or F32)
+ * and location. */
+regb_status regb_resample(const regb_volume* from, regb_volume* to, const float T[12], int allow_shift_copy,
+                          void* stream);
+
+/* ---- affine costs ---------------------------------------------------------------- */
+/* mutual_information<3>::operator() (reg/linear.hpp:173-203, GPU 207-252) for K
+ * candidate transforms at once: cost[k] = -MI of the 256x256 joint histogram of the
+ * uint8 fixed volume and the trilinear uint8 sample of the moving volume.
+ * hist_out (optional, host, K*65536 int32) receives the joint histograms. */
+regb_status regb_mi_cost(const regb_volume* fixed, const regb_volume* moving, const float* T, int K,
+                         double* cost, int32_t* hist_out, void* stream);
+/* correlation::operator() (reg/linear.hpp:23-78) for K transforms: 1 - r^2 with the
+ * smaller volume as the grid (transform inverted when the roles swap). */
+regb_status regb_corr_cost(const regb_volume* fixed, const regb_volume* moving, const float* T, int K,
+                           double* cost, void* stream);
+
+/* ---- displacement algebra -------------------------------------------------------- */
+/* tipl::compose_displacement(from, dis, to) (numerical/dif.hpp:90-115, 260-285). */
+regb_status regb_compose_displacement(const regb_volume* from, const regb_field* dis, regb_volume* to,
+                                      void* stream);
+/* tipl::accumulate_displacement(dis, new_dis) (numerical/dif.hpp:166-186, 311-329):
+ * new_dis <- dis composed with new_dis, in place. */
+regb_status regb_accumulate_displacement(const regb_field* dis, regb_field* new_dis, void* stream);
+/* downsample_with_padding (numerical/resampling.hpp:575-671); out dims (d+1)/2. */
+regb_status regb_downsample(const regb_volume* in, regb_volume* out, void* stream);
+/* best_d *= 2; upsample_with_padding(best_d, shape) (reg/cdm.hpp:402-403,
+ * numerical/resampling.hpp:849-891). */
+regb_status regb_upsample_field_x2(const regb_field* in, regb_field* out, void* stream);
+
+/* ---- CDM passes (reg/cdm.hpp) ----------------------------------------------------- */
+/* cdm_get_gradient (reg/cdm.hpp:84-151): new_d = gradient, *cost = mean cost. */
+regb_status regb_cdm_gradient(const regb_volume* Js, const regb_volume* It, regb_field* new_d, int gradient_type,
+                              float* cost, void* stream);
+/* cdm_solve_poisson (reg/cdm.hpp:158-253), 12 Jacobi sweeps, in place. */
+regb_status regb_cdm_poisson(regb_field* new_d, void* stream);
+/* cdm_max_displacement_length (reg/cdm.hpp:260-295). */
+regb_status regb_cdm_max_length(const regb_field* d, float* out, void* stream);
+/* cdm_smooth (reg/cdm.hpp:302-366): dd = blend(d, smoothing). */
+regb_status regb_cdm_smooth(const regb_field* d, regb_field* dd, float smoothing, void* stream);
+
+/* ---- whole registrations ---------------------------------------------------------- */
+/* tipl::reg::cdm_common<out,T,3>(It, Is, dis, terminated, param) (reg/cdm.hpp:534-558,
+ * the GPU path cdm_cuda 492-524): one modality; It/Is uint8 or float, same dims and
+ * dtype; dis_out receives the field.  Returns REGB_FALSE where the reference
+ * returns false.  terminated (may be NULL) is polled between iterations. */
+regb_status regb_cdm(const regb_volume* It, const regb_volume* Is, regb_field* dis_out, const regb_cdm_param* param,
+                     volatile const int* terminated);
+/* tipl::reg::linear<out,3>(from, from_vs, to, to_vs, arg, param, terminated)
+ * (reg/linear.hpp:622-700): uint8 volumes (one image pair), arg in/out, final cost
+ * out.  cost_evals (may be NULL) receives the number of cost evaluations. */
+regb_status regb_linear(const regb_volume* from, const float from_vs[3], const regb_volume* to,
+                        const float to_vs[3], float arg[12], const regb_linear_param* param,
+                        volatile const int* terminated, float* cost_out, long long* cost_evals);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

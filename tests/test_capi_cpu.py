@@ -1,0 +1,84 @@
+"""CPU-side checks of the C ABI: the library loads, exports every entry point that
+include/regb200.h declares, and its host-only transform algebra matches the
+reference's (golden fixtures) bit for bit.  No device is touched."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from tipl_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "regb200.h")
+
+
+def declared():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(regb_[a-z0-9_]+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def L():
+    from tipl_b200 import build
+
+    build.build()
+    return _lib.lib()
+
+
+def test_header_symbols_exported(L):
+    names = declared()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(L, n), f"{n} declared in regb200.h but not exported"
+    # and the Python binding covers them all
+    assert set(names) <= set(_lib.declared_symbols()) | {"regb_status"}
+
+
+def bits(a):
+    return np.asarray(a).view(np.uint32)
+
+
+def test_transforms_match_reference(L, golden):
+    import tipl_b200 as tb
+
+    g = golden("transforms")
+    for p, s, T, Ti in zip(g["params"], g["shapes"], g["T"], g["Tinv"]):
+        fs = (s[0], s[1], s[2])  # numpy (z, y, x)
+        ts = (s[3], s[4], s[5])
+        got = tb.affine_to_matrix(p[:12], fs, p[12:15], ts, p[15:18])
+        assert np.array_equal(bits(got), bits(T))
+        assert np.array_equal(bits(tb.matrix_inverse(T)), bits(Ti))
+
+
+def test_f64_composition_close(L, golden):
+    import tipl_b200 as tb
+
+    g = golden("transforms")
+    for p, s, T in zip(g["params"], g["shapes"], g["T"]):
+        fs = (s[0], s[1], s[2])
+        ts = (s[3], s[4], s[5])
+        T64 = tb.affine_to_matrix_f64(p[:12].astype(np.float64), fs, p[12:15], ts, p[15:18])
+        assert np.allclose(T64, T, rtol=1e-5, atol=1e-3)
+
+
+def test_bad_arguments_are_status_codes(L):
+    v = _lib.Volume(None, (C.c_int * 3)(4, 4, 4), _lib.U8, _lib.HOST)
+    st = L.regb_resample(C.byref(v), C.byref(v), None, 0, None)
+    assert st == _lib.REGB_ERR_ARG
+    assert b"null" in L.regb_last_error()
+    assert L.regb_matrix_inverse(None) == _lib.REGB_ERR_ARG
+    sing = np.zeros(12, np.float32)
+    assert L.regb_matrix_inverse(sing.ctypes.data_as(C.c_void_p)) == _lib.REGB_FALSE
+
+
+def test_param_defaults(L):
+    p = _lib.LinearParam()
+    L.regb_linear_param_default(C.byref(p))
+    assert (p.reg_type, p.cost_type, p.search_count, p.absolute_bound) == (15, 1, 16, 1)
+    q = _lib.CdmParam()
+    L.regb_cdm_param_default(C.byref(q))
+    assert (q.resolution, q.min_dimension, chr(q.gradient_type)) == (2.0, 16, "r")
+    assert abs(q.speed - 0.3) < 1e-7 and abs(q.smoothing - 0.05) < 1e-7

@@ -1,0 +1,202 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle and the golden
+fixtures made from the reference.
+
+Bars: bit-exact for integer/byte/index results (uint8 resamples, joint-histogram
+counts, correlation cost built from exact integer moments) and for every FP32 CDM
+pass (the kernels reproduce the reference's operation order, FMA contraction off);
+the MI cost, a double sum of n*ln(n/(row*col)) reduced in a different order, within
+1e-12 relative; the CDM mean cost within 1 float ulp.
+"""
+import numpy as np
+import pytest
+
+import tipl_b200 as tb
+from tipl_b200 import phantom as ph
+
+pytestmark = pytest.mark.gpu
+
+
+def bits(a):
+    a = np.asarray(a)
+    return a.view({1: np.uint8, 4: np.uint32, 8: np.uint64}[a.dtype.itemsize])
+
+
+def same(a, b):
+    return np.array_equal(bits(a), bits(b))
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from tipl_b200 import build
+
+    build.build()
+
+
+# ----------------------------------------------------------------- resample
+def test_resample_golden(golden):
+    g = golden("resample")
+    shape = tuple(g["out_shape"])
+    for T, o8, of in zip(g["T"], g["out8"], g["outf"]):
+        assert same(tb.resample(g["src8"], shape, T), o8)
+        assert same(tb.resample(g["srcf"], shape, T), of)
+
+
+@pytest.mark.parametrize("shape", [(91, 109, 91), (17, 9, 5), (1, 8, 8), (64, 64, 64)])
+def test_resample_vs_oracle(orc, shape):
+    rng = np.random.default_rng(11)
+    src = (rng.random(shape) * 256).astype(np.uint8)
+    srcf = rng.random(shape).astype(np.float32)
+    for k in range(3):
+        p = ph.random_affine(rng, rot_deg=12, trans_vox=4)
+        T = orc.affine_to_matrix(p, shape, (1, 1, 1), shape, (1, 1, 1))
+        assert same(tb.resample(src, shape, T), orc.resample(src, shape, T))
+        assert same(tb.resample(srcf, shape, T), orc.resample(srcf, shape, T))
+
+
+def test_resample_device_tensors(orc):
+    import torch
+
+    rng = np.random.default_rng(3)
+    src = (rng.random((40, 37, 33)) * 256).astype(np.uint8)
+    p = ph.random_affine(rng)
+    T = orc.affine_to_matrix(p, src.shape, (1, 1, 1), src.shape, (1, 1, 1))
+    d = torch.from_numpy(src).cuda()
+    out = tb.resample(d, src.shape, T)
+    torch.cuda.synchronize()
+    assert same(out.cpu().numpy(), orc.resample(src, src.shape, T))
+
+
+# ----------------------------------------------------------------- affine costs
+def test_affine_costs_golden(golden):
+    g = golden("affine_costs")
+    f, m = g["fixed"], g["moving"]
+    cost, hist = tb.mi_cost(f, m, g["T"], return_hist=True)
+    for k in range(len(g["T"])):
+        assert same(hist[k], g["hist"][k])
+        assert cost[k] == pytest.approx(g["mi"][k], rel=1e-12)
+    assert np.array_equal(tb.corr_cost(f, m, g["T"]), g["corr"])  # exact moments: bit-exact
+    assert np.array_equal(tb.corr_cost(m, f, g["T"]), g["corr_swap"])
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 64), (91, 109, 91)])
+def test_affine_costs_vs_oracle(orc, shape):
+    rng = np.random.default_rng(5)
+    t, mv, _ = ph.affine_pair(shape, rng=rng)
+    f8, m8 = ph.normalize_to_u8(t), ph.normalize_to_u8(mv)
+    Ts = np.array([orc.affine_to_matrix(ph.random_affine(rng, rot_deg=6, trans_vox=3), shape, (1, 1, 1), shape,
+                                        (1, 1, 1)) for _ in range(6)])
+    Ts[0] = np.array([1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0], np.float32)
+    cost, hist = tb.mi_cost(f8, m8, Ts, return_hist=True)
+    for k, T in enumerate(Ts):
+        h = orc.mi_hist(f8, m8, T)
+        assert same(hist[k], h)
+        assert cost[k] == pytest.approx(orc.mi_cost(f8, m8, T), rel=1e-12)
+    corr = tb.corr_cost(f8, m8, Ts)
+    for k, T in enumerate(Ts):
+        assert corr[k] == orc.corr_cost(f8, m8, T)
+
+
+def test_affine_costs_full_size_properties(orc):
+    """182x218x182 (the affine workload's grid): every voxel lands in exactly one bin,
+    counts and costs match the oracle, and a K-candidate batch equals K single calls."""
+    shape = (182, 218, 182)
+    rng = np.random.default_rng(ph.seed_for(2))
+    t, mv, p_true = ph.affine_pair(shape, rng=rng)
+    f8, m8 = ph.normalize_to_u8(t), ph.normalize_to_u8(mv)
+    Ts = np.array([orc.affine_to_matrix(ph.random_affine(rng, rot_deg=4, trans_vox=2), shape, (1, 1, 1), shape,
+                                        (1, 1, 1)) for _ in range(4)])
+    cost, hist = tb.mi_cost(f8, m8, Ts, return_hist=True)
+    assert (hist.sum(axis=1) == f8.size).all()
+    h0 = orc.mi_hist(f8, m8, Ts[0])
+    assert same(hist[0], h0)
+    single = np.array([tb.mi_cost(f8, m8, T[None])[0] for T in Ts])
+    assert np.array_equal(single, cost)  # batching does not change any cost
+    assert cost[0] == pytest.approx(orc.mi_cost_from_hist(h0, orc.histogram(f8)), rel=1e-12)
+    c = tb.corr_cost(f8, m8, Ts)
+    assert c[1] == orc.corr_cost(f8, m8, Ts[1])
+
+
+def test_corr_integer_shift_copy(orc):
+    rng = np.random.default_rng(9)
+    f = (rng.random((30, 31, 29)) * 256).astype(np.uint8)
+    m = (rng.random((33, 30, 27)) * 256).astype(np.uint8)
+    T = np.array([1, 0, 0, 0, 1, 0, 0, 0, 1, 2, -1, 3], np.float32)
+    assert tb.corr_cost(f, m, T[None])[0] == orc.corr_cost(f, m, T)
+    assert tb.corr_cost(m, f, T[None])[0] == orc.corr_cost(m, f, T)
+
+
+# ----------------------------------------------------------------- CDM passes
+@pytest.mark.parametrize("ci", range(4))
+def test_cdm_passes_golden(golden, ci):
+    g = golden("cdm_passes")
+    c = {k.split("_", 1)[1]: g[k] for k in g.files if k.startswith(f"c{ci}_")}
+    assert same(tb.compose_displacement(c["Is"], c["d"]), c["compose8"])
+    assert same(tb.compose_displacement(c["Isf"], c["d"]), c["composef"])
+    for gt in "rd":
+        nd, cost = tb.cdm_gradient(c["Is"], c["It"], gt)
+        assert same(nd, c[f"grad8_{gt}"])
+        assert np.float32(cost) == c[f"cost8_{gt}"]
+        nd, cost = tb.cdm_gradient(c["Isf"], c["Itf"], gt)
+        assert same(nd, c[f"gradf_{gt}"])
+        assert abs(np.float32(cost) - c[f"costf_{gt}"]) <= np.spacing(np.abs(c[f"costf_{gt}"]))
+    assert same(tb.cdm_poisson(c["d"]), c["poisson"])
+    assert np.float32(tb.cdm_max_length(c["d"])) == c["maxlen"]
+    assert same(tb.accumulate_displacement(c["cd"], c["d"]), c["accumulate"])
+    assert same(tb.cdm_smooth(c["d"], 0.4), c["smooth"])
+    assert same(tb.downsample(c["Is"]), c["down8"])
+    assert same(tb.downsample(c["Isf"]), c["downf"])
+    assert same(tb.upsample_field_x2(c["up_in"], c["Is"].shape), c["up"])
+
+
+@pytest.mark.parametrize("shape", [(46, 55, 46), (91, 109, 91)])
+def test_cdm_passes_vs_oracle(orc, shape):
+    rng = np.random.default_rng(21)
+    t, m, _ = ph.cdm_pair(shape, rng=rng)
+    t8, m8 = ph.normalize_to_u8(t), ph.normalize_to_u8(m)
+    d = ph.smooth_field(shape, rng, 4.0, 2.5)
+    cd = ph.smooth_field(shape, rng, 5.0, 1.5)
+    for It, Is in ((t8, m8), (t, m)):
+        Js = tb.compose_displacement(Is, d)
+        assert same(Js, orc.compose(Is, d))
+        nd, cost = tb.cdm_gradient(Js, It, "r")
+        ond, ocost = orc.cdm_gradient(Js, It, "r")
+        assert same(nd, ond)
+        assert abs(np.float32(cost) - np.float32(ocost)) <= np.spacing(np.float32(abs(ocost)))
+    p = tb.cdm_poisson(nd)
+    assert same(p, orc.cdm_poisson(nd))
+    assert np.float32(tb.cdm_max_length(p)) == np.float32(orc.cdm_max_len(p))
+    assert same(tb.accumulate_displacement(cd, p), orc.accumulate(cd, p))
+    assert same(tb.cdm_smooth(p, 0.2), orc.cdm_smooth(p, 0.2))
+
+
+# ----------------------------------------------------------------- CDM end to end
+def test_cdm_end_to_end_golden(golden):
+    g = golden("cdm_e2e")
+    d8, ok8 = tb.reg.cdm(g["It8"], g["Is8"])
+    assert ok8 == bool(g["ok8"]) and same(d8, g["d8"])
+    df, okf = tb.reg.cdm(g["Itf"], g["Isf"])
+    assert okf == bool(g["okf"])
+    assert same(df, g["df"])
+
+
+@pytest.mark.parametrize("shape,min_dim", [((40, 40, 40), 16), ((37, 45, 30), 8), ((64, 64, 64), 16)])
+def test_cdm_end_to_end_vs_oracle(orc, shape, min_dim):
+    rng = np.random.default_rng(31)
+    t, m, _ = ph.cdm_pair(shape, rng=rng)
+    t8, m8 = ph.normalize_to_u8(t), ph.normalize_to_u8(m)
+    for It, Is in ((t8, m8), (t, m)):
+        d, ok = tb.reg.cdm(It, Is, tb.reg.cdm_param(min_dimension=min_dim))
+        od, ook, _ = orc.cdm(It, Is, min_dimension=min_dim)
+        assert ok == ook
+        assert same(d, od), float(np.abs(d - od).max())
+
+
+def test_cdm_zero_image_fails(orc):
+    z = np.zeros((20, 20, 20), np.uint8)
+    d, ok = tb.reg.cdm(z, z)
+    od, ook, _ = orc.cdm(z, z)
+    assert ok is False and ook is False

@@ -1,0 +1,264 @@
+"""tipl_b200 -- the TIPL registration hot path on B200 (sm_100a).
+
+Python mirror of the reference's calls for this path, over the C ABI of
+libregb200.so (include/regb200.h).  Names and argument meaning follow the
+reference:
+
+=============================  ===================================================
+reference                      here
+=============================  ===================================================
+tipl::reg::linear              ``reg.linear(from_, from_vs, to, to_vs, arg, ...)``
+tipl::reg::cdm_common          ``reg.cdm(It, Is, param)``
+tipl::resample                 ``resample(src, out_shape, T)``
+tipl::compose_displacement     ``compose_displacement(src, dis)``
+tipl::accumulate_displacement  ``accumulate_displacement(dis, new_dis)``
+mutual_information / corr      ``mi_cost`` / ``corr_cost`` (K transforms at once)
+transformation_matrix(...)     ``affine_to_matrix(param, ...)``
+=============================  ===================================================
+
+Arrays are numpy arrays shaped (z, y, x) (x-fastest memory, the reference's
+layout) -- host memory, staged by the library -- or CUDA torch tensors of the same
+shape, used in place on the device.  Displacement fields are (z, y, x, 3) float32
+with components (dx, dy, dz).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import CdmParam, Field, LinearParam, RegbError, Volume  # noqa: F401
+
+__all__ = ["affine_to_matrix", "affine_to_matrix_f64", "matrix_inverse", "resample", "mi_cost", "corr_cost",
+           "compose_displacement", "accumulate_displacement", "downsample", "upsample_field_x2", "cdm_gradient",
+           "cdm_poisson", "cdm_max_length", "cdm_smooth", "reg", "RegbError", "version"]
+
+
+def version() -> str:
+    return _lib.lib().regb_version().decode()
+
+
+def _is_dev(a) -> bool:
+    return hasattr(a, "is_cuda") and a.is_cuda
+
+
+def _dims(shape):
+    z, y, x = shape[:3]
+    arr = (C.c_int * 3)(int(x), int(y), int(z))
+    return arr
+
+
+def _dtype_code(a) -> int:
+    name = str(a.dtype)
+    if name in ("uint8", "torch.uint8"):
+        return _lib.U8
+    if name in ("float32", "torch.float32"):
+        return _lib.F32
+    raise TypeError(f"unsupported dtype {a.dtype}")
+
+
+def _vol(a) -> Volume:
+    if _is_dev(a):
+        assert a.is_contiguous()
+        return Volume(a.data_ptr(), _dims(a.shape), _dtype_code(a), _lib.DEVICE)
+    assert a.flags["C_CONTIGUOUS"]
+    return Volume(a.ctypes.data, _dims(a.shape), _dtype_code(a), _lib.HOST)
+
+
+def _field(a) -> Field:
+    if _is_dev(a):
+        assert a.is_contiguous() and a.shape[-1] == 3
+        return Field(a.data_ptr(), _dims(a.shape), _lib.DEVICE)
+    assert a.flags["C_CONTIGUOUS"] and a.dtype == np.float32 and a.shape[-1] == 3
+    return Field(a.ctypes.data, _dims(a.shape), _lib.HOST)
+
+
+def _like(a, shape, dtype=None):
+    if _is_dev(a):
+        import torch
+
+        return torch.zeros(tuple(shape), dtype=dtype or a.dtype, device=a.device)
+    return np.zeros(tuple(shape), dtype=dtype or a.dtype)
+
+
+def _host(a, dtype):
+    if _is_dev(a):
+        return a
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+
+
+# ---------------------------------------------------------------- transforms
+def affine_to_matrix(param, from_shape, from_vs, to_shape, to_vs) -> np.ndarray:
+    """transformation_matrix(affine_param, from, from_vs, to, to_vs) as 12 floats."""
+    p = np.ascontiguousarray(param, np.float32)
+    T = np.zeros(12, np.float32)
+    fd = np.array(list(_dims(from_shape)), np.int32)
+    td = np.array(list(_dims(to_shape)), np.int32)
+    _lib.check(_lib.lib().regb_affine_to_matrix(_fptr(p), _fptr(fd), _fptr(np.asarray(from_vs, np.float32)),
+                                                _fptr(td), _fptr(np.asarray(to_vs, np.float32)), _fptr(T)))
+    return T
+
+
+def affine_to_matrix_f64(param, from_shape, from_vs, to_shape, to_vs) -> np.ndarray:
+    p = np.ascontiguousarray(param, np.float64)
+    T = np.zeros(12, np.float64)
+    fd = np.array(list(_dims(from_shape)), np.int32)
+    td = np.array(list(_dims(to_shape)), np.int32)
+    _lib.check(_lib.lib().regb_affine_to_matrix_f64(_fptr(p), _fptr(fd), _fptr(np.asarray(from_vs, np.float64)),
+                                                    _fptr(td), _fptr(np.asarray(to_vs, np.float64)), _fptr(T)))
+    return T
+
+
+def matrix_inverse(T) -> np.ndarray:
+    M = np.ascontiguousarray(T, np.float32).copy()
+    _lib.check(_lib.lib().regb_matrix_inverse(_fptr(M)), allow=(_lib.REGB_OK, _lib.REGB_FALSE))
+    return M
+
+
+# ---------------------------------------------------------------- resample / costs
+def resample(src, out_shape, T, allow_shift_copy=True, out=None, stream=None):
+    """tipl::resample<linear>(src, out_shape, T)."""
+    out = _like(src, out_shape) if out is None else out
+    Tm = np.ascontiguousarray(T, np.float32)
+    _lib.check(_lib.lib().regb_resample(C.byref(_vol(src)), C.byref(_vol(out)), _fptr(Tm), int(allow_shift_copy),
+                                        _stream(stream)))
+    return out
+
+
+def mi_cost(fixed, moving, Ts, return_hist=False, stream=None):
+    """-MI of the 256x256 joint histogram for each of K transforms (reference MI functor)."""
+    Tm = np.ascontiguousarray(Ts, np.float32).reshape(-1, 12)
+    K = Tm.shape[0]
+    cost = np.zeros(K, np.float64)
+    hist = np.zeros((K, 65536), np.int32) if return_hist else None
+    _lib.check(_lib.lib().regb_mi_cost(C.byref(_vol(fixed)), C.byref(_vol(moving)), _fptr(Tm), K, _fptr(cost),
+                                       _fptr(hist) if hist is not None else None, _stream(stream)))
+    return (cost, hist) if return_hist else cost
+
+
+def corr_cost(fixed, moving, Ts, stream=None):
+    """1 - r^2 for each of K transforms (reference correlation functor)."""
+    Tm = np.ascontiguousarray(Ts, np.float32).reshape(-1, 12)
+    K = Tm.shape[0]
+    cost = np.zeros(K, np.float64)
+    _lib.check(_lib.lib().regb_corr_cost(C.byref(_vol(fixed)), C.byref(_vol(moving)), _fptr(Tm), K, _fptr(cost),
+                                         _stream(stream)))
+    return cost
+
+
+# ---------------------------------------------------------------- displacement algebra / CDM passes
+def compose_displacement(src, dis, stream=None):
+    out = _like(src, src.shape)
+    _lib.check(_lib.lib().regb_compose_displacement(C.byref(_vol(src)), C.byref(_field(_host(dis, np.float32))),
+                                                    C.byref(_vol(out)), _stream(stream)))
+    return out
+
+
+def accumulate_displacement(dis, new_dis, stream=None):
+    """Returns dis composed with new_dis (the reference updates new_dis in place)."""
+    nd = new_dis.clone() if _is_dev(new_dis) else np.array(new_dis, np.float32, copy=True)
+    _lib.check(_lib.lib().regb_accumulate_displacement(C.byref(_field(_host(dis, np.float32))), C.byref(_field(nd)),
+                                                       _stream(stream)))
+    return nd
+
+
+def downsample(img, stream=None):
+    z, y, x = img.shape
+    out = _like(img, ((z + 1) // 2, (y + 1) // 2, (x + 1) // 2))
+    _lib.check(_lib.lib().regb_downsample(C.byref(_vol(img)), C.byref(_vol(out)), _stream(stream)))
+    return out
+
+
+def upsample_field_x2(d, out_shape, stream=None):
+    out = _like(d, tuple(out_shape) + (3,), dtype=None)
+    _lib.check(_lib.lib().regb_upsample_field_x2(C.byref(_field(_host(d, np.float32))), C.byref(_field(out)),
+                                                 _stream(stream)))
+    return out
+
+
+def cdm_gradient(Js, It, gradient_type="r", stream=None):
+    nd = _like(Js, tuple(Js.shape) + (3,), dtype=_f32_like(Js))
+    c = C.c_float(0)
+    _lib.check(_lib.lib().regb_cdm_gradient(C.byref(_vol(Js)), C.byref(_vol(It)), C.byref(_field(nd)),
+                                            ord(gradient_type), C.byref(c), _stream(stream)))
+    return nd, float(c.value)
+
+
+def _f32_like(a):
+    if _is_dev(a):
+        import torch
+
+        return torch.float32
+    return np.float32
+
+
+def cdm_poisson(d, stream=None):
+    nd = d.clone() if _is_dev(d) else np.array(d, np.float32, copy=True)
+    _lib.check(_lib.lib().regb_cdm_poisson(C.byref(_field(nd)), _stream(stream)))
+    return nd
+
+
+def cdm_max_length(d, stream=None) -> float:
+    c = C.c_float(0)
+    _lib.check(_lib.lib().regb_cdm_max_length(C.byref(_field(_host(d, np.float32))), C.byref(c), _stream(stream)))
+    return float(c.value)
+
+
+def cdm_smooth(d, smoothing, out=None, stream=None):
+    src = _host(d, np.float32)
+    dd = _like(src, src.shape) if out is None else out
+    _lib.check(_lib.lib().regb_cdm_smooth(C.byref(_field(src)), C.byref(_field(dd)), float(smoothing),
+                                          _stream(stream)))
+    return dd
+
+
+# ---------------------------------------------------------------- whole registrations
+class reg:
+    """tipl::reg entry points."""
+
+    AFFINE, RIGID_BODY, TRANSLOCATION = 15, 3, 1
+    CORR, MI = 0, 1
+
+    @staticmethod
+    def linear_param(reg_type=15, cost_type=1, bound=0, search_count=16, absolute_bound=1) -> LinearParam:
+        return LinearParam(reg_type, cost_type, bound, search_count, absolute_bound)
+
+    @staticmethod
+    def cdm_param(resolution=2.0, speed=0.3, smoothing=0.05, min_dimension=16, gradient_type="r") -> CdmParam:
+        return CdmParam(resolution, speed, smoothing, min_dimension, ord(gradient_type))
+
+    @staticmethod
+    def linear(from_, from_vs, to, to_vs, arg=None, param: LinearParam | None = None, terminated=None):
+        """tipl::reg::linear: returns (cost, arg[12], cost_evaluations)."""
+        a = (np.array([0, 0, 0, 0, 0, 0, 1, 1, 1, 0, 0, 0], np.float32) if arg is None
+             else np.array(arg, np.float32, copy=True))
+        p = param or reg.linear_param()
+        cost = C.c_float(0)
+        evals = C.c_longlong(0)
+        term = None if terminated is None else C.cast(terminated, C.c_void_p)
+        st = _lib.lib().regb_linear(C.byref(_vol(from_)), _fptr(np.asarray(from_vs, np.float32)), C.byref(_vol(to)),
+                                    _fptr(np.asarray(to_vs, np.float32)), _fptr(a), C.byref(p), term,
+                                    C.byref(cost), C.byref(evals))
+        _lib.check(st, allow=(_lib.REGB_OK, _lib.REGB_CANCELLED))
+        return float(cost.value), a, int(evals.value)
+
+    @staticmethod
+    def cdm(It, Is, param: CdmParam | None = None, terminated=None, out=None):
+        """tipl::reg::cdm_common: returns (field, ok)."""
+        d = _like(It, tuple(It.shape) + (3,), dtype=_f32_like(It)) if out is None else out
+        p = param or reg.cdm_param()
+        term = None if terminated is None else C.cast(terminated, C.c_void_p)
+        st = _lib.lib().regb_cdm(C.byref(_vol(It)), C.byref(_vol(Is)), C.byref(_field(d)), C.byref(p), term)
+        _lib.check(st, allow=(_lib.REGB_OK, _lib.REGB_FALSE, _lib.REGB_CANCELLED))
+        return d, st != _lib.REGB_FALSE

@@ -1,0 +1,119 @@
+"""ctypes binding of libregb200.so (the C ABI in include/regb200.h).
+
+The library is the product: there is no fallback.  Loading fails loudly when the
+.so is missing (build it with ``python -m tipl_b200.build``)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libregb200.so")
+
+REGB_OK = 0
+REGB_FALSE = 1
+REGB_ERR_ARG = -1
+REGB_ERR_CUDA = -2
+REGB_ERR_NOMEM = -3
+REGB_CANCELLED = -4
+REGB_ERR_NOTFOUND = -5
+REGB_PENDING = -6
+REGB_ERR_BUDGET = -7
+
+U8, F32, U16, BF16 = 0, 1, 2, 3
+HOST, DEVICE = 0, 1
+
+
+class Volume(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("dim", C.c_int * 3), ("dtype", C.c_int), ("location", C.c_int)]
+
+
+class Field(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("dim", C.c_int * 3), ("location", C.c_int)]
+
+
+class LinearParam(C.Structure):
+    _fields_ = [("reg_type", C.c_int), ("cost_type", C.c_int), ("bound", C.c_int), ("search_count", C.c_uint),
+                ("absolute_bound", C.c_int)]
+
+
+class CdmParam(C.Structure):
+    _fields_ = [("resolution", C.c_float), ("speed", C.c_float), ("smoothing", C.c_float),
+                ("min_dimension", C.c_uint), ("gradient_type", C.c_int)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("launches", C.c_longlong), ("mi_launches", C.c_longlong), ("mi_tasks", C.c_longlong),
+                ("mi_voxels", C.c_double), ("mi_bytes", C.c_double), ("mi_ms", C.c_double),
+                ("corr_launches", C.c_longlong), ("corr_tasks", C.c_longlong), ("corr_voxels", C.c_double),
+                ("corr_bytes", C.c_double), ("corr_ms", C.c_double)]
+
+
+class RegbError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        super().__init__(f"regb status {status}: {what}")
+        self.status = status
+
+
+_lib = None
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "regb_version": (C.c_char_p, []),
+    "regb_last_error": (C.c_char_p, []),
+    "regb_device_info": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_size_t),
+                                   C.POINTER(C.c_size_t)]),
+    "regb_release": (C.c_int, []),
+    "regb_stats_reset": (C.c_int, [C.c_int]),
+    "regb_stats_get": (C.c_int, [C.POINTER(Stats)]),
+    "regb_linear_param_default": (None, [C.POINTER(LinearParam)]),
+    "regb_cdm_param_default": (None, [C.POINTER(CdmParam)]),
+    "regb_affine_to_matrix": (C.c_int, [C.c_void_p] * 6),
+    "regb_affine_to_matrix_f64": (C.c_int, [C.c_void_p] * 6),
+    "regb_matrix_inverse": (C.c_int, [C.c_void_p]),
+    "regb_resample": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p]),
+    "regb_mi_cost": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p,
+                               C.c_void_p, C.c_void_p]),
+    "regb_corr_cost": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p,
+                                 C.c_void_p]),
+    "regb_compose_displacement": (C.c_int, [C.POINTER(Volume), C.POINTER(Field), C.POINTER(Volume), C.c_void_p]),
+    "regb_accumulate_displacement": (C.c_int, [C.POINTER(Field), C.POINTER(Field), C.c_void_p]),
+    "regb_downsample": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p]),
+    "regb_upsample_field_x2": (C.c_int, [C.POINTER(Field), C.POINTER(Field), C.c_void_p]),
+    "regb_cdm_gradient": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.POINTER(Field), C.c_int,
+                                    C.POINTER(C.c_float), C.c_void_p]),
+    "regb_cdm_poisson": (C.c_int, [C.POINTER(Field), C.c_void_p]),
+    "regb_cdm_max_length": (C.c_int, [C.POINTER(Field), C.POINTER(C.c_float), C.c_void_p]),
+    "regb_cdm_smooth": (C.c_int, [C.POINTER(Field), C.POINTER(Field), C.c_float, C.c_void_p]),
+    "regb_cdm": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.POINTER(Field), C.POINTER(CdmParam),
+                           C.c_void_p]),
+    "regb_linear": (C.c_int, [C.POINTER(Volume), C.c_void_p, C.POINTER(Volume), C.c_void_p, C.c_void_p,
+                              C.POINTER(LinearParam), C.c_void_p, C.POINTER(C.c_float),
+                              C.POINTER(C.c_longlong)]),
+}
+
+
+def lib():
+    """The loaded library (raises when it is absent)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m tipl_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def declared_symbols():
+    return sorted(_SIGS)
+
+
+def check(status: int, allow=(REGB_OK,)) -> int:
+    if status in allow:
+        return status
+    msg = lib().regb_last_error()
+    raise RegbError(status, msg.decode() if msg else "")

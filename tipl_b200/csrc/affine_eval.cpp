@@ -1,0 +1,141 @@
+#include "affine_eval.h"
+#include "stats.h"
+#include <algorithm>
+#include <cstring>
+
+namespace regb {
+
+void TaskScratch::ensure(int k, bool need_hist, cudaStream_t st)
+{
+    if (k <= cap && (!need_hist || hist.n >= (size_t)cap * 65536))
+        return;
+    const int c = std::max(k, std::max(16, cap * 2));
+    if (need_hist) {
+        hist.alloc((size_t)c * 65536, st);
+        hist.zero();
+    }
+    moments.alloc((size_t)c * 3, st);
+    moments.zero();
+    ticket.alloc((size_t)c, st);
+    ticket.zero();
+    cost.alloc((size_t)c, st);
+    tasks.alloc((size_t)c, st);
+    h_tasks.alloc((size_t)c);
+    h_cost.alloc((size_t)c);
+    cap = c;
+}
+
+void set_task_chunks(AffineTask& t, int cost_type)
+{
+    const long long n = t.fd.n();
+    long long chunk;
+    if (cost_type == REGB_COST_MI) {
+        // 16-bit per-block counters: at most 65535 voxels per block.
+        chunk = (n + 147) / 148;
+        chunk = std::max<long long>(chunk, 32768);
+        chunk = std::min<long long>(chunk, 65535);
+    } else
+        chunk = 32768;
+    t.chunk = (int)chunk;
+    t.nchunk = (int)std::max<long long>(1, (n + chunk - 1) / chunk);
+}
+
+void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, double* out)
+{
+    int max_chunks = 1;
+    for (int k = 0; k < K; ++k) {
+        AffineTask& t = s.h_tasks.p[k];
+        t.ticket = s.ticket.p + k;
+        t.cost = s.cost.p + k;
+        t.moments = s.moments.p + 3 * k;
+        t.hist = (cost_type == REGB_COST_MI) ? s.hist.p + (size_t)k * 65536 : nullptr;
+        max_chunks = std::max(max_chunks, t.nchunk);
+    }
+    REGB_CK(cudaMemcpyAsync(s.tasks.p, s.h_tasks.p, sizeof(AffineTask) * K, cudaMemcpyHostToDevice, st));
+    double vox = 0.0, bytes = 0.0;
+    for (int k = 0; k < K; ++k) {
+        const AffineTask& t = s.h_tasks.p[k];
+        vox += (double)t.fd.n();
+        // algorithmic bytes of one evaluation: the fixed grid and the sampled volume
+        // once each, plus the 256x256 int32 histogram written and read (MI)
+        bytes += (double)t.fd.n() + (double)t.md.n() + (cost_type == REGB_COST_MI ? 524288.0 : 0.0);
+    }
+    KernelTimer tm;
+    tm.begin(st, cost_type == REGB_COST_MI ? 0 : 1);
+    if (cost_type == REGB_COST_MI)
+        REGB_CK(launch_mi(s.tasks.p, K, max_chunks, st));
+    else
+        REGB_CK(launch_corr(s.tasks.p, K, max_chunks, st));
+    tm.end(st, K, vox, bytes);
+    count_launch();
+    REGB_CK(cudaMemcpyAsync(s.h_cost.p, s.cost.p, sizeof(double) * K, cudaMemcpyDeviceToHost, st));
+    REGB_CK(cudaStreamSynchronize(st));
+    std::memcpy(out, s.h_cost.p, sizeof(double) * K);
+}
+
+AffineEvaluator::AffineEvaluator(const std::vector<Pair>& levels, int cost_type, cudaStream_t st)
+    : cost_type_(cost_type), st_(st)
+{
+    lv_.resize(levels.size());
+    PinBuf<unsigned long long> h(2);
+    for (size_t i = 0; i < levels.size(); ++i) {
+        Lvl& L = lv_[i];
+        L.p = levels[i];
+        const uint8_t* grid = L.p.from;
+        long long n = L.p.fd.n();
+        if (cost_type == REGB_COST_CORR && L.p.fd.n() > L.p.td.n()) {  // reg/linear.hpp:28-33
+            L.swap = true;
+            grid = L.p.to;
+            n = L.p.td.n();
+        }
+        L.row_hist.alloc(256, st);
+        L.sums.alloc(2, st);
+        REGB_CK(launch_fixed_stats(grid, n, L.row_hist.p, L.sums.p, st));
+        REGB_CK(cudaMemcpyAsync(h.p, L.sums.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        REGB_CK(cudaStreamSynchronize(st));
+        L.sx = (long long)h.p[0];
+        L.sxx = (long long)h.p[1];
+    }
+}
+
+void AffineEvaluator::make_task(int level, const float* T, AffineTask& t) const
+{
+    const Lvl& L = lv_[level];
+    std::memset(&t, 0, sizeof(t));
+    float M[12];
+    std::memcpy(M, T, sizeof(M));
+    if (L.swap) {
+        matrix_inverse(M);  // a singular matrix is left unchanged, as the reference does
+        t.fixed = L.p.to;
+        t.fd = L.p.td;
+        t.moving = L.p.from;
+        t.md = L.p.fd;
+    } else {
+        t.fixed = L.p.from;
+        t.fd = L.p.fd;
+        t.moving = L.p.to;
+        t.md = L.p.td;
+    }
+    std::memcpy(t.T, M, sizeof(M));
+    t.mode = 0;
+    if (cost_type_ == REGB_COST_CORR && integer_shift(M, t.shift))
+        t.mode = 1;  // the CPU resample's integer-shift copy
+    t.row_hist = L.row_hist.p;
+    t.sx = L.sx;
+    t.sxx = L.sxx;
+    set_task_chunks(t, cost_type_);
+}
+
+std::vector<double> AffineEvaluator::eval(int level, const float* T, int K)
+{
+    std::vector<double> out(K);
+    if (K == 0)
+        return out;
+    s_.ensure(K, cost_type_ == REGB_COST_MI, st_);
+    for (int k = 0; k < K; ++k)
+        make_task(level, T + 12 * k, s_.h_tasks.p[k]);
+    run_affine_tasks(s_, K, cost_type_, st_, out.data());
+    return out;
+}
+
+}  // namespace regb

@@ -1,0 +1,60 @@
+// Batched affine cost evaluation: K candidate transforms of one image pair (at one
+// pyramid level) in a single launch.  Also the task-level entry used by the
+// serving engine to put candidates of many jobs into one launch.
+#pragma once
+#include <vector>
+#include "host.h"
+
+namespace regb {
+
+// Device scratch for up to `cap` tasks: MI histograms, correlation moments,
+// completion tickets, costs.  Kept zeroed between launches by the kernels.
+struct TaskScratch {
+    int cap = 0;
+    DevBuf<uint32_t> hist;
+    DevBuf<unsigned long long> moments;
+    DevBuf<unsigned int> ticket;
+    DevBuf<double> cost;
+    DevBuf<AffineTask> tasks;
+    PinBuf<AffineTask> h_tasks;
+    PinBuf<double> h_cost;
+    void ensure(int k, bool need_hist, cudaStream_t st);
+};
+
+// Fills the scratch pointers of h_tasks[0..K), launches the MI or correlation
+// kernel for all of them, and copies the costs back (synchronises st).
+void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, double* out);
+
+// Chunking of one task over its fixed-grid voxels.
+void set_task_chunks(AffineTask& t, int cost_type);
+
+class AffineEvaluator {
+public:
+    struct Pair {
+        const uint8_t* from;
+        Dim3 fd;
+        const uint8_t* to;
+        Dim3 td;
+    };
+    AffineEvaluator(const std::vector<Pair>& levels, int cost_type, cudaStream_t st);
+    // T: K transforms (12 floats each) mapping the level's from-grid to its to-volume.
+    std::vector<double> eval(int level, const float* T, int K);
+    // Builds the task of one candidate (used by the engine to batch across jobs).
+    void make_task(int level, const float* T, AffineTask& out) const;
+    int cost_type() const { return cost_type_; }
+
+private:
+    struct Lvl {
+        Pair p;
+        bool swap = false;  // correlation: the to-volume is the smaller one and becomes the grid
+        DevBuf<int32_t> row_hist;
+        DevBuf<unsigned long long> sums;
+        long long sx = 0, sxx = 0;
+    };
+    std::vector<Lvl> lv_;
+    int cost_type_;
+    cudaStream_t st_;
+    TaskScratch s_;
+};
+
+}  // namespace regb

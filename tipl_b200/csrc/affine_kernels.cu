@@ -1,0 +1,347 @@
+// Affine hot path: trilinear resample, the MI joint histogram with its MI
+// reduction, and the correlation moments with the correlation cost.
+//
+// Reference behaviour followed:
+//   resample                      numerical/resampling.hpp:1239-1298
+//   get_mutual_info               reg/linear.hpp:138-169
+//   get_mutual_info_mean          reg/linear.hpp:87-134
+//   correlation cost              reg/linear.hpp:23-78, numerical/statistics.hpp:569-625
+//
+// Batching: one launch evaluates many (job, candidate transform) tasks.  Each
+// task is split into voxel chunks; gridDim.y indexes tasks and gridDim.x chunks.
+// The last block of a task (ticket counter) reduces that task's counts to its
+// cost and clears the task's scratch, so the next launch finds it zeroed.
+#include <atomic>
+#include "common.cuh"
+#include "stats.h"
+#include "kernels.h"
+
+namespace regb {
+
+// ---------------------------------------------------------------- resample
+template <typename T>
+__global__ void __launch_bounds__(256) resample_kernel(const T* __restrict__ from, Dim3 fd, T* __restrict__ to,
+                                                       Dim3 td, Xform X)
+{
+    const long long n = td.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        unflat((int)i, td, x, y, z);
+        float px, py, pz;
+        apply_xform(X.m, (float)x, (float)y, (float)z, px, py, pz);
+        Cell c;
+        T v = T(0);
+        if (trilinear_cell(fd, px, py, pz, c))
+            v = assign_pix<T>(cell_sum(from, fd, c));
+        to[i] = v;
+    }
+}
+
+// The CPU resample's integer-shift fast path (numerical/resampling.hpp:1243-1262):
+// a copy of the overlap, zero elsewhere.
+template <typename T>
+__global__ void __launch_bounds__(256) shift_copy_kernel(const T* __restrict__ from, Dim3 fd, T* __restrict__ to,
+                                                         Dim3 td, int sx, int sy, int sz)
+{
+    const long long n = td.n();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        unflat((int)i, td, x, y, z);
+        int fx = x + sx, fy = y + sy, fz = z + sz;
+        T v = T(0);
+        if (fx >= 0 && fy >= 0 && fz >= 0 && fx < fd.w && fy < fd.h && fz < fd.d)
+            v = from[(fz * fd.h + fy) * fd.w + fx];
+        to[i] = v;
+    }
+}
+
+template <typename T>
+cudaError_t launch_resample(const T* from, Dim3 fd, T* to, Dim3 td, const float* Tm, const int* shift,
+                            cudaStream_t st)
+{
+    const long long n = td.n();
+    if (n == 0)
+        return cudaSuccess;
+    int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    if (shift)
+        shift_copy_kernel<T><<<blocks, 256, 0, st>>>(from, fd, to, td, shift[0], shift[1], shift[2]);
+    else {
+        Xform X;
+        for (int k = 0; k < 12; ++k)
+            X.m[k] = Tm[k];
+        resample_kernel<T><<<blocks, 256, 0, st>>>(from, fd, to, td, X);
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+template cudaError_t launch_resample<uint8_t>(const uint8_t*, Dim3, uint8_t*, Dim3, const float*, const int*,
+                                              cudaStream_t);
+template cudaError_t launch_resample<float>(const float*, Dim3, float*, Dim3, const float*, const int*,
+                                            cudaStream_t);
+
+// ---------------------------------------------------------------- MI
+// Per-block private histogram: 65536 bins packed two per 32-bit word as 16-bit
+// counters (128 KB of shared memory).  A block never counts more than
+// kMiChunkMax voxels, so no 16-bit counter can overflow.  Bin 0 (template 0,
+// moving sample 0 -- the background) is not counted at all: its count is the
+// voxel total minus every other bin, recovered in the reduction.
+constexpr int kMiThreads = 1024;
+constexpr int kMiSmemWords = 32768;
+
+__device__ __forceinline__ void mi_count(uint32_t* sh, uint32_t bin)
+{
+    if (bin != 0u)
+        atomicAdd(sh + (bin >> 1), 1u << ((bin & 1u) << 4));
+}
+
+// Reduction of a complete 256x256 histogram to the reference's MI cost
+// (reg/linear.hpp:87-104): column sums, then sum over non-zero bins of
+// n*ln(n/row/col) in double, divided by 65536 and negated.
+__device__ void mi_reduce_and_clear(uint32_t* __restrict__ hist, const int32_t* __restrict__ row_hist,
+                                    long long nvox, double* __restrict__ cost, uint32_t* smem)
+{
+    uint32_t* col = smem;                 // 256
+    unsigned long long* tot = (unsigned long long*)(smem + 256);  // 1
+    double* red = (double*)(smem + 512);  // 32
+    const int t = threadIdx.x;
+    if (t < 256)
+        col[t] = 0u;
+    if (t == 0)
+        *tot = 0ull;
+    __syncthreads();
+    // column partial sums: thread t covers column (t & 255), rows [64*(t>>8), +64)
+    {
+        const int j = t & 255, r0 = (t >> 8) * 64;
+        uint32_t s = 0;
+        for (int r = r0; r < r0 + 64; ++r)
+            s += __ldcg(hist + r * 256 + j);
+        atomicAdd(col + j, s);
+        unsigned long long ss = s;
+        ss = warp_sum(ss);
+        if ((t & 31) == 0)
+            atomicAdd(tot, ss);
+    }
+    __syncthreads();
+    const uint32_t n00 = (uint32_t)(nvox - (long long)*tot);  // the uncounted background bin
+    __syncthreads();
+    if (t == 0)
+        col[0] += n00;
+    __syncthreads();
+    double acc = 0.0;
+    for (int b = t; b < 65536; b += blockDim.x) {
+        uint32_t n = (b == 0) ? n00 : __ldcg(hist + b);
+        if (n) {
+            double mu = (double)n;
+            acc += mu * log(mu / (double)row_hist[b >> 8] / (double)col[b & 255]);
+        }
+    }
+    acc = block_sum(acc, red);
+    if (t == 0)
+        *cost = -(acc / 65536.0);
+    for (int b = t; b < 65536; b += blockDim.x)
+        hist[b] = 0u;
+}
+
+__global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __restrict__ tasks)
+{
+    extern __shared__ uint32_t sh[];
+    const AffineTask& tk = tasks[blockIdx.y];
+    const int chunk = blockIdx.x;
+    if (chunk >= tk.nchunk)
+        return;
+    for (int i = threadIdx.x * 4; i < kMiSmemWords; i += blockDim.x * 4)
+        *reinterpret_cast<uint4*>(sh + i) = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    const Dim3 fd = tk.fd, md = tk.md;
+    const long long n = fd.n();
+    const long long v0 = (long long)chunk * tk.chunk;
+    const long long v1 = min(n, v0 + tk.chunk);
+    const uint8_t* __restrict__ fixed = tk.fixed;
+    const uint8_t* __restrict__ moving = tk.moving;
+    for (long long i = v0 + threadIdx.x; i < v1; i += blockDim.x) {
+        int x, y, z;
+        unflat((int)i, fd, x, y, z);
+        float px, py, pz;
+        apply_xform(tk.T, (float)x, (float)y, (float)z, px, py, pz);
+        Cell c;
+        uint32_t to8 = 0;
+        if (trilinear_cell(md, px, py, pz, c))
+            to8 = assign_pix<uint8_t>(cell_sum(moving, md, c));
+        mi_count(sh, ((uint32_t)__ldg(fixed + i) << 8) | to8);
+    }
+    __syncthreads();
+    // flush non-zero counters to the task's global histogram
+    uint32_t* __restrict__ gh = tk.hist;
+    for (int wi = threadIdx.x; wi < kMiSmemWords; wi += blockDim.x) {
+        uint32_t w = sh[wi];
+        if (w) {
+            if (w & 0xffffu)
+                atomicAdd(gh + 2 * wi, w & 0xffffu);
+            if (w >> 16)
+                atomicAdd(gh + 2 * wi + 1, w >> 16);
+        }
+    }
+    if (tk.keep)
+        return;
+    __threadfence();
+    __syncthreads();
+    __shared__ unsigned int last;
+    if (threadIdx.x == 0)
+        last = (atomicAdd(tk.ticket, 1u) == (unsigned)tk.nchunk - 1u);
+    __syncthreads();
+    if (!last)
+        return;
+    __threadfence();
+    mi_reduce_and_clear(gh, tk.row_hist, n, tk.cost, sh);
+    if (threadIdx.x == 0)
+        *tk.ticket = 0u;
+}
+
+cudaError_t launch_mi(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
+{
+    static std::atomic<unsigned long long> attr_set{0};  // one bit per device
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr_set.load() & bit)) {
+        e = cudaFuncSetAttribute(mi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMiSmemWords * 4);
+        if (e != cudaSuccess)
+            return e;
+        attr_set.fetch_or(bit);
+    }
+    dim3 grid(max_chunks, ntask);
+    mi_kernel<<<grid, kMiThreads, kMiSmemWords * 4, st>>>(d_tasks);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- correlation
+// Exact integer moments of the resampled moving volume y against the fixed grid
+// x: sum y, sum y^2, sum x*y (the template's sum x and sum x^2 are per job).  A
+// thread sums at most kCorrPerThread voxels in 32 bits (255^2 * 64 < 2^32).
+constexpr int kCorrThreads = 256;
+
+__global__ void __launch_bounds__(kCorrThreads) corr_kernel(const AffineTask* __restrict__ tasks)
+{
+    const AffineTask& tk = tasks[blockIdx.y];
+    const int chunk = blockIdx.x;
+    if (chunk >= tk.nchunk)
+        return;
+    const Dim3 fd = tk.fd, md = tk.md;
+    const long long n = fd.n();
+    const long long v0 = (long long)chunk * tk.chunk;
+    const long long v1 = min(n, v0 + tk.chunk);
+    const uint8_t* __restrict__ fixed = tk.fixed;
+    const uint8_t* __restrict__ moving = tk.moving;
+    uint32_t sy = 0, syy = 0, sxy = 0;
+    for (long long i = v0 + threadIdx.x; i < v1; i += blockDim.x) {
+        int x, y, z;
+        unflat((int)i, fd, x, y, z);
+        uint32_t v = 0;
+        if (tk.mode == 1) {
+            int fx = x + tk.shift[0], fy = y + tk.shift[1], fz = z + tk.shift[2];
+            if (fx >= 0 && fy >= 0 && fz >= 0 && fx < md.w && fy < md.h && fz < md.d)
+                v = __ldg(moving + (fz * md.h + fy) * md.w + fx);
+        } else {
+            float px, py, pz;
+            apply_xform(tk.T, (float)x, (float)y, (float)z, px, py, pz);
+            Cell c;
+            if (trilinear_cell(md, px, py, pz, c))
+                v = assign_pix<uint8_t>(cell_sum(moving, md, c));
+        }
+        uint32_t f = __ldg(fixed + i);
+        sy += v;
+        syy += v * v;
+        sxy += f * v;
+    }
+    __shared__ unsigned long long red[32];
+    unsigned long long a = block_sum<unsigned long long>(sy, red);
+    unsigned long long b = block_sum<unsigned long long>(syy, red);
+    unsigned long long c = block_sum<unsigned long long>(sxy, red);
+    if (threadIdx.x == 0) {
+        atomicAdd(tk.moments + 0, a);
+        atomicAdd(tk.moments + 1, b);
+        atomicAdd(tk.moments + 2, c);
+    }
+    __threadfence();
+    __syncthreads();
+    __shared__ unsigned int last;
+    if (threadIdx.x == 0)
+        last = (atomicAdd(tk.ticket, 1u) == (unsigned)tk.nchunk - 1u);
+    __syncthreads();
+    if (!last || threadIdx.x != 0)
+        return;
+    __threadfence();
+    // tipl::correlation with exact integer moments (numerical/statistics.hpp:569-580),
+    // then 1 - r^2 in float (reg/linear.hpp:34-35).
+    const unsigned long long Sy = __ldcg(tk.moments + 0), Syy = __ldcg(tk.moments + 1), Sxy = __ldcg(tk.moments + 2);
+    const double dn = (double)n;
+    const double mx = (double)tk.sx / dn, my = (double)Sy / dn;
+    const double vx = (double)tk.sxx / dn - mx * mx, vy = (double)Syy / dn - my * my;
+    const double sd1 = vx > 0.0 ? sqrt(vx) : 0.0, sd2 = vy > 0.0 ? sqrt(vy) : 0.0;
+    double r = 0.0;
+    if (!(sd1 == 0.0 || sd2 == 0.0))
+        r = ((double)Sxy / dn - mx * my) / sd1 / sd2;
+    const float cf = (float)r;
+    *tk.cost = (double)(1.0f - cf * cf);
+    tk.moments[0] = tk.moments[1] = tk.moments[2] = 0ull;
+    *tk.ticket = 0u;
+}
+
+cudaError_t launch_corr(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
+{
+    dim3 grid(max_chunks, ntask);
+    corr_kernel<<<grid, kCorrThreads, 0, st>>>(d_tasks);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- template statistics
+// Row histogram of the fixed volume (histogram(from, 0, 255, 256), which for uint8
+// is the value count) and its exact sums for the correlation cost.
+__global__ void fixed_stats_kernel(const uint8_t* __restrict__ f, long long n, int32_t* __restrict__ hist,
+                                   unsigned long long* __restrict__ sums)
+{
+    __shared__ uint32_t h[256];
+    __shared__ unsigned long long red[32];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        h[i] = 0;
+    __syncthreads();
+    unsigned long long s = 0, ss = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        uint32_t v = __ldg(f + i);
+        atomicAdd(h + v, 1u);
+        s += v;
+        ss += v * v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (h[i])
+            atomicAdd((unsigned int*)hist + i, h[i]);
+    unsigned long long a = block_sum(s, red);
+    unsigned long long b = block_sum(ss, red);
+    if (threadIdx.x == 0) {
+        atomicAdd(sums, a);
+        atomicAdd(sums + 1, b);
+    }
+}
+
+cudaError_t launch_fixed_stats(const uint8_t* f, long long n, int32_t* hist, unsigned long long* sums,
+                               cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(hist, 0, 256 * sizeof(int32_t), st);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(sums, 0, 2 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess)
+        return e;
+    int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 4);
+    if (blocks < 1)
+        blocks = 1;
+    fixed_stats_kernel<<<blocks, 256, 0, st>>>(f, n, hist, sums);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace regb

@@ -1,0 +1,558 @@
+// extern "C" entry points of libregb200.so (declared in include/regb200.h).
+// Every entry validates its views, stages host memory through device buffers when
+// a view lives on the host, and turns failures into regb_status codes.
+#include <cstring>
+#include <new>
+#include <string>
+#include "affine_eval.h"
+#include "cdm_level.h"
+#include "host.h"
+
+namespace regb {
+const std::string& last_error();
+}
+
+using namespace regb;
+
+namespace {
+
+const long long kMaxVoxels = (1LL << 31) - 1;
+
+void check_dims(const int* d, const char* what)
+{
+    if (d[0] <= 0 || d[1] <= 0 || d[2] <= 0)
+        throw Failure(REGB_ERR_ARG, std::string(what) + ": non-positive dimension");
+    if ((long long)d[0] * d[1] * d[2] > kMaxVoxels)
+        throw Failure(REGB_ERR_ARG, std::string(what) + ": more than 2^31-1 voxels");
+}
+
+void check_vol(const regb_volume* v, const char* what, bool u8_or_f32 = true)
+{
+    if (!v || !v->ptr)
+        throw Failure(REGB_ERR_ARG, std::string(what) + ": null volume");
+    check_dims(v->dim, what);
+    if (u8_or_f32 && v->dtype != REGB_U8 && v->dtype != REGB_F32)
+        throw Failure(REGB_ERR_ARG, std::string(what) + ": dtype must be U8 or F32");
+    if (v->location != REGB_HOST && v->location != REGB_DEVICE)
+        throw Failure(REGB_ERR_ARG, std::string(what) + ": bad location");
+}
+
+void check_field(const regb_field* f, const char* what)
+{
+    if (!f || !f->ptr)
+        throw Failure(REGB_ERR_ARG, std::string(what) + ": null field");
+    check_dims(f->dim, what);
+    if (f->location != REGB_HOST && f->location != REGB_DEVICE)
+        throw Failure(REGB_ERR_ARG, std::string(what) + ": bad location");
+}
+
+bool same_dims(const int* a, const int* b) { return a[0] == b[0] && a[1] == b[1] && a[2] == b[2]; }
+size_t nvox(const int* d) { return (size_t)d[0] * d[1] * d[2]; }
+
+// Device view of a volume or field; host data is staged through an owned buffer.
+struct Staged {
+    DevBuf<uint8_t> own;
+    void* d = nullptr;
+    size_t bytes = 0;
+    bool host = false;
+    void in(void* ptr, size_t b, int location, cudaStream_t st, bool copy)
+    {
+        bytes = b;
+        host = (location == REGB_HOST);
+        if (!host) {
+            d = ptr;
+            return;
+        }
+        own.alloc(b, st);
+        d = own.p;
+        if (copy)
+            REGB_CK(cudaMemcpyAsync(d, ptr, b, cudaMemcpyHostToDevice, st));
+    }
+    void out(void* ptr, cudaStream_t st)
+    {
+        if (host)
+            REGB_CK(cudaMemcpyAsync(ptr, d, bytes, cudaMemcpyDeviceToHost, st));
+    }
+};
+
+template <typename F>
+regb_status guarded(F&& f)
+{
+    try {
+        return f();
+    } catch (const Failure& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return REGB_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return REGB_ERR_ARG;
+    }
+}
+
+// A single-segment CDM view for the standalone passes.
+struct OneSeg {
+    DevBuf<CdmSeg> seg;
+    DevBuf<CdmCtl> ctl;
+    DevBuf<double> part;
+    CdmSeg h{};
+    CdmCtl c{};
+    OneSeg(const int* dim, cudaStream_t st)
+    {
+        h.w = dim[0];
+        h.h = dim[1];
+        h.d = dim[2];
+        h.nblk = cdm_blocks_for((long long)dim[0] * dim[1] * dim[2]);
+        part.alloc(h.nblk, st);
+        ctl.alloc(1, st);
+        seg.alloc(1, st);
+        h.cost_part = part.p;
+        h.ctl = ctl.p;
+        std::memset(&c, 0, sizeof(c));
+        c.max_iter = 200;
+    }
+    void upload(cudaStream_t st)
+    {
+        REGB_CK(cudaMemcpyAsync(ctl.p, &c, sizeof(c), cudaMemcpyHostToDevice, st));
+        REGB_CK(cudaMemcpyAsync(seg.p, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+        REGB_CK(cudaStreamSynchronize(st));
+    }
+};
+
+int pix_of(int dtype) { return dtype == REGB_F32 ? 1 : 0; }
+
+}  // namespace
+
+extern "C" {
+
+void regb_linear_param_default(regb_linear_param* p)
+{
+    if (!p)
+        return;
+    p->reg_type = REGB_REG_AFFINE;
+    p->cost_type = REGB_COST_MI;
+    p->bound = REGB_BOUND_REG;
+    p->search_count = 16;
+    p->absolute_bound = 1;
+}
+
+void regb_cdm_param_default(regb_cdm_param* p)
+{
+    if (!p)
+        return;
+    p->resolution = 2.0f;
+    p->speed = 0.3f;
+    p->smoothing = 0.05f;
+    p->min_dimension = 16;
+    p->gradient_type = 'r';
+}
+
+const char* regb_version(void) { return "regb200 1.0 (sm_100a)"; }
+const char* regb_last_error(void) { return last_error().c_str(); }
+
+regb_status regb_device_info(int* device, int* sm_count, size_t* free_bytes, size_t* total_bytes)
+{
+    return guarded([&] {
+        int dev = 0;
+        REGB_CK(cudaGetDevice(&dev));
+        int sms = 0;
+        REGB_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        size_t fr = 0, tot = 0;
+        REGB_CK(cudaMemGetInfo(&fr, &tot));
+        if (device) *device = dev;
+        if (sm_count) *sm_count = sms;
+        if (free_bytes) *free_bytes = fr;
+        if (total_bytes) *total_bytes = tot;
+        return REGB_OK;
+    });
+}
+
+regb_status regb_release(void)
+{
+    return guarded([&] {
+        int dev = 0;
+        REGB_CK(cudaGetDevice(&dev));
+        cudaMemPool_t pool;
+        REGB_CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+        REGB_CK(cudaDeviceSynchronize());
+        REGB_CK(cudaMemPoolTrimTo(pool, 0));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_affine_to_matrix(const float param[12], const int from_dim[3], const float from_vs[3],
+                                  const int to_dim[3], const float to_vs[3], float T[12])
+{
+    if (!param || !from_dim || !from_vs || !to_dim || !to_vs || !T)
+        return REGB_ERR_ARG;
+    affine_to_matrix(param, from_dim, from_vs, to_dim, to_vs, T);
+    return REGB_OK;
+}
+
+regb_status regb_affine_to_matrix_f64(const double param[12], const int from_dim[3], const double from_vs[3],
+                                      const int to_dim[3], const double to_vs[3], double T[12])
+{
+    if (!param || !from_dim || !from_vs || !to_dim || !to_vs || !T)
+        return REGB_ERR_ARG;
+    affine_to_matrix_f64(param, from_dim, from_vs, to_dim, to_vs, T);
+    return REGB_OK;
+}
+
+regb_status regb_matrix_inverse(float T[12])
+{
+    if (!T)
+        return REGB_ERR_ARG;
+    return matrix_inverse(T) ? REGB_OK : REGB_FALSE;
+}
+
+regb_status regb_resample(const regb_volume* from, regb_volume* to, const float T[12], int allow_shift_copy,
+                          void* stream)
+{
+    return guarded([&] {
+        check_vol(from, "from");
+        check_vol(to, "to");
+        if (!T)
+            throw Failure(REGB_ERR_ARG, "null transform");
+        if (from->dtype != to->dtype)
+            throw Failure(REGB_ERR_ARG, "from/to dtype differ");
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t ps = pix_size(from->dtype);
+        Staged a, b;
+        a.in(from->ptr, nvox(from->dim) * ps, from->location, st, true);
+        b.in(to->ptr, nvox(to->dim) * ps, to->location, st, false);
+        int shift[3];
+        const int* sh = (allow_shift_copy && integer_shift(T, shift)) ? shift : nullptr;
+        Dim3 fd{from->dim[0], from->dim[1], from->dim[2]}, td{to->dim[0], to->dim[1], to->dim[2]};
+        if (from->dtype == REGB_U8)
+            REGB_CK(launch_resample<uint8_t>((const uint8_t*)a.d, fd, (uint8_t*)b.d, td, T, sh, st));
+        else
+            REGB_CK(launch_resample<float>((const float*)a.d, fd, (float*)b.d, td, T, sh, st));
+        b.out(to->ptr, st);
+        if (a.host || b.host)
+            REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+static regb_status affine_cost(const regb_volume* fixed, const regb_volume* moving, const float* T, int K,
+                               double* cost, int32_t* hist_out, int cost_type, void* stream)
+{
+    return guarded([&] {
+        check_vol(fixed, "fixed");
+        check_vol(moving, "moving");
+        if (fixed->dtype != REGB_U8 || moving->dtype != REGB_U8)
+            throw Failure(REGB_ERR_ARG, "affine costs take uint8 volumes (reg/linear.hpp:622-629)");
+        if (!T || !cost || K < 0)
+            throw Failure(REGB_ERR_ARG, "bad transform/cost arguments");
+        if (K == 0)
+            return REGB_OK;
+        cudaStream_t st = (cudaStream_t)stream;
+        Staged a, b;
+        a.in(fixed->ptr, nvox(fixed->dim), fixed->location, st, true);
+        b.in(moving->ptr, nvox(moving->dim), moving->location, st, true);
+        AffineEvaluator::Pair pr{(const uint8_t*)a.d, Dim3{fixed->dim[0], fixed->dim[1], fixed->dim[2]},
+                                 (const uint8_t*)b.d, Dim3{moving->dim[0], moving->dim[1], moving->dim[2]}};
+        AffineEvaluator ev({pr}, cost_type, st);
+        if (hist_out && cost_type == REGB_COST_MI) {
+            // histograms requested: evaluate one task at a time and read its counts
+            // before the kernel's last block clears them.
+            TaskScratch s;
+            s.ensure(1, true, st);
+            PinBuf<uint32_t> h(65536);
+            for (int k = 0; k < K; ++k) {
+                ev.make_task(0, T + 12 * k, s.h_tasks.p[0]);
+                AffineTask& t = s.h_tasks.p[0];
+                t.ticket = s.ticket.p;
+                t.cost = s.cost.p;
+                t.moments = s.moments.p;
+                t.hist = s.hist.p;
+                t.keep = 1;  // leave the counts in place for the read-back
+                REGB_CK(cudaMemcpyAsync(s.tasks.p, s.h_tasks.p, sizeof(AffineTask), cudaMemcpyHostToDevice, st));
+                REGB_CK(launch_mi(s.tasks.p, 1, t.nchunk, st));
+                REGB_CK(cudaMemcpyAsync(h.p, s.hist.p, 65536 * 4, cudaMemcpyDeviceToHost, st));
+                REGB_CK(cudaStreamSynchronize(st));
+                // bin 0 is not counted on the device; it is the remainder
+                long long tot = 0;
+                for (int i = 1; i < 65536; ++i)
+                    tot += h.p[i];
+                h.p[0] = (uint32_t)((long long)nvox(fixed->dim) - tot);
+                std::memcpy(hist_out + (size_t)k * 65536, h.p, 65536 * 4);
+                REGB_CK(cudaMemsetAsync(s.hist.p, 0, 65536 * 4, st));
+            }
+        }
+        std::vector<double> c = ev.eval(0, T, K);
+        std::memcpy(cost, c.data(), sizeof(double) * K);
+        return REGB_OK;
+    });
+}
+
+regb_status regb_mi_cost(const regb_volume* fixed, const regb_volume* moving, const float* T, int K, double* cost,
+                         int32_t* hist_out, void* stream)
+{
+    return affine_cost(fixed, moving, T, K, cost, hist_out, REGB_COST_MI, stream);
+}
+
+regb_status regb_corr_cost(const regb_volume* fixed, const regb_volume* moving, const float* T, int K, double* cost,
+                           void* stream)
+{
+    return affine_cost(fixed, moving, T, K, cost, nullptr, REGB_COST_CORR, stream);
+}
+
+regb_status regb_compose_displacement(const regb_volume* from, const regb_field* dis, regb_volume* to, void* stream)
+{
+    return guarded([&] {
+        check_vol(from, "from");
+        check_field(dis, "dis");
+        check_vol(to, "to");
+        if (!same_dims(from->dim, dis->dim) || !same_dims(from->dim, to->dim) || from->dtype != to->dtype)
+            throw Failure(REGB_ERR_ARG, "compose: shapes/dtypes differ");
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t n = nvox(from->dim), ps = pix_size(from->dtype);
+        Staged a, f, o;
+        a.in(from->ptr, n * ps, from->location, st, true);
+        f.in(dis->ptr, n * 12, dis->location, st, true);
+        o.in(to->ptr, n * ps, to->location, st, false);
+        OneSeg s(from->dim, st);
+        s.h.Is = a.d;
+        s.h.cur_d = (float*)f.d;
+        s.h.Js = o.d;
+        s.upload(st);
+        REGB_CK(launch_cdm_compose(s.seg.p, 1, s.h.nblk, pix_of(from->dtype), st));
+        o.out(to->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_accumulate_displacement(const regb_field* dis, regb_field* new_dis, void* stream)
+{
+    return guarded([&] {
+        check_field(dis, "dis");
+        check_field(new_dis, "new_dis");
+        if (!same_dims(dis->dim, new_dis->dim))
+            throw Failure(REGB_ERR_ARG, "accumulate: shapes differ");
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t n = nvox(dis->dim);
+        Staged a, b;
+        a.in(dis->ptr, n * 12, dis->location, st, true);
+        b.in(new_dis->ptr, n * 12, new_dis->location, st, true);
+        DevBuf<float> out(3 * n, st);
+        OneSeg s(dis->dim, st);
+        s.h.cur_d = (float*)a.d;
+        s.h.aux_d = (float*)b.d;
+        s.h.tmp_d = out.p;
+        s.c.scale = 1.0f;
+        s.upload(st);
+        REGB_CK(launch_cdm_accumulate(s.seg.p, 1, s.h.nblk, st));
+        REGB_CK(cudaMemcpyAsync(b.d, out.p, n * 12, cudaMemcpyDeviceToDevice, st));
+        b.out(new_dis->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_downsample(const regb_volume* in, regb_volume* out, void* stream)
+{
+    return guarded([&] {
+        check_vol(in, "in");
+        check_vol(out, "out");
+        const int od[3] = {(in->dim[0] + 1) / 2, (in->dim[1] + 1) / 2, (in->dim[2] + 1) / 2};
+        if (!same_dims(od, out->dim) || in->dtype != out->dtype)
+            throw Failure(REGB_ERR_ARG, "downsample: out must be (d+1)/2 with the same dtype");
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t ps = pix_size(in->dtype);
+        Staged a, b;
+        a.in(in->ptr, nvox(in->dim) * ps, in->location, st, true);
+        b.in(out->ptr, nvox(out->dim) * ps, out->location, st, false);
+        REGB_CK(launch_downsample(a.d, b.d, in->dim[0], in->dim[1], in->dim[2], pix_of(in->dtype), st));
+        b.out(out->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_upsample_field_x2(const regb_field* in, regb_field* out, void* stream)
+{
+    return guarded([&] {
+        check_field(in, "in");
+        check_field(out, "out");
+        cudaStream_t st = (cudaStream_t)stream;
+        Staged a, b;
+        a.in(in->ptr, nvox(in->dim) * 12, in->location, st, true);
+        b.in(out->ptr, nvox(out->dim) * 12, out->location, st, false);
+        REGB_CK(launch_upsample_field_x2((const float*)a.d, in->dim[0], in->dim[1], in->dim[2], (float*)b.d,
+                                         out->dim[0], out->dim[1], out->dim[2], st));
+        b.out(out->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_cdm_gradient(const regb_volume* Js, const regb_volume* It, regb_field* new_d, int gradient_type,
+                              float* cost, void* stream)
+{
+    return guarded([&] {
+        check_vol(Js, "Js");
+        check_vol(It, "It");
+        check_field(new_d, "new_d");
+        if (!same_dims(Js->dim, It->dim) || !same_dims(Js->dim, new_d->dim) || Js->dtype != It->dtype)
+            throw Failure(REGB_ERR_ARG, "gradient: shapes/dtypes differ");
+        if (gradient_type != 'r' && gradient_type != 'd')
+            throw Failure(REGB_ERR_ARG, "gradient_type must be 'r' or 'd'");
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t n = nvox(Js->dim), ps = pix_size(Js->dtype);
+        Staged a, b, o;
+        a.in(Js->ptr, n * ps, Js->location, st, true);
+        b.in(It->ptr, n * ps, It->location, st, true);
+        o.in(new_d->ptr, n * 12, new_d->location, st, false);
+        OneSeg s(Js->dim, st);
+        s.h.Js = a.d;
+        s.h.It = b.d;
+        s.h.new_d = (float*)o.d;
+        s.upload(st);
+        REGB_CK(launch_cdm_gradient(s.seg.p, 1, s.h.nblk, pix_of(Js->dtype), gradient_type, st));
+        DevBuf<float> c(1, st);
+        REGB_CK(launch_cost_mean(s.seg.p, 1, c.p, st));
+        float hc = 0.0f;
+        REGB_CK(cudaMemcpyAsync(&hc, c.p, 4, cudaMemcpyDeviceToHost, st));
+        o.out(new_d->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
+        if (cost)
+            *cost = hc;
+        return REGB_OK;
+    });
+}
+
+regb_status regb_cdm_poisson(regb_field* new_d, void* stream)
+{
+    return guarded([&] {
+        check_field(new_d, "new_d");
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t n = nvox(new_d->dim);
+        Staged a;
+        a.in(new_d->ptr, n * 12, new_d->location, st, true);
+        DevBuf<float> A(3 * n, st), B(3 * n, st);
+        OneSeg s(new_d->dim, st);
+        s.h.new_d = (float*)a.d;
+        s.h.aux_d = A.p;
+        s.h.tmp_d = B.p;
+        s.upload(st);
+        REGB_CK(launch_cdm_poisson(s.seg.p, 1, s.h.nblk, 12, st));
+        REGB_CK(cudaMemcpyAsync(a.d, A.p, n * 12, cudaMemcpyDeviceToDevice, st));
+        a.out(new_d->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_cdm_max_length(const regb_field* d, float* out, void* stream)
+{
+    return guarded([&] {
+        check_field(d, "d");
+        if (!out)
+            throw Failure(REGB_ERR_ARG, "null output");
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t n = nvox(d->dim);
+        Staged a;
+        a.in(d->ptr, n * 12, d->location, st, true);
+        OneSeg s(d->dim, st);
+        s.h.aux_d = (float*)a.d;
+        s.c.speed = 1.0f;
+        s.upload(st);
+        REGB_CK(launch_cdm_theta(s.seg.p, 1, s.h.nblk, st));
+        CdmCtl c;
+        REGB_CK(cudaMemcpyAsync(&c, s.ctl.p, sizeof(c), cudaMemcpyDeviceToHost, st));
+        REGB_CK(cudaStreamSynchronize(st));
+        *out = c.theta;
+        return REGB_OK;
+    });
+}
+
+regb_status regb_cdm_smooth(const regb_field* d, regb_field* dd, float smoothing, void* stream)
+{
+    return guarded([&] {
+        check_field(d, "d");
+        check_field(dd, "dd");
+        if (!same_dims(d->dim, dd->dim))
+            throw Failure(REGB_ERR_ARG, "smooth: shapes differ");
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t n = nvox(d->dim);
+        Staged a, b;
+        a.in(d->ptr, n * 12, d->location, st, true);
+        b.in(dd->ptr, n * 12, dd->location, st, true);
+        OneSeg s(d->dim, st);
+        s.h.tmp_d = (float*)a.d;
+        s.h.cur_d = (float*)b.d;
+        s.c.cur_smoothing = smoothing;
+        s.upload(st);
+        REGB_CK(launch_cdm_smooth(s.seg.p, 1, s.h.nblk, st));
+        b.out(dd->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_cdm(const regb_volume* It, const regb_volume* Is, regb_field* dis_out, const regb_cdm_param* param,
+                     volatile const int* terminated)
+{
+    return guarded([&] {
+        check_vol(It, "It");
+        check_vol(Is, "Is");
+        check_field(dis_out, "dis_out");
+        if (!same_dims(It->dim, Is->dim) || !same_dims(It->dim, dis_out->dim) || It->dtype != Is->dtype)
+            throw Failure(REGB_ERR_ARG, "cdm: It/Is/dis shapes or dtypes differ");
+        regb_cdm_param p;
+        regb_cdm_param_default(&p);
+        if (param)
+            p = *param;
+        if (p.gradient_type != 'r' && p.gradient_type != 'd')
+            throw Failure(REGB_ERR_ARG, "gradient_type must be 'r' or 'd'");
+        Stream s;
+        const size_t n = nvox(It->dim), ps = pix_size(It->dtype);
+        Staged a, b, f;
+        a.in(It->ptr, n * ps, It->location, s.s, true);
+        b.in(Is->ptr, n * ps, Is->location, s.s, true);
+        f.in(dis_out->ptr, n * 12, dis_out->location, s.s, false);
+        regb_status r = cdm_register(a.d, b.d, It->dim, pix_of(It->dtype), (float*)f.d, p, terminated, s.s);
+        if (r == REGB_OK || r == REGB_CANCELLED)
+            f.out(dis_out->ptr, s.s);
+        s.sync();
+        return r;
+    });
+}
+
+regb_status regb_linear(const regb_volume* from, const float from_vs[3], const regb_volume* to, const float to_vs[3],
+                        float arg[12], const regb_linear_param* param, volatile const int* terminated,
+                        float* cost_out, long long* cost_evals)
+{
+    return guarded([&] {
+        check_vol(from, "from");
+        check_vol(to, "to");
+        if (from->dtype != REGB_U8 || to->dtype != REGB_U8)
+            throw Failure(REGB_ERR_ARG, "linear takes uint8 volumes (reg/linear.hpp:622-629)");
+        if (!from_vs || !to_vs || !arg)
+            throw Failure(REGB_ERR_ARG, "null voxel size / arg");
+        regb_linear_param p;
+        regb_linear_param_default(&p);
+        if (param)
+            p = *param;
+        if (p.cost_type != REGB_COST_MI && p.cost_type != REGB_COST_CORR)
+            throw Failure(REGB_ERR_ARG, "cost_type must be MI or CORR");
+        Stream s;
+        Staged a, b;
+        a.in(from->ptr, nvox(from->dim), from->location, s.s, true);
+        b.in(to->ptr, nvox(to->dim), to->location, s.s, true);
+        LinearResult r = linear_register((const uint8_t*)a.d, from->dim, from_vs, (const uint8_t*)b.d, to->dim, to_vs,
+                                         arg, p, terminated, s.s);
+        s.sync();
+        if (cost_out)
+            *cost_out = r.cost;
+        if (cost_evals)
+            *cost_evals = r.evals;
+        return (terminated && *terminated) ? REGB_CANCELLED : REGB_OK;
+    });
+}
+
+}  // extern "C"

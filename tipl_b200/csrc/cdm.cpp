@@ -1,0 +1,159 @@
+// CDM nonlinear registration driver (reg/cdm.hpp:373-474, cdm_common 534-558) on
+// device-resident images of one job.
+//
+// Pyramid: levels are built by downsample_with_padding while min(shape) >
+// min_dimension (reg/cdm.hpp:382-392).  The coarsest level always iterates; a
+// finer level starts from the doubled, upsampled field of the level below and
+// iterates only when its resolution (param.resolution halved per level) is at
+// most 1 (reg/cdm.hpp:400-405).
+//
+// Each iteration is the kernel sequence of cdm_kernels.cu; the loop decisions run
+// on the device (CdmCtl), and this plain, single-job driver reads the done flag
+// back after every iteration, as the reference reads its cost back.
+#include <algorithm>
+#include <cfloat>
+#include <cstring>
+#include <vector>
+#include "cdm_level.h"
+#include "host.h"
+
+namespace regb {
+
+void CdmLevel::init(const void* It_, const void* Is_, int w, int h, int d, int pix_, const regb_cdm_param& p,
+                    float* best, cudaStream_t st)
+{
+    pix = pix_;
+    seg = CdmSeg{};
+    seg.w = w;
+    seg.h = h;
+    seg.d = d;
+    const long long n = (long long)w * h * d;
+    seg.nblk = cdm_blocks_for(n);
+    seg.It = It_;
+    seg.Is = Is_;
+    js.alloc((size_t)n * (pix ? 4 : 1), st);
+    cur.alloc(3 * n, st);
+    nd.alloc(3 * n, st);
+    aux.alloc(3 * n, st);
+    tmp.alloc(3 * n, st);
+    part.alloc(seg.nblk, st);
+    ctl.alloc(1, st);
+    seg.Js = js.p;
+    seg.cur_d = cur.p;
+    seg.best_d = best;
+    seg.new_d = nd.p;
+    seg.aux_d = aux.p;
+    seg.tmp_d = tmp.p;
+    seg.cost_part = part.p;
+    seg.ctl = ctl.p;
+    CdmCtl c;
+    std::memset(&c, 0, sizeof(c));
+    c.best_cost = FLT_MAX;
+    c.cur_smoothing = 0.8f;
+    c.speed = p.speed;
+    c.smoothing = p.smoothing;
+    c.max_iter = 200;
+    h_ctl = c;
+    REGB_CK(cudaMemcpyAsync(ctl.p, &h_ctl, sizeof(CdmCtl), cudaMemcpyHostToDevice, st));
+    REGB_CK(cudaMemcpyAsync(cur.p, best, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, st));  // cur_d(best_d)
+    d_seg.alloc(1, st);
+    REGB_CK(cudaMemcpyAsync(d_seg.p, &seg, sizeof(CdmSeg), cudaMemcpyHostToDevice, st));
+    REGB_CK(cudaStreamSynchronize(st));  // h_ctl / seg are stack-staged: keep the copies ordered before reuse
+}
+
+void launch_iteration(const CdmSeg* d_segs, int nseg, int blocks, int pix, int gradient_type, cudaStream_t st)
+{
+    REGB_CK(launch_cdm_compose(d_segs, nseg, blocks, pix, st));
+    REGB_CK(launch_cdm_gradient(d_segs, nseg, blocks, pix, gradient_type, st));
+    REGB_CK(launch_cdm_control(d_segs, nseg, blocks, st));
+    REGB_CK(launch_cdm_best_copy(d_segs, nseg, blocks, st));
+    REGB_CK(launch_cdm_poisson(d_segs, nseg, blocks, 12, st));
+    REGB_CK(launch_cdm_theta(d_segs, nseg, blocks, st));
+    REGB_CK(launch_cdm_accumulate(d_segs, nseg, blocks, st));
+    REGB_CK(launch_cdm_smooth(d_segs, nseg, blocks, st));
+}
+
+regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int pix, float* d_field,
+                         const regb_cdm_param& p, volatile const int* terminated, cudaStream_t st, int* iterations)
+{
+    const size_t psz = pix ? 4 : 1;
+    struct Lv {
+        int w, h, d;
+        const void* It;
+        const void* Is;
+        DevBuf<uint8_t> bt, bs;
+        DevBuf<float> best;
+        float resolution;
+    };
+    std::vector<Lv> lv;
+    lv.emplace_back();
+    lv[0].w = dim[0];
+    lv[0].h = dim[1];
+    lv[0].d = dim[2];
+    lv[0].It = d_It;
+    lv[0].Is = d_Is;
+    lv[0].resolution = p.resolution;
+    for (;;) {
+        Lv& c = lv.back();
+        if (!((unsigned int)std::min(c.w, std::min(c.h, c.d)) > p.min_dimension))
+            break;
+        Lv n;
+        n.w = (c.w + 1) / 2;
+        n.h = (c.h + 1) / 2;
+        n.d = (c.d + 1) / 2;
+        n.resolution = c.resolution / 2.0f;
+        const size_t nn = (size_t)n.w * n.h * n.d;
+        n.bt.alloc(nn * psz, st);
+        n.bs.alloc(nn * psz, st);
+        REGB_CK(launch_downsample(c.It, n.bt.p, c.w, c.h, c.d, pix, st));
+        REGB_CK(launch_downsample(c.Is, n.bs.p, c.w, c.h, c.d, pix, st));
+        n.It = n.bt.p;
+        n.Is = n.bs.p;
+        lv.push_back(std::move(n));
+    }
+    const int top = (int)lv.size() - 1;
+    int iters = 0;
+    regb_status status = REGB_OK;
+    for (int k = top; k >= 0; --k) {
+        Lv& L = lv[k];
+        const size_t n = (size_t)L.w * L.h * L.d;
+        float* best = d_field;
+        if (k > 0) {
+            L.best.alloc(3 * n, st);
+            best = L.best.p;
+        }
+        if (k == top)
+            REGB_CK(cudaMemsetAsync(best, 0, sizeof(float) * 3 * n, st));
+        else {
+            const Lv& C = lv[k + 1];
+            const float* cb = C.best.p;
+            REGB_CK(launch_upsample_field_x2(cb, C.w, C.h, C.d, best, L.w, L.h, L.d, st));
+            if (L.resolution > 1.0f)
+                continue;  // reg/cdm.hpp:404-405
+        }
+        if (status != REGB_OK)
+            continue;
+        CdmLevel run;
+        run.init(L.It, L.Is, L.w, L.h, L.d, pix, p, best, st);
+        for (int it = 0; it < 201; ++it) {
+            if (terminated && *terminated) {
+                status = REGB_CANCELLED;
+                break;
+            }
+            launch_iteration(run.d_seg.p, 1, run.seg.nblk, pix, p.gradient_type, st);
+            REGB_CK(cudaMemcpyAsync(&run.h_ctl, run.ctl.p, sizeof(CdmCtl), cudaMemcpyDeviceToHost, st));
+            REGB_CK(cudaStreamSynchronize(st));
+            if (run.h_ctl.done)
+                break;
+        }
+        iters += run.h_ctl.iters_run;
+        if (run.h_ctl.done == 2)
+            return REGB_FALSE;  // reg/cdm.hpp:428-429: a zero cost sum fails the whole call
+    }
+    REGB_CK(cudaStreamSynchronize(st));
+    if (iterations)
+        *iterations = iters;
+    return status;
+}
+
+}  // namespace regb

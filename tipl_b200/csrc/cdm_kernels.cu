@@ -1,0 +1,729 @@
+// CDM nonlinear registration passes (reg/cdm.hpp) and the displacement algebra
+// they use (numerical/dif.hpp), as segment kernels: blockIdx.y selects a job
+// level (CdmSeg), blockIdx.x < seg.nblk strides over its voxels.
+//
+// One iteration of a level (reg/cdm.hpp:418-470) is the launch sequence
+//   compose -> gradient -> control -> best_copy -> poisson -> theta -> accumulate -> smooth
+// The reference's host-side decisions (cost bookkeeping, cdm_improved, the
+// smoothing schedule, best_d restore, theta, the iteration cap) run in the control
+// and theta kernels against CdmCtl, so a level runs without any host round trip;
+// every later kernel of an iteration reads ctl->done and returns once a level has
+// left its loop.
+#include <cfloat>
+#include "common.cuh"
+#include "stats.h"
+
+namespace regb {
+
+constexpr int kCdmThreads = 256;
+
+int cdm_blocks_for(long long nvox)
+{
+    long long b = (nvox + kCdmThreads - 1) / kCdmThreads;
+    if (b > 148 * 8)
+        b = 148 * 8;
+    return (int)(b < 1 ? 1 : b);
+}
+
+#define SEG_BEGIN                                                  \
+    const CdmSeg& S = segs[blockIdx.y];                            \
+    if ((int)blockIdx.x >= S.nblk)                                 \
+        return;                                                    \
+    const Dim3 D{S.w, S.h, S.d};                                   \
+    const long long n = D.n();                                     \
+    const long long stride = (long long)S.nblk * blockDim.x;       \
+    const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+
+// ------------------------------------------------------------------ compose
+// compose_displacement (numerical/dif.hpp:90-107, 260-285): Js = Is where the
+// displacement is exactly zero, else the trilinear sample at x + d; failed
+// samples are 0.
+template <typename T>
+__global__ void __launch_bounds__(kCdmThreads) cdm_compose_kernel(const CdmSeg* __restrict__ segs)
+{
+    SEG_BEGIN
+    if (S.ctl->done)
+        return;
+    const T* __restrict__ Is = (const T*)S.Is;
+    T* __restrict__ Js = (T*)S.Js;
+    const float* __restrict__ cd = S.cur_d;
+    for (long long i = first; i < n; i += stride) {
+        const float dx = cd[3 * i], dy = cd[3 * i + 1], dz = cd[3 * i + 2];
+        T v;
+        if (dx == 0.0f && dy == 0.0f && dz == 0.0f)
+            v = Is[i];
+        else {
+            int x, y, z;
+            unflat((int)i, D, x, y, z);
+            float px = (float)x, py = (float)y, pz = (float)z;
+            px += dx;
+            py += dy;
+            pz += dz;
+            Cell c;
+            v = T(0);
+            if (trilinear_cell(D, px, py, pz, c))
+                v = assign_pix<T>(cell_sum(Is, D, c));
+        }
+        Js[i] = v;
+    }
+}
+
+// ------------------------------------------------------------------ gradient
+// Window sums of linear_regression over the clipped 5^3 window
+// (numerical/window.hpp:92-110, numerical/statistics.hpp:694-713).  Integer
+// pixels: exact integer sums (the reference sums in int64).  Float pixels: double
+// sums in the reference's visiting order with float cross products.
+struct Reg {
+    float a, b, r2;
+};
+
+__device__ __forceinline__ void regress_finish(double sx, double sy, double sxx, double syy, double sxy, int m,
+                                               Reg& r)
+{
+    const double dn = (double)m;
+    const double mx = sx / dn, my = sy / dn;
+    const double xv = sxx / dn - mx * mx;
+    const double yv = syy / dn - my * my;
+    if (xv == 0.0 || yv == 0.0) {
+        r.a = 0.0f;
+        r.b = (float)my;
+        r.r2 = 0.0f;
+        return;
+    }
+    const double cov = sxy / dn - mx * my;
+    r.a = (float)(cov / xv);
+    r.b = (float)(my - (double)r.a * mx);  // b uses the float-rounded slope
+    r.r2 = (float)(cov * cov / xv / yv);
+}
+
+template <typename T>
+struct WindowAcc;
+
+template <>
+struct WindowAcc<uint8_t> {
+    int sx = 0, sy = 0, sxx = 0, syy = 0, sxy = 0, m = 0;
+    __device__ __forceinline__ void add(uint8_t j, uint8_t t)
+    {
+        const int a = j, b = t;
+        sx += a;
+        sy += b;
+        sxx += a * a;
+        syy += b * b;
+        sxy += a * b;
+        ++m;
+    }
+    __device__ __forceinline__ void finish(Reg& r) const
+    {
+        regress_finish((double)sx, (double)sy, (double)sxx, (double)syy, (double)sxy, m, r);
+    }
+};
+
+template <>
+struct WindowAcc<float> {
+    double sx = 0, sy = 0, sxx = 0, syy = 0, sxy = 0;
+    int m = 0;
+    __device__ __forceinline__ void add(float j, float t)
+    {
+        // sum(): first element then +=; square_sum(): 0 + t*t in double;
+        // inner_product(): float product widened to double.
+        if (m == 0) {
+            sx = (double)j;
+            sy = (double)t;
+            sxy = (double)(j * t);
+        } else {
+            sx += (double)j;
+            sy += (double)t;
+            sxy += (double)(j * t);
+        }
+        const double dj = j, dt = t;
+        sxx += dj * dj;
+        syy += dt * dt;
+        ++m;
+    }
+    __device__ __forceinline__ void finish(Reg& r) const { regress_finish(sx, sy, sxx, syy, sxy, m, r); }
+};
+
+template <typename T>
+__device__ __forceinline__ float pix_diff(T a, T b)
+{
+    return (float)(a - b);
+}
+template <>
+__device__ __forceinline__ float pix_diff<uint8_t>(uint8_t a, uint8_t b)
+{
+    return (float)((int)a - (int)b);
+}
+
+// gradient_at (numerical/numerical.hpp:102-109)
+template <typename T>
+__device__ __forceinline__ float3 grad_at(const T* __restrict__ I, const Dim3& D, int x, int y, int z, long long i)
+{
+    float3 g;
+    const long long w = D.w, wh = D.wh();
+    g.x = (x + 1 < D.w && x) ? pix_diff(I[i + 1], I[i - 1]) : 0.0f;
+    g.y = (y + 1 < D.h && y) ? pix_diff(I[i + w], I[i - w]) : 0.0f;
+    g.z = (z + 1 < D.d && z) ? pix_diff(I[i + wh], I[i - wh]) : 0.0f;
+    return g;
+}
+
+// cdm_get_gradient_r_imp / _d_imp (reg/cdm.hpp:46-78): new_d = 0 + gradient term;
+// the cost of every voxel (0 where skipped) is summed per block in double.
+template <typename T>
+__global__ void __launch_bounds__(kCdmThreads) cdm_gradient_kernel(const CdmSeg* __restrict__ segs, int gtype)
+{
+    SEG_BEGIN
+    if (S.ctl->done)
+        return;
+    const T* __restrict__ Js = (const T*)S.Js;
+    const T* __restrict__ It = (const T*)S.It;
+    float* __restrict__ nd = S.new_d;
+    double csum = 0.0;
+    for (long long i = first; i < n; i += stride) {
+        int x, y, z;
+        unflat((int)i, D, x, y, z);
+        float3 out = make_float3(0.0f, 0.0f, 0.0f);
+        float cost = 0.0f;
+        const T js = Js[i], it = It[i];
+        if (gtype == 'd') {
+            float3 g = grad_at(Js, D, x, y, z, i);
+            const float dif = pix_diff(js, it);
+            g.x *= dif;
+            g.y *= dif;
+            g.z *= dif;
+            out.x = 0.0f + g.x;
+            out.y = 0.0f + g.y;
+            out.z = 0.0f + g.z;
+            cost = dif * dif;
+        } else if (!(js == T(0) || it == T(0))) {
+            const int xu = min(D.w - x - 1, 2), yu = min(D.h - y - 1, 2), zu = min(D.d - z - 1, 2);
+            const int xl = min(x, 2), yl = min(y, 2), zl = min(z, 2);
+            const long long w = D.w, wh = D.wh();
+            WindowAcc<T> acc;
+            // iterate_xyz order (numerical/window.hpp:54-72)
+            for (int pz = 0; pz < 2; ++pz) {
+                const int zc = pz ? zl : zu;
+                for (int dz = pz; dz <= zc; ++dz) {
+                    const long long zi = i + (pz ? -dz : dz) * wh;
+                    for (int py = 0; py < 2; ++py) {
+                        const int yc = py ? yl : yu;
+                        for (int dy = py; dy <= yc; ++dy) {
+                            const long long yi = zi + (py ? -dy : dy) * w;
+                            for (int dx = 0; dx <= xu; ++dx)
+                                acc.add(Js[yi + dx], It[yi + dx]);
+                            for (int dx = 1; dx <= xl; ++dx)
+                                acc.add(Js[yi - dx], It[yi - dx]);
+                        }
+                    }
+                }
+            }
+            Reg r;
+            acc.finish(r);
+            if (r.a > 0.0f) {
+                float3 g = grad_at(Js, D, x, y, z, i);
+                const float s = r.r2 * ((float)js * r.a + r.b - (float)it);
+                g.x *= s;
+                g.y *= s;
+                g.z *= s;
+                out.x = 0.0f + g.x;
+                out.y = 0.0f + g.y;
+                out.z = 0.0f + g.z;
+                cost = -r.r2;
+            }
+        }
+        nd[3 * i] = out.x;
+        nd[3 * i + 1] = out.y;
+        nd[3 * i + 2] = out.z;
+        csum += (double)cost;
+    }
+    __shared__ double red[32];
+    csum = block_sum(csum, red);
+    if (threadIdx.x == 0)
+        S.cost_part[blockIdx.x] = csum;
+}
+
+// ------------------------------------------------------------------ control
+// cdm_improved (reg/cdm.hpp:19-34): regression of the last costs on their index
+// (int x, float y; statistics.hpp:694-713); a positive slope means "not improved".
+__device__ bool cdm_improved_dev(CdmCtl* c)
+{
+    const int n = c->ncost;
+    if (n > 5) {
+        long long sx = 0, sxx = 0;
+        double sy = (double)c->cost[0], syy = 0.0, sxy = (double)(0.0f * c->cost[0]);
+        for (int i = 0; i < n; ++i) {
+            sx += i;
+            sxx += (long long)i * i;
+        }
+        for (int i = 1; i < n; ++i) {
+            sy += (double)c->cost[i];
+            sxy += (double)((float)i * c->cost[i]);
+        }
+        for (int i = 0; i < n; ++i) {
+            const double t = c->cost[i];
+            syy += t * t;
+        }
+        const double mx = (double)sx / n, my = sy / n;
+        const double xv = (double)sxx / n - mx * mx, yv = syy / n - my * my;
+        float a = 0.0f;
+        if (!(xv == 0.0 || yv == 0.0))
+            a = (float)((sxy / n - mx * my) / xv);
+        if (a > 0.0f)
+            return false;
+        if (n > 7) {
+            for (int i = 1; i < n; ++i)
+                c->cost[i - 1] = c->cost[i];
+            c->ncost = n - 1;
+        }
+    }
+    return true;
+}
+
+// Mean of the per-block cost partials, summed in a fixed order.
+__device__ float seg_cost_mean(const CdmSeg& S)
+{
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int k = threadIdx.x; k < S.nblk; k += blockDim.x)
+        s += S.cost_part[k];
+    s = block_sum(s, red);
+    __shared__ float out;
+    if (threadIdx.x == 0)
+        out = (float)(s / (double)((long long)S.w * S.h * S.d));
+    __syncthreads();
+    return out;
+}
+
+// The body of the reference's iteration loop between the gradient and the
+// Poisson solve (reg/cdm.hpp:418-460).  One block per segment.
+__global__ void cdm_control_kernel(const CdmSeg* __restrict__ segs)
+{
+    const CdmSeg& S = segs[blockIdx.y];
+    CdmCtl* c = S.ctl;
+    if (c->done) {
+        if (threadIdx.x == 0)
+            c->save_best = c->restore = 0;
+        return;
+    }
+    const float mean_cost = seg_cost_mean(S);
+    if (threadIdx.x != 0)
+        return;
+    c->save_best = 0;
+    c->restore = 0;
+    if (c->index >= c->max_iter) {
+        c->done = 1;
+        return;
+    }
+    float sum_cost = 0.0f;
+    sum_cost += mean_cost;
+    c->last_cost = sum_cost;
+    if (sum_cost == 0.0f) {
+        c->done = 2;
+        return;
+    }
+    c->cost[c->ncost++] = sum_cost / 1.0f;
+    const float cur = c->cost[c->ncost - 1];
+    if (cur < c->best_cost) {
+        c->best_cost = cur;
+        if (c->index)
+            c->save_best = 1;
+    }
+    if (!cdm_improved_dev(c)) {
+        if (c->cur_smoothing <= c->smoothing) {
+            c->done = 1;
+            ++c->iters_run;
+            return;
+        }
+        c->restore = 1;
+        c->cur_smoothing *= 0.5f;
+        c->ncost = 0;
+    }
+    ++c->index;
+    ++c->iters_run;
+}
+
+// best_d = cur_d when the cost improved (reg/cdm.hpp:447-452); otherwise, on a
+// stall, cur_d = best_d (reg/cdm.hpp:457).  Runs even on the iteration that
+// leaves the loop, as the reference saves best_d before its break.
+__global__ void __launch_bounds__(kCdmThreads) cdm_best_copy_kernel(const CdmSeg* __restrict__ segs)
+{
+    SEG_BEGIN
+    const CdmCtl* c = S.ctl;
+    const float* src;
+    float* dst;
+    if (c->save_best) {
+        src = S.cur_d;
+        dst = S.best_d;
+    } else if (c->restore) {
+        src = S.best_d;
+        dst = S.cur_d;
+    } else
+        return;
+    for (long long i = first; i < 3 * n; i += stride)
+        dst[i] = src[i];
+}
+
+// ------------------------------------------------------------------ Poisson
+// cdm_solve_poisson (reg/cdm.hpp:158-253): s0 = new_d * (-1/6); then Jacobi sweeps
+// s' = (new_d - s[-1] - s[+1] - s[-w] - s[+w] - s[-wh] - s[+wh]) * (-1/6) with the
+// neighbours taken by flat index, bounds on the flat index only.
+__global__ void __launch_bounds__(kCdmThreads) cdm_poisson_init_kernel(const CdmSeg* __restrict__ segs)
+{
+    SEG_BEGIN
+    if (S.ctl->done)
+        return;
+    const float c = -0.5f / 3.0f;
+    for (long long i = first; i < 3 * n; i += stride)
+        S.aux_d[i] = S.new_d[i] * c;
+}
+
+__global__ void __launch_bounds__(kCdmThreads) cdm_poisson_sweep_kernel(const CdmSeg* __restrict__ segs, int parity)
+{
+    SEG_BEGIN
+    if (S.ctl->done)
+        return;
+    const float* __restrict__ s = parity ? S.tmp_d : S.aux_d;
+    float* __restrict__ o = parity ? S.aux_d : S.tmp_d;
+    const float* __restrict__ rhs = S.new_d;
+    const long long w = D.w, wh = D.wh();
+    const float inv_d2 = -0.5f / 3.0f;
+    for (long long p = first; p < n; p += stride) {
+        float v[3] = {rhs[3 * p], rhs[3 * p + 1], rhs[3 * p + 2]};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (p >= 1) v[c] -= s[3 * (p - 1) + c];
+            if (p < n - 1) v[c] -= s[3 * (p + 1) + c];
+            if (p >= w) v[c] -= s[3 * (p - w) + c];
+            if (p < n - w) v[c] -= s[3 * (p + w) + c];
+            if (p >= wh) v[c] -= s[3 * (p - wh) + c];
+            if (p < n - wh) v[c] -= s[3 * (p + wh) + c];
+            v[c] *= inv_d2;
+            o[3 * p + c] = v[c];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ theta
+// cdm_max_displacement_length (reg/cdm.hpp:260-295), only while theta == 0 (the
+// first iteration of a level); the last block sets theta and speed/theta, or
+// leaves the loop when theta is 0 (reg/cdm.hpp:463-467).
+__global__ void __launch_bounds__(kCdmThreads) cdm_theta_kernel(const CdmSeg* __restrict__ segs)
+{
+    SEG_BEGIN
+    CdmCtl* c = S.ctl;
+    if (c->done || c->theta != 0.0f)
+        return;
+    const float* __restrict__ d = S.aux_d;
+    float m = 0.0f;
+    for (long long i = first; i < n; i += stride) {
+        const float x = d[3 * i], y = d[3 * i + 1], z = d[3 * i + 2];
+        const float l2 = x * x + y * y + z * z;
+        const float l = (float)sqrt((double)l2);
+        m = fmaxf(m, l);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0)
+        atomicMax(&c->theta_bits, __float_as_uint(m));
+    __threadfence();
+    __syncthreads();
+    __shared__ unsigned int last;
+    if (threadIdx.x == 0)
+        last = (atomicAdd(&c->ticket, 1u) == (unsigned)S.nblk - 1u);
+    __syncthreads();
+    if (!last || threadIdx.x != 0)
+        return;
+    __threadfence();
+    const float theta = __uint_as_float(atomicAdd(&c->theta_bits, 0u));
+    c->ticket = 0u;
+    c->theta = theta;
+    if (theta == 0.0f)
+        c->done = 1;
+    else
+        c->scale = c->speed / theta;
+}
+
+// ------------------------------------------------------------------ accumulate
+// new_d *= speed/theta (reg/cdm.hpp:467) fused with accumulate_displacement
+// (numerical/dif.hpp:166-186): out = (cur_d + id)(x + new_d) - x where new_d is
+// non-zero and the sample lands inside, else cur_d.  The mapping cur_d + id is
+// formed per corner exactly as displacement_to_mapping stores it.
+__global__ void __launch_bounds__(kCdmThreads) cdm_accumulate_kernel(const CdmSeg* __restrict__ segs)
+{
+    SEG_BEGIN
+    const CdmCtl* c = S.ctl;
+    if (c->done)
+        return;
+    const float scale = c->scale;
+    const float* __restrict__ nd = S.aux_d;
+    const float* __restrict__ cd = S.cur_d;
+    float* __restrict__ out = S.tmp_d;
+    const int w = D.w, wh = D.wh();
+    for (long long i = first; i < n; i += stride) {
+        float dx = nd[3 * i] * scale, dy = nd[3 * i + 1] * scale, dz = nd[3 * i + 2] * scale;
+        int x, y, z;
+        unflat((int)i, D, x, y, z);
+        bool ok = false;
+        if (dx != 0.0f || dy != 0.0f || dz != 0.0f) {
+            dx += (float)x;
+            dy += (float)y;
+            dz += (float)z;
+            Cell cl;
+            if (trilinear_cell(D, dx, dy, dz, cl)) {
+                const int b = cl.base;
+                const int bx = b % w, by = (b / w) % D.h, bz = b / wh;
+                const int off[8] = {0, 1, w, w + 1, wh, wh + 1, wh + w, wh + w + 1};
+                const int ox[8] = {0, 1, 0, 1, 0, 1, 0, 1};
+                const int oy[8] = {0, 0, 1, 1, 0, 0, 1, 1};
+                const int oz[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+                float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const float* q = cd + 3LL * (b + off[k]);
+                    const float mx = q[0] + (float)(bx + ox[k]);
+                    const float my = q[1] + (float)(by + oy[k]);
+                    const float mz = q[2] + (float)(bz + oz[k]);
+                    if (k == 0) {
+                        ax = mx * cl.r[0];
+                        ay = my * cl.r[0];
+                        az = mz * cl.r[0];
+                    } else {
+                        ax += mx * cl.r[k];
+                        ay += my * cl.r[k];
+                        az += mz * cl.r[k];
+                    }
+                }
+                out[3 * i] = ax - (float)x;
+                out[3 * i + 1] = ay - (float)y;
+                out[3 * i + 2] = az - (float)z;
+                ok = true;
+            }
+        }
+        if (!ok) {
+            out[3 * i] = cd[3 * i];
+            out[3 * i + 1] = cd[3 * i + 1];
+            out[3 * i + 2] = cd[3 * i + 2];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ smooth
+// cdm_smooth (reg/cdm.hpp:302-366): cur_d = d*(1-s) + (s/6) * (d[+1] + d[-1] +
+// d[+w] + d[-w] + d[+wh] + d[-wh]) by flat index; s == 0 leaves cur_d as it is.
+__global__ void __launch_bounds__(kCdmThreads) cdm_smooth_kernel(const CdmSeg* __restrict__ segs)
+{
+    SEG_BEGIN
+    const CdmCtl* c = S.ctl;
+    if (c->done)
+        return;
+    const float sm = c->cur_smoothing;
+    if (sm == 0.0f)
+        return;
+    const float w_6 = sm / (2.0f * 3.0f);
+    const float w_1 = 1.0f - sm;
+    const float* __restrict__ d = S.tmp_d;
+    float* __restrict__ dd = S.cur_d;
+    const long long w = D.w, wh = D.wh();
+    for (long long p = first; p < n; p += stride) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float v = 0.0f;
+            if (p + 1 < n) v += d[3 * (p + 1) + k];
+            if (p >= 1) v += d[3 * (p - 1) + k];
+            if (p + w < n) v += d[3 * (p + w) + k];
+            if (p >= w) v += d[3 * (p - w) + k];
+            if (p + wh < n) v += d[3 * (p + wh) + k];
+            if (p >= wh) v += d[3 * (p - wh) + k];
+            v *= w_6;
+            dd[3 * p + k] = d[3 * p + k] * w_1 + v;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ pyramid
+// downsample_with_padding (numerical/resampling.hpp:575-603): 2x box mean; a
+// missing +1 neighbour repeats the nearest present one; integer pixels sum in
+// 16 bits and shift by 3, float pixels divide by 8.
+template <typename T>
+__global__ void downsample_kernel(const T* __restrict__ in, Dim3 di, T* __restrict__ out, Dim3 dout)
+{
+    const long long n = dout.n();
+    const long long w = di.w, wh = (long long)di.wh();
+    const long long shift[8] = {0, 1, w, 1 + w, wh, wh + 1, wh + w, wh + 1 + w};
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        unflat((int)o, dout, x, y, z);
+        const int x2 = 2 * x, y2 = 2 * y, z2 = 2 * z;
+        int has = 0;
+        if (x2 + 1 < di.w) has += 1;
+        if (y2 + 1 < di.h) has += 2;
+        if (z2 + 1 < di.d) has += 4;
+        const long long base = ((long long)z2 * di.h + y2) * di.w + x2;
+        T buf[8];
+        buf[0] = in[base];
+        if constexpr (sizeof(T) == 1) {
+            unsigned int acc = buf[0];
+#pragma unroll
+            for (int k = 1; k < 8; ++k) {
+                const int h = has & k;
+                buf[k] = (h == k) ? in[base + shift[k]] : buf[h];
+                acc = (acc + buf[k]) & 0xffffu;
+            }
+            out[o] = (T)(acc >> 3);
+        } else {
+            T acc = buf[0];
+#pragma unroll
+            for (int k = 1; k < 8; ++k) {
+                const int h = has & k;
+                buf[k] = (h == k) ? in[base + shift[k]] : buf[h];
+                acc += buf[k];
+            }
+            out[o] = acc / 8;
+        }
+    }
+}
+
+cudaError_t launch_downsample(const void* in, void* out, int w, int h, int d, int pix, cudaStream_t st)
+{
+    Dim3 di{w, h, d}, dout{(w + 1) / 2, (h + 1) / 2, (d + 1) / 2};
+    int blocks = cdm_blocks_for(dout.n());
+    if (pix == 0)
+        downsample_kernel<uint8_t><<<blocks, kCdmThreads, 0, st>>>((const uint8_t*)in, di, (uint8_t*)out, dout);
+    else
+        downsample_kernel<float><<<blocks, kCdmThreads, 0, st>>>((const float*)in, di, (float*)out, dout);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// best_d *= 2; upsample_with_padding (reg/cdm.hpp:402-403,
+// numerical/resampling.hpp:849-891): out(x) = trilinear(2*in, x * 0.5), 0 where the
+// sample fails.  The doubling is exact, so it is applied to the corner values.
+__global__ void upsample_x2_kernel(const float* __restrict__ in, Dim3 di, float* __restrict__ out, Dim3 dout)
+{
+    const long long n = dout.n();
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        unflat((int)o, dout, x, y, z);
+        float vx = (float)x, vy = (float)y, vz = (float)z;
+        vx *= 0.5f;
+        vy *= 0.5f;
+        vz *= 0.5f;
+        Cell c;
+        float3 v = make_float3(0.f, 0.f, 0.f);
+        if (trilinear_cell(di, vx, vy, vz, c)) {
+            const int w = di.w, wh = di.wh(), b = c.base;
+            const int off[8] = {0, 1, w, w + 1, wh, wh + 1, wh + w, wh + w + 1};
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float* q = in + 3LL * (b + off[k]);
+                const float qx = q[0] * 2.0f, qy = q[1] * 2.0f, qz = q[2] * 2.0f;
+                if (k == 0) {
+                    v.x = qx * c.r[0];
+                    v.y = qy * c.r[0];
+                    v.z = qz * c.r[0];
+                } else {
+                    v.x += qx * c.r[k];
+                    v.y += qy * c.r[k];
+                    v.z += qz * c.r[k];
+                }
+            }
+        }
+        out[3 * o] = v.x;
+        out[3 * o + 1] = v.y;
+        out[3 * o + 2] = v.z;
+    }
+}
+
+cudaError_t launch_upsample_field_x2(const float* in, int iw, int ih, int id, float* out, int ow, int oh, int od,
+                                     cudaStream_t st)
+{
+    Dim3 di{iw, ih, id}, dout{ow, oh, od};
+    upsample_x2_kernel<<<cdm_blocks_for(dout.n()), kCdmThreads, 0, st>>>(in, di, out, dout);
+    count_launch();
+    return cudaGetLastError();
+}
+
+__global__ void cost_mean_kernel(const CdmSeg* __restrict__ segs, float* __restrict__ out)
+{
+    const float m = seg_cost_mean(segs[blockIdx.y]);
+    if (threadIdx.x == 0)
+        out[blockIdx.y] = m;
+}
+
+cudaError_t launch_cost_mean(const CdmSeg* segs, int nseg, float* out, cudaStream_t st)
+{
+    cost_mean_kernel<<<dim3(1, nseg), 256, 0, st>>>(segs, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ launchers
+#define SEG_GRID dim3(blocks, nseg)
+
+cudaError_t launch_cdm_compose(const CdmSeg* segs, int nseg, int blocks, int pix, cudaStream_t st)
+{
+    if (pix == 0)
+        cdm_compose_kernel<uint8_t><<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+    else
+        cdm_compose_kernel<float><<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cdm_gradient(const CdmSeg* segs, int nseg, int blocks, int pix, int gradient_type,
+                                cudaStream_t st)
+{
+    if (pix == 0)
+        cdm_gradient_kernel<uint8_t><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, gradient_type);
+    else
+        cdm_gradient_kernel<float><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, gradient_type);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cdm_control(const CdmSeg* segs, int nseg, int, cudaStream_t st)
+{
+    cdm_control_kernel<<<dim3(1, nseg), 256, 0, st>>>(segs);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cdm_best_copy(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st)
+{
+    cdm_best_copy_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cdm_poisson(const CdmSeg* segs, int nseg, int blocks, int sweeps, cudaStream_t st)
+{
+    cdm_poisson_init_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+    for (int k = 0; k < sweeps; ++k)
+        cdm_poisson_sweep_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs, k & 1);
+    count_launch(sweeps);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cdm_theta(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st)
+{
+    cdm_theta_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cdm_accumulate(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st)
+{
+    cdm_accumulate_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cdm_smooth(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st)
+{
+    cdm_smooth_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace regb

@@ -1,0 +1,24 @@
+// Device state of one CDM level of one job (fields, scratch, control block).
+#pragma once
+#include "host.h"
+
+namespace regb {
+
+struct CdmLevel {
+    int pix = 0;
+    CdmSeg seg{};
+    CdmCtl h_ctl{};
+    DevBuf<uint8_t> js;
+    DevBuf<float> cur, nd, aux, tmp;
+    DevBuf<double> part;
+    DevBuf<CdmCtl> ctl;
+    DevBuf<CdmSeg> d_seg;
+    // best is the level's in/out field (starts as the upsampled coarser result).
+    void init(const void* It, const void* Is, int w, int h, int d, int pix, const regb_cdm_param& p, float* best,
+              cudaStream_t st);
+};
+
+// One iteration of every segment in d_segs (reg/cdm.hpp:418-470).
+void launch_iteration(const CdmSeg* d_segs, int nseg, int blocks, int pix, int gradient_type, cudaStream_t st);
+
+}  // namespace regb

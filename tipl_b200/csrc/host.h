@@ -1,0 +1,150 @@
+// Host-side runtime shared by the drivers and the C ABI: error reporting, device
+// buffers on the stream-ordered allocator, the transform algebra.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include "../../include/regb200.h"
+#include "kernels.h"
+
+namespace regb {
+
+// Carries a regb_status out of deep host code; caught at the ABI boundary.
+struct Failure : std::runtime_error {
+    regb_status code;
+    Failure(regb_status c, const std::string& what) : std::runtime_error(what), code(c) {}
+};
+
+void set_last_error(const std::string& s);
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what);
+
+#define REGB_CK(x)                                  \
+    do {                                            \
+        cudaError_t e_ = (x);                       \
+        if (e_ != cudaSuccess)                      \
+            ::regb::throw_cuda(e_, #x);             \
+    } while (0)
+
+void ensure_device();  // pool release threshold etc., once per device
+
+// A device buffer from the stream-ordered pool (cudaMallocAsync); freed on the
+// same stream, so reuse is ordered without device-wide synchronisation.
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t st = nullptr;
+    DevBuf() = default;
+    DevBuf(size_t count, cudaStream_t s) { alloc(count, s); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), st(o.st) { o.p = nullptr; o.n = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept
+    {
+        if (this != &o) {
+            reset();
+            p = o.p;
+            n = o.n;
+            st = o.st;
+            o.p = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
+    void alloc(size_t count, cudaStream_t s)
+    {
+        reset();
+        ensure_device();
+        st = s;
+        n = count;
+        if (count) {
+            cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), s);
+            if (e != cudaSuccess) {
+                p = nullptr;
+                n = 0;
+                (void)cudaGetLastError();
+                throw Failure(REGB_ERR_NOMEM, std::string("device allocation failed: ") + cudaGetErrorString(e));
+            }
+        }
+    }
+    void zero() { REGB_CK(cudaMemsetAsync(p, 0, n * sizeof(T), st)); }
+    void reset()
+    {
+        if (p)
+            cudaFreeAsync(p, st);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { reset(); }
+};
+
+// Pinned host staging buffer.
+template <typename T>
+struct PinBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    PinBuf() = default;
+    explicit PinBuf(size_t c) { alloc(c); }
+    PinBuf(const PinBuf&) = delete;
+    PinBuf& operator=(const PinBuf&) = delete;
+    void alloc(size_t c)
+    {
+        if (c <= n)
+            return;
+        reset();
+        REGB_CK(cudaMallocHost((void**)&p, c * sizeof(T)));
+        n = c;
+    }
+    void reset()
+    {
+        if (p)
+            cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~PinBuf() { reset(); }
+};
+
+// Owns a non-blocking stream.
+struct Stream {
+    cudaStream_t s = nullptr;
+    Stream() { REGB_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+    ~Stream()
+    {
+        if (s)
+            cudaStreamDestroy(s);
+    }
+    Stream(const Stream&) = delete;
+    Stream& operator=(const Stream&) = delete;
+    void sync() { REGB_CK(cudaStreamSynchronize(s)); }
+};
+
+size_t pix_size(int dtype);
+
+// ---- transform algebra (numerical/transformation.hpp) ----
+void affine_to_matrix(const float* param, const int* from_dim, const float* from_vs, const int* to_dim,
+                      const float* to_vs, float* T);
+void affine_to_matrix_f64(const double* param, const int* from_dim, const double* from_vs, const int* to_dim,
+                          const double* to_vs, double* T);
+bool matrix_inverse(float* T);
+bool integer_shift(const float* T, int* shift);
+
+// ---- whole-registration drivers ----
+struct LinearResult {
+    float cost = 0.0f;
+    long long evals = 0;
+};
+// The affine search of tipl::reg::linear on device-resident uint8 volumes.
+LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
+                             const int* tdim, const float* to_vs, float* arg, const regb_linear_param& p,
+                             volatile const int* terminated, cudaStream_t st);
+
+// The CDM driver (reg/cdm.hpp:373-474) on device-resident images; d_field receives
+// the full-resolution field.  Returns REGB_OK, REGB_FALSE or REGB_CANCELLED.
+regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int pix, float* d_field,
+                         const regb_cdm_param& p, volatile const int* terminated, cudaStream_t st,
+                         int* iterations = nullptr);
+
+}  // namespace regb

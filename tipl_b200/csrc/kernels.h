@@ -1,0 +1,111 @@
+// Internal (C++) interface between the host drivers and the CUDA kernels.
+// Nothing here is part of the C ABI (include/regb200.h).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#ifdef __CUDACC__
+#define REGB_HD __host__ __device__
+#else
+#define REGB_HD
+#endif
+
+namespace regb {
+
+struct Dim3 {
+    int w, h, d;
+    REGB_HD long long n() const { return (long long)w * h * d; }
+    REGB_HD int wh() const { return w * h; }
+};
+
+// One affine cost evaluation: a (job, candidate transform) pair.  All pointers are
+// device pointers.  hist/moments/ticket are per-task scratch that must be zero on
+// entry; the kernel's last block re-zeroes them.
+struct AffineTask {
+    const uint8_t* fixed;   // the grid the cost is summed over (template)
+    const uint8_t* moving;  // the sampled volume
+    Dim3 fd;                // fixed extent
+    Dim3 md;                // moving extent
+    float T[12];            // fixed voxel -> moving voxel (sr row-major, shift)
+    int mode;               // 0 trilinear, 1 integer-shift copy (correlation only)
+    int keep;               // MI: 1 = leave the counts in hist (no reduction, no clearing)
+    int shift[3];
+    int nchunk;             // voxel chunks of this task
+    int chunk;              // voxels per chunk
+    uint32_t* hist;                // MI: 65536 counters
+    const int32_t* row_hist;       // MI: template value histogram (256)
+    unsigned long long* moments;   // correlation: sum y, sum y^2, sum x*y
+    long long sx, sxx;             // correlation: template sum x, sum x^2
+    unsigned int* ticket;          // blocks finished
+    double* cost;                  // output
+};
+
+// Device control block of one CDM level of one job (the reference's host-side
+// loop state, reg/cdm.hpp:408-470, kept on the device so iterations need no host
+// round trip).
+struct CdmCtl {
+    float cost[8];
+    int ncost;
+    float best_cost;
+    float cur_smoothing;
+    float theta;
+    float scale;           // speed / theta
+    float speed;
+    float smoothing;       // cdm_param::smoothing (the stop threshold)
+    int index;             // iteration of this level
+    int max_iter;          // 200
+    int done;              // 1 = loop left (break / iteration cap / theta 0), 2 = zero cost (failure)
+    int save_best;         // this iteration: best_d <- cur_d
+    int restore;           // this iteration: cur_d <- best_d
+    unsigned int theta_bits;  // max |new_d| of the first iteration (float bits)
+    unsigned int ticket;
+    float last_cost;
+    int iters_run;
+};
+
+// One CDM job level as seen by the iteration kernels (blockIdx.y = segment).
+struct CdmSeg {
+    int w, h, d;
+    int nblk;         // blocks this segment uses (a function of its size only, so a
+                      // job's reduction order does not depend on what it is batched with)
+    const void* It;   // template (fixed) image at this level
+    const void* Is;   // subject (moving) image at this level
+    void* Js;         // composed subject (scratch, pixel type)
+    float* cur_d;     // current field
+    float* best_d;    // best field
+    float* new_d;     // gradient -> Poisson result (scratch)
+    float* aux_d;     // Poisson iterate A / Poisson result (scratch)
+    float* tmp_d;     // Poisson iterate B / accumulated field (scratch)
+    double* cost_part;  // per-block partial cost sums (nblk entries)
+    CdmCtl* ctl;
+};
+
+template <typename T>
+cudaError_t launch_resample(const T* from, Dim3 fd, T* to, Dim3 td, const float* Tm, const int* shift,
+                            cudaStream_t st);
+cudaError_t launch_mi(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
+cudaError_t launch_corr(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
+cudaError_t launch_fixed_stats(const uint8_t* f, long long n, int32_t* hist, unsigned long long* sums,
+                               cudaStream_t st);
+
+// CDM passes.  pix: 0 = uint8, 1 = float.  segs is a device array of nseg segments;
+// blocks is gridDim.x per segment.
+cudaError_t launch_cdm_compose(const CdmSeg* segs, int nseg, int blocks, int pix, cudaStream_t st);
+cudaError_t launch_cdm_gradient(const CdmSeg* segs, int nseg, int blocks, int pix, int gradient_type,
+                                cudaStream_t st);
+cudaError_t launch_cdm_control(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st);
+cudaError_t launch_cdm_best_copy(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st);
+cudaError_t launch_cdm_poisson(const CdmSeg* segs, int nseg, int blocks, int sweeps, cudaStream_t st);
+cudaError_t launch_cdm_theta(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st);
+cudaError_t launch_cdm_accumulate(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st);
+cudaError_t launch_cdm_smooth(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st);
+
+// Pyramid passes (single volume, device pointers).
+cudaError_t launch_downsample(const void* in, void* out, int w, int h, int d, int pix, cudaStream_t st);
+cudaError_t launch_upsample_field_x2(const float* in, int iw, int ih, int id, float* out, int ow, int oh, int od,
+                                     cudaStream_t st);
+// Sum of a segment's cost partials -> float mean (the reference's mean(cost_map)).
+cudaError_t launch_cost_mean(const CdmSeg* segs, int nseg, float* out, cudaStream_t st);
+int cdm_blocks_for(long long nvox);
+
+}  // namespace regb

@@ -1,0 +1,99 @@
+#include "stats.h"
+#include <mutex>
+#include <vector>
+#include "../../include/regb200.h"
+
+namespace regb {
+
+std::atomic<long long> g_launches{0};
+
+namespace {
+struct Pending {
+    cudaEvent_t a, b;
+    int kind;
+    long long tasks;
+    double voxels, bytes;
+};
+std::mutex g_m;
+std::atomic<int> g_timing{0};
+std::vector<Pending> g_pending;
+regb_stats g_acc{};
+
+void drain_locked()
+{
+    for (auto& p : g_pending) {
+        float ms = 0.0f;
+        if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            if (p.kind == 0) {
+                g_acc.mi_launches += 1;
+                g_acc.mi_tasks += p.tasks;
+                g_acc.mi_voxels += p.voxels;
+                g_acc.mi_bytes += p.bytes;
+                g_acc.mi_ms += ms;
+            } else {
+                g_acc.corr_launches += 1;
+                g_acc.corr_tasks += p.tasks;
+                g_acc.corr_voxels += p.voxels;
+                g_acc.corr_bytes += p.bytes;
+                g_acc.corr_ms += ms;
+            }
+        }
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    g_pending.clear();
+    (void)cudaGetLastError();
+}
+}  // namespace
+
+void KernelTimer::begin(cudaStream_t st, int k)
+{
+    on = g_timing.load() != 0;
+    kind = k;
+    if (!on)
+        return;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+        on = false;
+        (void)cudaGetLastError();
+        return;
+    }
+    cudaEventRecord(a, st);
+}
+
+void KernelTimer::end(cudaStream_t st, long long tasks, double voxels, double bytes)
+{
+    if (!on)
+        return;
+    cudaEventRecord(b, st);
+    std::lock_guard<std::mutex> g(g_m);
+    g_pending.push_back({a, b, kind, tasks, voxels, bytes});
+}
+
+}  // namespace regb
+
+using namespace regb;
+
+extern "C" {
+
+regb_status regb_stats_reset(int timing)
+{
+    std::lock_guard<std::mutex> g(g_m);
+    drain_locked();
+    g_acc = regb_stats{};
+    g_launches.store(0);
+    g_timing.store(timing ? 1 : 0);
+    return REGB_OK;
+}
+
+regb_status regb_stats_get(regb_stats* out)
+{
+    if (!out)
+        return REGB_ERR_ARG;
+    std::lock_guard<std::mutex> g(g_m);
+    drain_locked();
+    *out = g_acc;
+    out->launches = g_launches.load();
+    return REGB_OK;
+}
+
+}  // extern "C"
