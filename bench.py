@@ -163,6 +163,27 @@ def run_reference(args):
     return 0
 
 
+def kernel_case(args):
+    """Three launches of one cost kernel on the full-size pair, K candidates each."""
+    import torch
+
+    import tipl_b200 as tb
+    from tipl_b200 import phantom as ph
+
+    f8, m8, _ = make_pair(0)
+    fd = torch.from_numpy(f8).cuda()
+    md = torch.from_numpy(m8).cuda()
+    rng = np.random.default_rng(1)
+    Ts = np.array([tb.affine_to_matrix(ph.random_affine(rng, rot_deg=5, trans_vox=3), SHAPE, VS, SHAPE, VS)
+                   for _ in range(args.k)], np.float32)
+    fn = tb.mi_cost if args.kernel_case == "mi" else tb.corr_cost
+    for _ in range(3):
+        c = fn(fd, md, Ts)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": args.kernel_case, "k": args.k, "cost0": float(c[0])}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -172,9 +193,14 @@ def main():
     ap.add_argument("--mode", default="plain", choices=["plain", "served"])
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-case", choices=["mi", "corr"], default=None,
+                    help="run only K-candidate cost batches of the full-size pair (for profiler captures)")
+    ap.add_argument("--k", type=int, default=12)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernel_case:
+        return kernel_case(args)
 
     import torch
 
