@@ -133,6 +133,20 @@ regb_status regb_resample(const regb_volume* from, regb_volume* to, const float 
  * hist_out (optional, host, K*65536 int32) receives the joint histograms. */
 regb_status regb_mi_cost(const regb_volume* fixed, const regb_volume* moving, const float* T, int K,
                          double* cost, int32_t* hist_out, void* stream);
+/* No counterpart in the reference.  The MI cost of regb_mi_cost for callers that
+ * cannot allocate device memory -- a processing callback inside a host application
+ * that owns all device memory through its own pool, or a latency-critical loop that
+ * must not take the device-wide synchronisation cudaMalloc/cudaFree can cause.
+ * fixed/moving are uint8 DEVICE pointers (dims w,h,d), T is K host transforms, cost
+ * is a DEVICE array of K doubles.  Nothing is allocated: all scratch lives in one
+ * file-scope device array (4 MiB of joint histograms plus a few KiB), so K <= 16 and
+ * larger K is rejected with REGB_ERR_ARG.  The first call on a device looks up that
+ * array's device address, so make that first call before any stream capture.
+ * Every call shares the array: calls that overlap on the GPU (different streams or
+ * host threads without ordering) race and give wrong costs.  Returns after the costs
+ * are written. */
+regb_status regb_mi_cost_noalloc(const uint8_t* fixed, const int fixed_dim[3], const uint8_t* moving,
+                                 const int moving_dim[3], const float* T, int K, double* cost, void* stream);
 /* correlation::operator() (reg/linear.hpp:23-78) for K transforms: 1 - r^2 with the
  * smaller volume as the grid (transform inverted when the roles swap). */
 regb_status regb_corr_cost(const regb_volume* fixed, const regb_volume* moving, const float* T, int K,
