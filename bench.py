@@ -177,10 +177,22 @@ def kernel_case(args):
     Ts = np.array([tb.affine_to_matrix(ph.random_affine(rng, rot_deg=5, trans_vox=3), SHAPE, VS, SHAPE, VS)
                    for _ in range(args.k)], np.float32)
     fn = tb.mi_cost if args.kernel_case == "mi" else tb.corr_cost
+    from tipl_b200 import _lib
+
+    L = _lib.lib()
     for _ in range(3):
         c = fn(fd, md, Ts)
+    L.regb_stats_reset(1)
+    for _ in range(10):
+        c = fn(fd, md, Ts)
+    st = _lib.Stats()
+    L.regb_stats_get(st)
     torch.cuda.synchronize()
-    print(json.dumps({"kernel_case": args.kernel_case, "k": args.k, "cost0": float(c[0])}))
+    ms = (st.mi_ms / max(1, st.mi_launches)) if args.kernel_case == "mi" else (st.corr_ms / max(1, st.corr_launches))
+    vox = (st.mi_voxels / max(1, st.mi_launches)) if args.kernel_case == "mi" else (
+        st.corr_voxels / max(1, st.corr_launches))
+    print(json.dumps({"kernel_case": args.kernel_case, "k": args.k, "cost0": float(c[0]), "ms_per_launch": ms,
+                      "voxel_evals_per_s": vox / (ms / 1000.0)}))
     return 0
 
 

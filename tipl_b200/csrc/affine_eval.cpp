@@ -27,17 +27,20 @@ void TaskScratch::ensure(int k, bool need_hist, cudaStream_t st)
 
 void set_task_chunks(AffineTask& t, int cost_type)
 {
-    const long long n = t.fd.n();
-    long long chunk;
+    // a chunk is a run of whole rows of the fixed grid
+    const long long w = t.fd.w, rows = (long long)t.fd.h * t.fd.d;
+    long long rpc;
     if (cost_type == REGB_COST_MI) {
-        // 16-bit per-block counters: at most 65535 voxels per block.
-        chunk = (n + 147) / 148;
-        chunk = std::max<long long>(chunk, 32768);
-        chunk = std::min<long long>(chunk, 65535);
+        // 16-bit per-block counters: at most 65535 voxels per block; about one block
+        // per SM for a large grid, at least 32K voxels per block for a small one.
+        const long long hi = std::max<long long>(1, 65535 / w);
+        rpc = (rows + 147) / 148;
+        rpc = std::max<long long>(rpc, (32768 + w - 1) / w);
+        rpc = std::min<long long>(rpc, hi);
     } else
-        chunk = 32768;
-    t.chunk = (int)chunk;
-    t.nchunk = (int)std::max<long long>(1, (n + chunk - 1) / chunk);
+        rpc = std::max<long long>(1, (32768 + w - 1) / w);
+    t.chunk = (int)rpc;
+    t.nchunk = (int)std::max<long long>(1, (rows + rpc - 1) / rpc);
 }
 
 void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, double* out)

@@ -87,7 +87,7 @@ template cudaError_t launch_resample<float>(const float*, Dim3, float*, Dim3, co
 // kMiChunkMax voxels, so no 16-bit counter can overflow.  Bin 0 (template 0,
 // moving sample 0 -- the background) is not counted at all: its count is the
 // voxel total minus every other bin, recovered in the reduction.
-constexpr int kMiThreads = 1024;
+constexpr int kMiThreads = 768;  // 80 registers a thread at one block per SM
 constexpr int kMiSmemWords = 32768;
 
 __device__ __forceinline__ void mi_count(uint32_t* sh, uint32_t bin)
@@ -111,11 +111,11 @@ __device__ void mi_reduce_and_clear(uint32_t* __restrict__ hist, const int32_t* 
     if (t == 0)
         *tot = 0ull;
     __syncthreads();
-    // column partial sums: thread t covers column (t & 255), rows [64*(t>>8), +64)
+    // column partial sums: thread t covers column (t & 255), every (blockDim/256)-th row
     {
-        const int j = t & 255, r0 = (t >> 8) * 64;
+        const int j = t & 255, rstep = blockDim.x >> 8;
         uint32_t s = 0;
-        for (int r = r0; r < r0 + 64; ++r)
+        for (int r = t >> 8; r < 256; r += rstep)
             s += __ldcg(hist + r * 256 + j);
         atomicAdd(col + j, s);
         unsigned long long ss = s;
@@ -154,22 +154,43 @@ __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __r
     for (int i = threadIdx.x * 4; i < kMiSmemWords; i += blockDim.x * 4)
         *reinterpret_cast<uint4*>(sh + i) = make_uint4(0, 0, 0, 0);
     __syncthreads();
-    const Dim3 fd = tk.fd, md = tk.md;
+    const Dim3 fd = tk.fd;
+    const SampleGeo g = sample_geo(tk.md);
     const long long n = fd.n();
-    const long long v0 = (long long)chunk * tk.chunk;
-    const long long v1 = min(n, v0 + tk.chunk);
-    const uint8_t* __restrict__ fixed = tk.fixed;
+    // a chunk is a run of whole rows (y, z); warps take rows, lanes take x
+    const int rows = fd.h * fd.d;
+    const int r0 = chunk * tk.chunk, r1 = min(rows, r0 + tk.chunk);
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const uint8_t* __restrict__ moving = tk.moving;
-    for (long long i = v0 + threadIdx.x; i < v1; i += blockDim.x) {
-        int x, y, z;
-        unflat((int)i, fd, x, y, z);
-        float px, py, pz;
-        apply_xform(tk.T, (float)x, (float)y, (float)z, px, py, pz);
-        Cell c;
-        uint32_t to8 = 0;
-        if (trilinear_cell(md, px, py, pz, c))
-            to8 = assign_pix<uint8_t>(cell_sum(moving, md, c));
-        mi_count(sh, ((uint32_t)__ldg(fixed + i) << 8) | to8);
+    const float* __restrict__ T = tk.T;
+    ColXform cx;
+    cx.set(T);
+    // two rows per warp at a time: the second row's corner loads overlap the first's
+    for (int r = r0 + (threadIdx.x >> 5); r < r1; r += 2 * nw) {
+        const int rb = r + nw;
+        const bool two = rb < r1;
+        RowXform xa, xb;
+        xa.set(T, r % fd.h, r / fd.h);
+        xb.set(T, (two ? rb : r) % fd.h, (two ? rb : r) / fd.h);
+        const uint8_t* __restrict__ fa = tk.fixed + (long long)r * fd.w;
+        const uint8_t* __restrict__ fb = tk.fixed + (long long)(two ? rb : r) * fd.w;
+        float fx = (float)lane;
+        for (int x = lane; x < fd.w; x += 32, fx += 32.0f) {
+            float px, py, pz;
+            U8Sample A, B;
+            xa.at(cx, fx, px, py, pz);
+            A.prepare(moving, g, px, py, pz);
+            xb.at(cx, fx, px, py, pz);
+            B.prepare(moving, g, px, py, pz);
+            B.ok = B.ok && two;
+            const uint32_t fva = __ldg(fa + x);
+            const uint32_t fvb = two ? (uint32_t)__ldg(fb + x) : 0u;
+            A.load(g);
+            B.load(g);
+            mi_count(sh, (fva << 8) | A.finish());
+            if (two)
+                mi_count(sh, (fvb << 8) | B.finish());
+        }
     }
     __syncthreads();
     // flush non-zero counters to the task's global histogram
@@ -231,31 +252,38 @@ __global__ void __launch_bounds__(kCorrThreads) corr_kernel(const AffineTask* __
     if (chunk >= tk.nchunk)
         return;
     const Dim3 fd = tk.fd, md = tk.md;
+    const SampleGeo g = sample_geo(md);
     const long long n = fd.n();
-    const long long v0 = (long long)chunk * tk.chunk;
-    const long long v1 = min(n, v0 + tk.chunk);
-    const uint8_t* __restrict__ fixed = tk.fixed;
+    const int rows = fd.h * fd.d;
+    const int r0 = chunk * tk.chunk, r1 = min(rows, r0 + tk.chunk);
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const uint8_t* __restrict__ moving = tk.moving;
+    const float* __restrict__ T = tk.T;
+    ColXform cx;
+    cx.set(T);
     uint32_t sy = 0, syy = 0, sxy = 0;
-    for (long long i = v0 + threadIdx.x; i < v1; i += blockDim.x) {
-        int x, y, z;
-        unflat((int)i, fd, x, y, z);
-        uint32_t v = 0;
-        if (tk.mode == 1) {
-            int fx = x + tk.shift[0], fy = y + tk.shift[1], fz = z + tk.shift[2];
-            if (fx >= 0 && fy >= 0 && fz >= 0 && fx < md.w && fy < md.h && fz < md.d)
-                v = __ldg(moving + (fz * md.h + fy) * md.w + fx);
-        } else {
-            float px, py, pz;
-            apply_xform(tk.T, (float)x, (float)y, (float)z, px, py, pz);
-            Cell c;
-            if (trilinear_cell(md, px, py, pz, c))
-                v = assign_pix<uint8_t>(cell_sum(moving, md, c));
+    for (int r = r0 + (threadIdx.x >> 5); r < r1; r += nw) {
+        const int yy = r % fd.h, zz = r / fd.h;
+        RowXform rx;
+        rx.set(T, yy, zz);
+        const uint8_t* __restrict__ frow = tk.fixed + (long long)r * fd.w;
+        float fx = (float)lane;
+        for (int x = lane; x < fd.w; x += 32, fx += 32.0f) {
+            uint32_t v = 0;
+            if (tk.mode == 1) {
+                const int ax = x + tk.shift[0], ay = yy + tk.shift[1], az = zz + tk.shift[2];
+                if (ax >= 0 && ay >= 0 && az >= 0 && ax < md.w && ay < md.h && az < md.d)
+                    v = __ldg(moving + (az * md.h + ay) * md.w + ax);
+            } else {
+                float px, py, pz;
+                rx.at(cx, fx, px, py, pz);
+                v = sample_u8(moving, g, px, py, pz);
+            }
+            const uint32_t f = __ldg(frow + x);
+            sy += v;
+            syy += v * v;
+            sxy += f * v;
         }
-        uint32_t f = __ldg(fixed + i);
-        sy += v;
-        syy += v * v;
-        sxy += f * v;
     }
     __shared__ unsigned long long red[32];
     unsigned long long a = block_sum<unsigned long long>(sy, red);

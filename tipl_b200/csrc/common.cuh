@@ -112,6 +112,154 @@ __device__ __forceinline__ float3 cell_sum_vec(const float* __restrict__ F, cons
     return acc;
 }
 
+// ---- exact conversions on the FP/ALU pipes (the conversion unit is the
+// bottleneck of the sampling loops otherwise) ----
+constexpr float kTwo23 = 8388608.0f;
+
+// float(v) for 0 <= v < 2^23: the bits of 2^23 + v, minus 2^23 (both steps exact).
+__device__ __forceinline__ float u8_to_f(uint32_t v) { return __uint_as_float(0x4B000000u | v) - kTwo23; }
+
+// floor(x) for 0 <= x < 2^23: x + 2^23 rounded toward zero is 2^23 + floor(x);
+// returns floor(x) as float and sets i to it as an integer.
+__device__ __forceinline__ float floor_pos(float x, int& i)
+{
+    const float r = __fadd_rz(x, kTwo23);
+    i = __float_as_int(r) - 0x4B000000;
+    return r - kTwo23;
+}
+
+// Extent of a sampled volume with the float upper limits of the cell test.
+struct SampleGeo {
+    int w, h, wh;
+    float wl, hl, dl;  // w-1, h-1, d-1
+};
+__device__ __forceinline__ SampleGeo sample_geo(const Dim3& D)
+{
+    return SampleGeo{D.w, D.h, D.w * D.h, (float)(D.w - 1), (float)(D.h - 1), (float)(D.d - 1)};
+}
+
+// The reference's uint8 trilinear estimate (interpolation.hpp:337-383 with the
+// uint8 assign of 28-34) at (x, y, z); 0 where the cell test fails.  Same values as
+// trilinear_cell + cell_sum + assign_pix<uint8_t>, with every float<->int
+// conversion done by the exact tricks above.
+__device__ __forceinline__ uint32_t sample_u8(const uint8_t* __restrict__ I, const SampleGeo& g, float x, float y,
+                                              float z)
+{
+    if (x < 0.0f || y < 0.0f || z < 0.0f)
+        return 0u;
+    if (!(x < g.wl) || !(y < g.hl) || !(z < g.dl))
+        return 0u;
+    int ix, iy, iz;
+    const float fx = floor_pos(x, ix), fy = floor_pos(y, iy), fz = floor_pos(z, iz);
+    const float p0 = x - fx, p1 = y - fy, p2 = z - fz;
+    const float n0 = 1.0f - p0, n1 = 1.0f - p1, n2 = 1.0f - p2;
+    const float n0n1 = n0 * n1, p0n1 = p0 * n1, n0p1 = n0 * p1, p0p1 = p0 * p1;
+    const uint8_t* q = I + ((iz * g.h + iy) * g.w + ix);
+    const int w = g.w, wh = g.wh;
+    float acc = u8_to_f(__ldg(q)) * (n0n1 * n2);
+    acc += u8_to_f(__ldg(q + 1)) * (p0n1 * n2);
+    acc += u8_to_f(__ldg(q + w)) * (n0p1 * n2);
+    acc += u8_to_f(__ldg(q + w + 1)) * (p0p1 * n2);
+    acc += u8_to_f(__ldg(q + wh)) * (n0n1 * p2);
+    acc += u8_to_f(__ldg(q + wh + 1)) * (p0n1 * p2);
+    acc += u8_to_f(__ldg(q + wh + w)) * (n0p1 * p2);
+    acc += u8_to_f(__ldg(q + wh + w + 1)) * (p0p1 * p2);
+    if (acc <= 0.0f)
+        return 0u;
+    return (uint32_t)(__float_as_int(__fadd_rz(acc, kTwo23)) - 0x4B000000);  // trunc of acc in (0, 256)
+}
+
+// The same estimate split in two halves so a thread can keep several samples'
+// loads in flight: prepare() runs the cell test and forms the weights' factors,
+// load() issues the eight corner loads, finish() sums them and truncates.
+struct U8Sample {
+    const uint8_t* q;
+    float p0, p1, p2, n0, n1, n2;
+    uint32_t v[8];
+    bool ok;
+    __device__ __forceinline__ void prepare(const uint8_t* __restrict__ I, const SampleGeo& g, float x, float y,
+                                            float z)
+    {
+        ok = !(x < 0.0f || y < 0.0f || z < 0.0f) && (x < g.wl) && (y < g.hl) && (z < g.dl);
+        if (!ok)
+            return;
+        int ix, iy, iz;
+        const float fx = floor_pos(x, ix), fy = floor_pos(y, iy), fz = floor_pos(z, iz);
+        p0 = x - fx;
+        p1 = y - fy;
+        p2 = z - fz;
+        n0 = 1.0f - p0;
+        n1 = 1.0f - p1;
+        n2 = 1.0f - p2;
+        q = I + ((iz * g.h + iy) * g.w + ix);
+    }
+    __device__ __forceinline__ void load(const SampleGeo& g)
+    {
+        if (!ok)
+            return;
+        const int w = g.w, wh = g.wh;
+        v[0] = __ldg(q);
+        v[1] = __ldg(q + 1);
+        v[2] = __ldg(q + w);
+        v[3] = __ldg(q + w + 1);
+        v[4] = __ldg(q + wh);
+        v[5] = __ldg(q + wh + 1);
+        v[6] = __ldg(q + wh + w);
+        v[7] = __ldg(q + wh + w + 1);
+    }
+    __device__ __forceinline__ uint32_t finish() const
+    {
+        if (!ok)
+            return 0u;
+        const float n0n1 = n0 * n1, p0n1 = p0 * n1, n0p1 = n0 * p1, p0p1 = p0 * p1;
+        float acc = u8_to_f(v[0]) * (n0n1 * n2);
+        acc += u8_to_f(v[1]) * (p0n1 * n2);
+        acc += u8_to_f(v[2]) * (n0p1 * n2);
+        acc += u8_to_f(v[3]) * (p0p1 * n2);
+        acc += u8_to_f(v[4]) * (n0n1 * p2);
+        acc += u8_to_f(v[5]) * (p0n1 * p2);
+        acc += u8_to_f(v[6]) * (n0p1 * p2);
+        acc += u8_to_f(v[7]) * (p0p1 * p2);
+        if (acc <= 0.0f)
+            return 0u;
+        return (uint32_t)(__float_as_int(__fadd_rz(acc, kTwo23)) - 0x4B000000);
+    }
+};
+
+// Per-row part of the transform: for a fixed row (y, z), y*T[3a+1] and z*T[3a+2]
+// of each axis a; the per-voxel remainder ((x*T0 + yT1) + zT2) + s keeps the
+// reference's summation order.  The x column and the shift are held once (ColXform)
+// and shared by every row a thread works on.
+struct ColXform {
+    float t0[3], s[3];
+    __device__ __forceinline__ void set(const float* T)
+    {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            t0[a] = T[3 * a];
+            s[a] = T[9 + a];
+        }
+    }
+};
+struct RowXform {
+    float yt[3], zt[3];
+    __device__ __forceinline__ void set(const float* T, int y, int z)
+    {
+        const float fy = (float)y, fz = (float)z;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            yt[a] = fy * T[3 * a + 1];
+            zt[a] = fz * T[3 * a + 2];
+        }
+    }
+    __device__ __forceinline__ void at(const ColXform& c, float fx, float& px, float& py, float& pz) const
+    {
+        px = fx * c.t0[0] + yt[0] + zt[0] + c.s[0];
+        py = fx * c.t0[1] + yt[1] + zt[1] + c.s[1];
+        pz = fx * c.t0[2] + yt[2] + zt[2] + c.s[2];
+    }
+};
+
 __device__ __forceinline__ void unflat(int i, const Dim3& D, int& x, int& y, int& z)
 {
     x = i % D.w;

@@ -30,8 +30,8 @@ struct AffineTask {
     int mode;               // 0 trilinear, 1 integer-shift copy (correlation only)
     int keep;               // MI: 1 = leave the counts in hist (no reduction, no clearing)
     int shift[3];
-    int nchunk;             // voxel chunks of this task
-    int chunk;              // voxels per chunk
+    int nchunk;             // chunks of this task
+    int chunk;              // rows (y, z) of the fixed grid per chunk
     uint32_t* hist;                // MI: 65536 counters
     const int32_t* row_hist;       // MI: template value histogram (256)
     unsigned long long* moments;   // correlation: sum y, sum y^2, sum x*y
