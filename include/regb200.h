@@ -190,6 +190,78 @@ regb_status regb_linear(const regb_volume* from, const float from_vs[3], const r
                         const float to_vs[3], float arg[12], const regb_linear_param* param,
                         volatile const int* terminated, float* cost_out, long long* cost_evals);
 
+/* ---- serving engine ---------------------------------------------------------------
+ * No counterpart in the reference (which registers one pair per call): registration
+ * jobs submitted as they arrive run concurrently on one GPU.  Their affine probe sets
+ * are evaluated together in shared launches and their CDM levels iterate together,
+ * with continuous batching (jobs join and leave between launches).  A job starts
+ * when a slot is free and its estimated device memory fits the budget.  Each job's
+ * result equals what regb_linear / regb_cdm give for it alone. */
+typedef struct regb_engine regb_engine;
+
+typedef struct {
+    size_t hbm_budget_bytes;   /* admission budget for running jobs; 0 = 80% of free memory */
+    int max_active;            /* concurrent jobs; 0 = 64 */
+    int gather_us;             /* once the device is free, how long a cost batch waits for
+                                  more jobs to join; 0 = 30 us */
+    int cdm_iters_per_round;   /* CDM iterations launched between two reads of the done
+                                  flags; 0 = 4 */
+} regb_engine_config;
+
+/* One registration: affine (tipl::reg::linear) of moving to the template, then
+ * optionally CDM (tipl::reg::cdm_common) of the template against the affine-
+ * resampled moving volume (the reg/mm_reg.hpp:348-416 pipeline).  Host buffers must
+ * stay valid until the job has finished. */
+typedef struct {
+    int template_id;           /* resident template (regb_engine_add_template), or -1 */
+    regb_volume fixed;         /* used when template_id < 0 */
+    float fixed_vs[3];
+    regb_volume moving;
+    float moving_vs[3];
+    int run_linear;            /* 1 = run the affine stage (uint8 volumes) */
+    regb_linear_param linear;
+    float arg[12];             /* initial affine parameters */
+    int run_cdm;               /* 1 = run CDM after the affine stage */
+    regb_cdm_param cdm;
+    float* field_out;          /* optional: receives the CDM field (template dims x 3 floats) */
+    int field_location;        /* REGB_HOST or REGB_DEVICE for field_out */
+} regb_job;
+
+typedef struct {
+    int status;                /* REGB_OK, REGB_CANCELLED or an error code */
+    float linear_cost;
+    float arg[12];
+    long long cost_evals;
+    int cdm_ok;                /* 1 when CDM ran and returned true */
+    int cdm_iterations;
+    double queued_ms;          /* submit -> start */
+    double run_ms;             /* start -> done */
+} regb_result;
+
+typedef struct {
+    int queued, running;
+    size_t used_bytes, budget_bytes;
+    long long affine_launches, affine_tasks, cdm_rounds;
+} regb_engine_stats;
+
+void regb_engine_config_default(regb_engine_config* c);
+void regb_job_default(regb_job* j);
+regb_status regb_engine_create(const regb_engine_config* cfg, regb_engine** out);
+/* Cancels queued and running jobs, waits for the running ones, frees everything. */
+regb_status regb_engine_destroy(regb_engine* e);
+/* Copies a template volume to the device once; jobs then refer to it by id. */
+regb_status regb_engine_add_template(regb_engine* e, const regb_volume* vol, const float vs[3], int* template_id);
+/* Queues a job; REGB_ERR_BUDGET when it can never fit the budget. */
+regb_status regb_engine_submit(regb_engine* e, const regb_job* job, uint64_t* id);
+/* REGB_OK with the result when the job has finished, REGB_PENDING otherwise. */
+regb_status regb_engine_poll(regb_engine* e, uint64_t id, regb_result* out);
+regb_status regb_engine_wait(regb_engine* e, uint64_t id, regb_result* out);
+/* Sets the job's terminated flag (polled between iterations); a queued job ends at once. */
+regb_status regb_engine_cancel(regb_engine* e, uint64_t id);
+/* Drops a finished job's record. */
+regb_status regb_engine_release_job(regb_engine* e, uint64_t id);
+regb_status regb_engine_get_stats(regb_engine* e, regb_engine_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

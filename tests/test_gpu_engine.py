@@ -1,0 +1,94 @@
+"""Serving engine: jobs of different shapes run together with continuous batching;
+each job's result must equal the result of the plain single-job calls (regb_linear,
+then regb_cdm on the affine-resampled subject) bit for bit -- alone vs in the mix.
+Also admission by the HBM budget and cancellation of a queued job."""
+import numpy as np
+import pytest
+
+import tipl_b200 as tb
+from tipl_b200 import _lib
+from tipl_b200 import phantom as ph
+
+pytestmark = pytest.mark.gpu
+
+TSHAPE = (40, 44, 36)
+MSHAPES = [(40, 44, 36), (36, 40, 38), (44, 46, 40), (30, 50, 34)]
+
+
+@pytest.fixture(scope="module")
+def data():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    rng = np.random.default_rng(ph.seed_for(5, 1))
+    tmpl = ph.normalize_to_u8(ph.class_phantom(TSHAPE, rng))
+    movs = []
+    for s in MSHAPES:
+        t2 = ph.class_phantom(s, rng)
+        p = ph.random_affine(rng, rot_deg=6, trans_vox=2)
+        T = ph.affine_matrix_f32(p, s, (1, 1, 1), s, (1, 1, 1))
+        movs.append(ph.normalize_to_u8(ph.rician(ph.apply_matrix(t2, T, s), rng)))
+    return tmpl, movs
+
+
+def alone(tmpl, mov, with_cdm):
+    cost, arg, evals = tb.reg.linear(tmpl, (1, 1, 1), mov, (1, 1, 1))
+    field = None
+    if with_cdm:
+        T = tb.affine_to_matrix(arg, tmpl.shape, (1, 1, 1), mov.shape, (1, 1, 1))
+        Is = tb.resample(mov, tmpl.shape, T, allow_shift_copy=True)
+        field, ok = tb.reg.cdm(tmpl, Is)
+        assert ok
+    return cost, arg, evals, field
+
+
+@pytest.mark.parametrize("with_cdm", [False, True])
+def test_alone_vs_in_the_mix(data, with_cdm):
+    tmpl, movs = data
+    ref = [alone(tmpl, m, with_cdm) for m in movs]
+    with tb.Engine(max_active=8) as eng:
+        tid = eng.add_template(tmpl)
+        fields = [np.zeros(tmpl.shape + (3,), np.float32) for _ in movs]
+        ids = [eng.submit(m, template=tid, cdm=with_cdm, field_out=f if with_cdm else None)
+               for m, f in zip(movs, fields)]
+        res = [eng.wait(i) for i in ids]
+        st = eng.stats()
+    # the mix really was batched: fewer launches than the jobs' probe rounds alone
+    assert st["affine_tasks"] == sum(r[2] for r in ref)
+    for r, (cost, arg, evals, field), f in zip(res, ref, fields):
+        assert r["status"] == 0
+        assert r["linear_cost"] == np.float32(cost)
+        assert np.array_equal(r["arg"].view(np.uint32), arg.view(np.uint32))
+        assert r["cost_evals"] == evals
+        if with_cdm:
+            assert r["cdm_ok"]
+            assert np.array_equal(f.view(np.uint32), field.view(np.uint32))
+
+
+def test_budget_admission_and_cancel(data):
+    tmpl, movs = data
+    # a budget that admits one job at a time: the rest queue, then run
+    one = 16 << 20
+    with tb.Engine(hbm_budget_bytes=one + (4 << 20), max_active=8) as eng:
+        tid = eng.add_template(tmpl)
+        ids = [eng.submit(m, template=tid) for m in movs[:3]]
+        res = [eng.wait(i) for i in ids]
+        assert all(r["status"] == 0 for r in res)
+        assert res[2]["queued_ms"] > 0.0
+    # a job that can never fit
+    with tb.Engine(hbm_budget_bytes=1 << 20) as eng:
+        tid = eng.add_template(tmpl)
+        with pytest.raises(_lib.RegbError) as e:
+            eng.submit(movs[0], template=tid, cdm=True)
+        assert e.value.status == _lib.REGB_ERR_BUDGET
+    # cancelling a queued job ends it at once
+    with tb.Engine(max_active=1) as eng:
+        tid = eng.add_template(tmpl)
+        a = eng.submit(movs[0], template=tid)
+        b = eng.submit(movs[1], template=tid)
+        eng.cancel(b)
+        rb = eng.wait(b)
+        ra = eng.wait(a)
+        assert rb["status"] == _lib.REGB_CANCELLED
+        assert ra["status"] == 0

@@ -32,7 +32,7 @@ from ._lib import CdmParam, Field, LinearParam, RegbError, Volume  # noqa: F401
 
 __all__ = ["affine_to_matrix", "affine_to_matrix_f64", "matrix_inverse", "resample", "mi_cost", "corr_cost",
            "compose_displacement", "accumulate_displacement", "downsample", "upsample_field_x2", "cdm_gradient",
-           "cdm_poisson", "cdm_max_length", "cdm_smooth", "reg", "RegbError", "version"]
+           "cdm_poisson", "cdm_max_length", "cdm_smooth", "reg", "Engine", "RegbError", "version"]
 
 
 def version() -> str:
@@ -262,3 +262,120 @@ class reg:
         st = _lib.lib().regb_cdm(C.byref(_vol(It)), C.byref(_vol(Is)), C.byref(_field(d)), C.byref(p), term)
         _lib.check(st, allow=(_lib.REGB_OK, _lib.REGB_FALSE, _lib.REGB_CANCELLED))
         return d, st != _lib.REGB_FALSE
+
+
+# ---------------------------------------------------------------- serving engine
+class Engine:
+    """Continuous-batching registration server on one GPU (regb_engine_* in the C ABI).
+
+    Jobs run concurrently: their affine probe sets share launches and their CDM
+    levels iterate together.  Host arrays passed to submit() are kept alive here
+    until the job is released."""
+
+    def __init__(self, hbm_budget_bytes=0, max_active=64, gather_us=30, cdm_iters_per_round=4):
+        L = _lib.lib()
+        cfg = _lib.EngineConfig()
+        L.regb_engine_config_default(C.byref(cfg))
+        cfg.hbm_budget_bytes = int(hbm_budget_bytes)
+        cfg.max_active = int(max_active)
+        cfg.gather_us = int(gather_us)
+        cfg.cdm_iters_per_round = int(cdm_iters_per_round)
+        h = C.c_void_p()
+        _lib.check(L.regb_engine_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._keep = {}
+        self._tkeep = []
+
+    def add_template(self, vol, vs=(1.0, 1.0, 1.0)) -> int:
+        tid = C.c_int(-1)
+        v = _vol(vol)
+        _lib.check(_lib.lib().regb_engine_add_template(self._h, C.byref(v), _fptr(np.asarray(vs, np.float32)),
+                                                       C.byref(tid)))
+        self._tkeep.append(vol)
+        return tid.value
+
+    def submit(self, moving, moving_vs=(1.0, 1.0, 1.0), template=None, fixed=None, fixed_vs=(1.0, 1.0, 1.0),
+               linear=True, linear_param: LinearParam | None = None, arg=None, cdm=False,
+               cdm_param: CdmParam | None = None, field_out=None) -> int:
+        L = _lib.lib()
+        j = _lib.Job()
+        L.regb_job_default(C.byref(j))
+        keep = [moving]
+        if template is not None:
+            j.template_id = int(template)
+        else:
+            j.template_id = -1
+            j.fixed = _vol(fixed)
+            keep.append(fixed)
+        j.fixed_vs[:] = [float(v) for v in fixed_vs]
+        j.moving = _vol(moving)
+        j.moving_vs[:] = [float(v) for v in moving_vs]
+        j.run_linear = int(bool(linear))
+        if linear_param is not None:
+            j.linear = linear_param
+        if arg is not None:
+            j.arg[:] = [float(v) for v in arg]
+        j.run_cdm = int(bool(cdm))
+        if cdm_param is not None:
+            j.cdm = cdm_param
+        if field_out is not None:
+            if _is_dev(field_out):
+                j.field_out = field_out.data_ptr()
+                j.field_location = _lib.DEVICE
+            else:
+                assert field_out.dtype == np.float32 and field_out.flags["C_CONTIGUOUS"]
+                j.field_out = field_out.ctypes.data
+                j.field_location = _lib.HOST
+            keep.append(field_out)
+        jid = C.c_uint64(0)
+        _lib.check(L.regb_engine_submit(self._h, C.byref(j), C.byref(jid)))
+        self._keep[jid.value] = keep
+        return jid.value
+
+    @staticmethod
+    def _res(r):
+        return {"status": r.status, "linear_cost": r.linear_cost, "arg": np.array(r.arg[:], np.float32),
+                "cost_evals": r.cost_evals, "cdm_ok": bool(r.cdm_ok), "cdm_iterations": r.cdm_iterations,
+                "queued_ms": r.queued_ms, "run_ms": r.run_ms}
+
+    def poll(self, jid):
+        r = _lib.Result()
+        st = _lib.lib().regb_engine_poll(self._h, C.c_uint64(jid), C.byref(r))
+        if st == _lib.REGB_PENDING:
+            return None
+        _lib.check(st)
+        return self._res(r)
+
+    def wait(self, jid, release=True):
+        r = _lib.Result()
+        _lib.check(_lib.lib().regb_engine_wait(self._h, C.c_uint64(jid), C.byref(r)))
+        if release:
+            _lib.lib().regb_engine_release_job(self._h, C.c_uint64(jid))
+            self._keep.pop(jid, None)
+        return self._res(r)
+
+    def cancel(self, jid):
+        _lib.check(_lib.lib().regb_engine_cancel(self._h, C.c_uint64(jid)))
+
+    def stats(self):
+        s = _lib.EngineStats()
+        _lib.check(_lib.lib().regb_engine_get_stats(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def close(self):
+        if self._h:
+            _lib.lib().regb_engine_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -49,6 +49,30 @@ class Stats(C.Structure):
                 ("corr_bytes", C.c_double), ("corr_ms", C.c_double)]
 
 
+class EngineConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_active", C.c_int), ("gather_us", C.c_int),
+                ("cdm_iters_per_round", C.c_int)]
+
+
+class Job(C.Structure):
+    _fields_ = [("template_id", C.c_int), ("fixed", Volume), ("fixed_vs", C.c_float * 3), ("moving", Volume),
+                ("moving_vs", C.c_float * 3), ("run_linear", C.c_int), ("linear", LinearParam),
+                ("arg", C.c_float * 12), ("run_cdm", C.c_int), ("cdm", CdmParam), ("field_out", C.c_void_p),
+                ("field_location", C.c_int)]
+
+
+class Result(C.Structure):
+    _fields_ = [("status", C.c_int), ("linear_cost", C.c_float), ("arg", C.c_float * 12),
+                ("cost_evals", C.c_longlong), ("cdm_ok", C.c_int), ("cdm_iterations", C.c_int),
+                ("queued_ms", C.c_double), ("run_ms", C.c_double)]
+
+
+class EngineStats(C.Structure):
+    _fields_ = [("queued", C.c_int), ("running", C.c_int), ("used_bytes", C.c_size_t),
+                ("budget_bytes", C.c_size_t), ("affine_launches", C.c_longlong), ("affine_tasks", C.c_longlong),
+                ("cdm_rounds", C.c_longlong)]
+
+
 class RegbError(RuntimeError):
     def __init__(self, status: int, what: str):
         super().__init__(f"regb status {status}: {what}")
@@ -89,6 +113,17 @@ _SIGS = {
     "regb_cdm_smooth": (C.c_int, [C.POINTER(Field), C.POINTER(Field), C.c_float, C.c_void_p]),
     "regb_cdm": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.POINTER(Field), C.POINTER(CdmParam),
                            C.c_void_p]),
+    "regb_engine_config_default": (None, [C.POINTER(EngineConfig)]),
+    "regb_job_default": (None, [C.POINTER(Job)]),
+    "regb_engine_create": (C.c_int, [C.POINTER(EngineConfig), C.POINTER(C.c_void_p)]),
+    "regb_engine_destroy": (C.c_int, [C.c_void_p]),
+    "regb_engine_add_template": (C.c_int, [C.c_void_p, C.POINTER(Volume), C.c_void_p, C.POINTER(C.c_int)]),
+    "regb_engine_submit": (C.c_int, [C.c_void_p, C.POINTER(Job), C.POINTER(C.c_uint64)]),
+    "regb_engine_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Result)]),
+    "regb_engine_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Result)]),
+    "regb_engine_cancel": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "regb_engine_release_job": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "regb_engine_get_stats": (C.c_int, [C.c_void_p, C.POINTER(EngineStats)]),
     "regb_linear": (C.c_int, [C.POINTER(Volume), C.c_void_p, C.POINTER(Volume), C.c_void_p, C.c_void_p,
                               C.POINTER(LinearParam), C.c_void_p, C.POINTER(C.c_float),
                               C.POINTER(C.c_longlong)]),

@@ -1,4 +1,5 @@
 #include "affine_eval.h"
+#include "batcher.h"
 #include "stats.h"
 #include <algorithm>
 #include <cstring>
@@ -23,6 +24,18 @@ void TaskScratch::ensure(int k, bool need_hist, cudaStream_t st)
     h_tasks.alloc((size_t)c);
     h_cost.alloc((size_t)c);
     cap = c;
+}
+
+void TaskScratch::release()
+{
+    hist.reset();
+    moments.reset();
+    ticket.reset();
+    cost.reset();
+    tasks.reset();
+    h_tasks.reset();
+    h_cost.reset();
+    cap = 0;
 }
 
 void set_task_chunks(AffineTask& t, int cost_type)
@@ -134,6 +147,13 @@ std::vector<double> AffineEvaluator::eval(int level, const float* T, int K)
     std::vector<double> out(K);
     if (K == 0)
         return out;
+    if (batcher_) {
+        std::vector<AffineTask> t(K);
+        for (int k = 0; k < K; ++k)
+            make_task(level, T + 12 * k, t[k]);
+        batcher_->eval(t.data(), K, cost_type_, out.data());
+        return out;
+    }
     s_.ensure(K, cost_type_ == REGB_COST_MI, st_);
     for (int k = 0; k < K; ++k)
         make_task(level, T + 12 * k, s_.h_tasks.p[k]);

@@ -19,7 +19,10 @@ struct TaskScratch {
     PinBuf<AffineTask> h_tasks;
     PinBuf<double> h_cost;
     void ensure(int k, bool need_hist, cudaStream_t st);
+    void release();
 };
+
+class AffineBatcher;
 
 // Fills the scratch pointers of h_tasks[0..K), launches the MI or correlation
 // kernel for all of them, and copies the costs back (synchronises st).
@@ -42,6 +45,8 @@ public:
     // Builds the task of one candidate (used by the engine to batch across jobs).
     void make_task(int level, const float* T, AffineTask& out) const;
     int cost_type() const { return cost_type_; }
+    // Route evaluations through a cross-job batcher instead of launching directly.
+    void set_batcher(AffineBatcher* b) { batcher_ = b; }
 
 private:
     struct Lvl {
@@ -55,6 +60,7 @@ private:
     int cost_type_;
     cudaStream_t st_;
     TaskScratch s_;
+    AffineBatcher* batcher_ = nullptr;
 };
 
 }  // namespace regb

@@ -16,6 +16,7 @@
 #include <vector>
 #include "cdm_level.h"
 #include "host.h"
+#include "scheduler.h"
 
 namespace regb {
 
@@ -74,7 +75,8 @@ void launch_iteration(const CdmSeg* d_segs, int nseg, int blocks, int pix, int g
 }
 
 regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int pix, float* d_field,
-                         const regb_cdm_param& p, volatile const int* terminated, cudaStream_t st, int* iterations)
+                         const regb_cdm_param& p, volatile const int* terminated, cudaStream_t st, int* iterations,
+                         CdmScheduler* sched)
 {
     const size_t psz = pix ? 4 : 1;
     struct Lv {
@@ -135,7 +137,16 @@ regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int
             continue;
         CdmLevel run;
         run.init(L.It, L.Is, L.w, L.h, L.d, pix, p, best, st);
-        for (int it = 0; it < 201; ++it) {
+        if (sched) {
+            // batched with the other jobs' levels; the scheduler returns once this
+            // level's loop has ended
+            sched->run(run, p.gradient_type, terminated);
+            REGB_CK(cudaMemcpyAsync(&run.h_ctl, run.ctl.p, sizeof(CdmCtl), cudaMemcpyDeviceToHost, st));
+            REGB_CK(cudaStreamSynchronize(st));
+            if (terminated && *terminated && !run.h_ctl.done)
+                status = REGB_CANCELLED;
+        }
+        for (int it = 0; !sched && it < 201; ++it) {
             if (terminated && *terminated) {
                 status = REGB_CANCELLED;
                 break;

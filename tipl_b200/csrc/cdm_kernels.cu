@@ -657,6 +657,23 @@ cudaError_t launch_cost_mean(const CdmSeg* segs, int nseg, float* out, cudaStrea
     return cudaGetLastError();
 }
 
+// done flags of many segments gathered into one array (one read-back per round)
+__global__ void cdm_status_kernel(const CdmSeg* __restrict__ segs, int n, int* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        out[i] = segs[i].ctl->done;
+}
+
+cudaError_t launch_cdm_status(const CdmSeg* segs, int nseg, int* out, cudaStream_t st)
+{
+    if (nseg <= 0)
+        return cudaSuccess;
+    cdm_status_kernel<<<(nseg + 127) / 128, 128, 0, st>>>(segs, nseg, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ launchers
 #define SEG_GRID dim3(blocks, nseg)
 

@@ -1,0 +1,504 @@
+// Serving engine: registration jobs submitted as they arrive run concurrently on
+// one GPU with continuous batching.
+//
+//   admission  -- a job starts when a slot is free and its estimated device memory
+//                 fits the engine's HBM budget; others wait in arrival order;
+//   affine     -- each running job drives its own optimiser (host threads); its
+//                 probe sets go to the shared AffineBatcher, which evaluates the
+//                 pending sets of all jobs in one launch;
+//   nonlinear  -- each job's CDM levels are segments of the shared CdmScheduler,
+//                 which iterates all of them in the same launches;
+//   state      -- volumes, pyramids, fields and optimiser state stay on the device
+//                 for the whole job; templates can be made resident once and shared.
+// A job's result does not depend on what it ran alongside: every cost and every
+// CDM decision is computed from that job's data alone (the tests check alone vs
+// in the mix).
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include "batcher.h"
+#include "host.h"
+#include "scheduler.h"
+
+using Clock = std::chrono::steady_clock;
+
+namespace regb {
+
+struct EngineTemplate {
+    DevBuf<uint8_t> data;
+    int dim[3];
+    int dtype;
+    float vs[3];
+};
+
+struct EngineJob {
+    uint64_t id = 0;
+    regb_job spec{};
+    regb_result res{};
+    int state = 0;  // 0 queued, 1 running, 2 done
+    size_t est = 0;
+    volatile int cancel = 0;
+    Clock::time_point t_submit, t_start, t_end;
+};
+
+class Engine {
+public:
+    explicit Engine(const regb_engine_config& c)
+        : cfg_(c), batcher_(c.gather_us > 0 ? c.gather_us : 30), sched_(c.cdm_iters_per_round > 0 ? c.cdm_iters_per_round : 4)
+    {
+        REGB_CK(cudaGetDevice(&dev_));
+        if (cfg_.max_active <= 0)
+            cfg_.max_active = 64;
+        if (cfg_.hbm_budget_bytes == 0) {
+            size_t fr = 0, tot = 0;
+            REGB_CK(cudaMemGetInfo(&fr, &tot));
+            cfg_.hbm_budget_bytes = (size_t)(0.8 * (double)fr);
+        }
+    }
+    ~Engine()
+    {
+        {
+            std::unique_lock<std::mutex> lk(m_);
+            for (auto& kv : jobs_)
+                kv.second->cancel = 1;
+            queue_.clear();
+            cv_.wait(lk, [&] { return running_ == 0; });
+        }
+        templates_.clear();
+        cudaStreamSynchronize(util_.s);
+    }
+
+    int add_template(const regb_volume& v, const float* vs)
+    {
+        auto t = std::make_unique<EngineTemplate>();
+        const size_t n = (size_t)v.dim[0] * v.dim[1] * v.dim[2] * pix_size(v.dtype);
+        // on the engine's own stream, which outlives every template buffer
+        t->data.alloc(n, util_.s);
+        REGB_CK(cudaMemcpyAsync(t->data.p, v.ptr, n, v.location == REGB_HOST ? cudaMemcpyHostToDevice
+                                                                              : cudaMemcpyDeviceToDevice, util_.s));
+        util_.sync();
+        std::memcpy(t->dim, v.dim, sizeof(t->dim));
+        t->dtype = v.dtype;
+        std::memcpy(t->vs, vs, sizeof(t->vs));
+        std::lock_guard<std::mutex> g(m_);
+        templates_.push_back(std::move(t));
+        return (int)templates_.size() - 1;
+    }
+
+    uint64_t submit(const regb_job& j)
+    {
+        auto job = std::make_unique<EngineJob>();
+        job->spec = j;
+        job->t_submit = Clock::now();
+        std::lock_guard<std::mutex> g(m_);
+        if (j.template_id >= (int)templates_.size())
+            throw Failure(REGB_ERR_ARG, "unknown template id");
+        job->est = estimate(j);
+        if (job->est > cfg_.hbm_budget_bytes)
+            throw Failure(REGB_ERR_BUDGET, "job needs more device memory than the engine's budget");
+        job->id = next_id_++;
+        EngineJob* p = job.get();
+        jobs_[p->id] = std::move(job);
+        queue_.push_back(p);
+        admit_locked();
+        return p->id;
+    }
+
+    regb_status poll(uint64_t id, regb_result* out, bool wait)
+    {
+        std::unique_lock<std::mutex> lk(m_);
+        auto it = jobs_.find(id);
+        if (it == jobs_.end())
+            return REGB_ERR_NOTFOUND;
+        EngineJob* j = it->second.get();
+        if (wait)
+            cv_.wait(lk, [&] { return j->state == 2; });
+        if (j->state != 2)
+            return REGB_PENDING;
+        if (out)
+            *out = j->res;
+        return REGB_OK;
+    }
+
+    regb_status cancel(uint64_t id)
+    {
+        std::lock_guard<std::mutex> g(m_);
+        auto it = jobs_.find(id);
+        if (it == jobs_.end())
+            return REGB_ERR_NOTFOUND;
+        EngineJob* j = it->second.get();
+        j->cancel = 1;
+        if (j->state == 0) {  // still queued: finish it here
+            for (auto q = queue_.begin(); q != queue_.end(); ++q)
+                if (*q == j) {
+                    queue_.erase(q);
+                    break;
+                }
+            j->res.status = REGB_CANCELLED;
+            j->state = 2;
+            cv_.notify_all();
+        }
+        return REGB_OK;
+    }
+
+    void forget(uint64_t id)
+    {
+        std::lock_guard<std::mutex> g(m_);
+        auto it = jobs_.find(id);
+        if (it != jobs_.end() && it->second->state == 2)
+            jobs_.erase(it);
+    }
+
+    regb_engine_stats stats()
+    {
+        std::lock_guard<std::mutex> g(m_);
+        regb_engine_stats s{};
+        s.queued = (int)queue_.size();
+        s.running = running_;
+        s.used_bytes = used_;
+        s.budget_bytes = cfg_.hbm_budget_bytes;
+        s.affine_launches = batcher_.launches();
+        s.affine_tasks = batcher_.tasks_evaluated();
+        s.cdm_rounds = sched_.rounds();
+        return s;
+    }
+
+private:
+    // Device memory a job holds while it runs (its own volumes and pyramids, the
+    // affine-resampled subject and the CDM fields); the shared batch scratch and
+    // resident templates are not counted.
+    size_t estimate(const regb_job& j) const
+    {
+        const int* fd = (j.template_id >= 0) ? templates_.at(j.template_id)->dim : j.fixed.dim;
+        const int ftype = (j.template_id >= 0) ? templates_.at(j.template_id)->dtype : j.fixed.dtype;
+        const double nf = (double)fd[0] * fd[1] * fd[2];
+        const double nm = (double)j.moving.dim[0] * j.moving.dim[1] * j.moving.dim[2];
+        const double ps = (double)pix_size(ftype);
+        double b = 0.0;
+        if (j.template_id < 0)
+            b += nf * ps;
+        b += nm * (double)pix_size(j.moving.dtype);
+        if (j.run_linear)
+            b += 0.15 * (nf + nm);
+        if (j.run_cdm) {
+            b += nf * ps + 12.0 * nf;  // resampled subject, output field
+            // the largest iterated level: 5 fields + composed image
+            int w = fd[0], h = fd[1], d = fd[2];
+            float res = j.cdm.resolution;
+            double worst = 0.0;
+            std::vector<double> lv;
+            std::vector<float> lr;
+            for (;;) {
+                lv.push_back((double)w * h * d);
+                lr.push_back(res);
+                if (!((unsigned)std::min(w, std::min(h, d)) > j.cdm.min_dimension))
+                    break;
+                w = (w + 1) / 2;
+                h = (h + 1) / 2;
+                d = (d + 1) / 2;
+                res /= 2.0f;
+            }
+            for (size_t k = 0; k < lv.size(); ++k)
+                if (k + 1 == lv.size() || lr[k] <= 1.0f)
+                    worst = std::max(worst, lv[k]);
+            b += worst * (60.0 + ps) + 0.3 * nf * ps;
+        }
+        return (size_t)b + (16u << 20);
+    }
+
+    void admit_locked()
+    {
+        while (!queue_.empty() && running_ < cfg_.max_active && used_ + queue_.front()->est <= cfg_.hbm_budget_bytes) {
+            EngineJob* j = queue_.front();
+            queue_.pop_front();
+            j->state = 1;
+            j->t_start = Clock::now();
+            ++running_;
+            used_ += j->est;
+            std::thread([this, j] { run(j); }).detach();
+        }
+    }
+
+    void run(EngineJob* j)
+    {
+        cudaSetDevice(dev_);
+        regb_result r{};
+        try {
+            r = execute(j);
+        } catch (const Failure& f) {
+            r.status = f.code;
+            set_last_error(f.what());
+        } catch (const std::exception& e) {
+            r.status = REGB_ERR_ARG;
+            set_last_error(e.what());
+        }
+        std::lock_guard<std::mutex> g(m_);
+        j->t_end = Clock::now();
+        r.queued_ms = std::chrono::duration<double, std::milli>(j->t_start - j->t_submit).count();
+        r.run_ms = std::chrono::duration<double, std::milli>(j->t_end - j->t_start).count();
+        j->res = r;
+        j->state = 2;
+        --running_;
+        used_ -= j->est;
+        admit_locked();
+        cv_.notify_all();
+    }
+
+    regb_result execute(EngineJob* j)
+    {
+        const regb_job& s = j->spec;
+        regb_result r{};
+        std::memcpy(r.arg, s.arg, sizeof(r.arg));
+        Stream st;
+        // fixed volume: resident template or the job's own
+        const void* d_fixed;
+        int fdim[3];
+        int fdtype;
+        float fvs[3];
+        DevBuf<uint8_t> own_fixed, own_moving;
+        if (s.template_id >= 0) {
+            const EngineTemplate* t;
+            {
+                std::lock_guard<std::mutex> g(m_);
+                t = templates_.at(s.template_id).get();
+            }
+            d_fixed = t->data.p;
+            std::memcpy(fdim, t->dim, sizeof(fdim));
+            fdtype = t->dtype;
+            std::memcpy(fvs, t->vs, sizeof(fvs));
+        } else {
+            const size_t b = (size_t)s.fixed.dim[0] * s.fixed.dim[1] * s.fixed.dim[2] * pix_size(s.fixed.dtype);
+            if (s.fixed.location == REGB_HOST) {
+                own_fixed.alloc(b, st.s);
+                REGB_CK(cudaMemcpyAsync(own_fixed.p, s.fixed.ptr, b, cudaMemcpyHostToDevice, st.s));
+                d_fixed = own_fixed.p;
+            } else
+                d_fixed = s.fixed.ptr;
+            std::memcpy(fdim, s.fixed.dim, sizeof(fdim));
+            fdtype = s.fixed.dtype;
+            std::memcpy(fvs, s.fixed_vs, sizeof(fvs));
+        }
+        const size_t mb = (size_t)s.moving.dim[0] * s.moving.dim[1] * s.moving.dim[2] * pix_size(s.moving.dtype);
+        const void* d_moving = s.moving.ptr;
+        if (s.moving.location == REGB_HOST) {
+            own_moving.alloc(mb, st.s);
+            REGB_CK(cudaMemcpyAsync(own_moving.p, s.moving.ptr, mb, cudaMemcpyHostToDevice, st.s));
+            d_moving = own_moving.p;
+        }
+        st.sync();
+        r.status = REGB_OK;
+        if (s.run_linear) {
+            batcher_.add_client();
+            LinearResult lr;
+            try {
+                lr = linear_register((const uint8_t*)d_fixed, fdim, fvs, (const uint8_t*)d_moving, s.moving.dim,
+                                     s.moving_vs, r.arg, s.linear, &j->cancel, st.s, &batcher_);
+            } catch (...) {
+                batcher_.remove_client();
+                throw;
+            }
+            batcher_.remove_client();
+            r.linear_cost = lr.cost;
+            r.cost_evals = lr.evals;
+        }
+        if (j->cancel) {
+            r.status = REGB_CANCELLED;
+            return r;
+        }
+        if (s.run_cdm) {
+            // the subject resampled onto the template grid with the affine found
+            // (the mm_reg pipeline, reg/mm_reg.hpp:379-416)
+            const int pix = (fdtype == REGB_F32) ? 1 : 0;
+            const size_t nf = (size_t)fdim[0] * fdim[1] * fdim[2];
+            DevBuf<uint8_t> Is(nf * (pix ? 4 : 1), st.s);
+            float T[12];
+            affine_to_matrix(r.arg, fdim, fvs, s.moving.dim, s.moving_vs, T);
+            int shift[3];
+            const int* sh = integer_shift(T, shift) ? shift : nullptr;
+            const Dim3 md{s.moving.dim[0], s.moving.dim[1], s.moving.dim[2]}, fdd{fdim[0], fdim[1], fdim[2]};
+            if (pix)
+                REGB_CK(launch_resample<float>((const float*)d_moving, md, (float*)Is.p, fdd, T, sh, st.s));
+            else
+                REGB_CK(launch_resample<uint8_t>((const uint8_t*)d_moving, md, Is.p, fdd, T, sh, st.s));
+            DevBuf<float> field(3 * nf, st.s);
+            int iters = 0;
+            regb_status cs = cdm_register(d_fixed, Is.p, fdim, pix, field.p, s.cdm, &j->cancel, st.s, &iters, &sched_);
+            r.cdm_ok = (cs == REGB_OK) ? 1 : 0;
+            r.cdm_iterations = iters;
+            if (cs == REGB_CANCELLED)
+                r.status = REGB_CANCELLED;
+            if (s.field_out && cs != REGB_FALSE)
+                REGB_CK(cudaMemcpyAsync(s.field_out, field.p, sizeof(float) * 3 * nf,
+                                        s.field_location == REGB_DEVICE ? cudaMemcpyDeviceToDevice
+                                                                        : cudaMemcpyDeviceToHost,
+                                        st.s));
+            st.sync();
+        }
+        return r;
+    }
+
+    regb_engine_config cfg_;
+    int dev_ = 0;
+    AffineBatcher batcher_;
+    CdmScheduler sched_;
+    std::mutex m_;
+    std::condition_variable cv_;
+    Stream util_;  // declared before templates_: destroyed after their buffers are freed on it
+    std::vector<std::unique_ptr<EngineTemplate>> templates_;
+    std::map<uint64_t, std::unique_ptr<EngineJob>> jobs_;
+    std::deque<EngineJob*> queue_;
+    int running_ = 0;
+    size_t used_ = 0;
+    uint64_t next_id_ = 1;
+};
+
+}  // namespace regb
+
+using namespace regb;
+
+struct regb_engine {
+    std::unique_ptr<Engine> e;
+};
+
+namespace {
+template <typename F>
+regb_status eguard(F&& f)
+{
+    try {
+        return f();
+    } catch (const Failure& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return REGB_ERR_ARG;
+    }
+}
+
+bool vol_ok(const regb_volume& v)
+{
+    return v.ptr && v.dim[0] > 0 && v.dim[1] > 0 && v.dim[2] > 0 &&
+           (long long)v.dim[0] * v.dim[1] * v.dim[2] < (1LL << 31) && pix_size(v.dtype) &&
+           (v.dtype == REGB_U8 || v.dtype == REGB_F32) && (v.location == REGB_HOST || v.location == REGB_DEVICE);
+}
+}  // namespace
+
+extern "C" {
+
+void regb_engine_config_default(regb_engine_config* c)
+{
+    if (!c)
+        return;
+    c->hbm_budget_bytes = 0;
+    c->max_active = 64;
+    c->gather_us = 30;
+    c->cdm_iters_per_round = 4;
+}
+
+void regb_job_default(regb_job* j)
+{
+    if (!j)
+        return;
+    std::memset(j, 0, sizeof(*j));
+    j->template_id = -1;
+    j->fixed_vs[0] = j->fixed_vs[1] = j->fixed_vs[2] = 1.0f;
+    j->moving_vs[0] = j->moving_vs[1] = j->moving_vs[2] = 1.0f;
+    j->run_linear = 1;
+    regb_linear_param_default(&j->linear);
+    regb_cdm_param_default(&j->cdm);
+    j->arg[6] = j->arg[7] = j->arg[8] = 1.0f;
+    j->field_location = REGB_HOST;
+}
+
+regb_status regb_engine_create(const regb_engine_config* cfg, regb_engine** out)
+{
+    return eguard([&] {
+        if (!out)
+            throw Failure(REGB_ERR_ARG, "null output");
+        regb_engine_config c;
+        regb_engine_config_default(&c);
+        if (cfg)
+            c = *cfg;
+        ensure_device();
+        auto* e = new regb_engine;
+        e->e = std::make_unique<Engine>(c);
+        *out = e;
+        return REGB_OK;
+    });
+}
+
+regb_status regb_engine_destroy(regb_engine* e)
+{
+    return eguard([&] {
+        delete e;
+        return REGB_OK;
+    });
+}
+
+regb_status regb_engine_add_template(regb_engine* e, const regb_volume* vol, const float vs[3], int* template_id)
+{
+    return eguard([&] {
+        if (!e || !vol || !vs || !template_id || !vol_ok(*vol))
+            throw Failure(REGB_ERR_ARG, "bad template arguments");
+        *template_id = e->e->add_template(*vol, vs);
+        return REGB_OK;
+    });
+}
+
+regb_status regb_engine_submit(regb_engine* e, const regb_job* job, uint64_t* id)
+{
+    return eguard([&] {
+        if (!e || !job || !id)
+            throw Failure(REGB_ERR_ARG, "null argument");
+        if (!vol_ok(job->moving) || (job->template_id < 0 && !vol_ok(job->fixed)))
+            throw Failure(REGB_ERR_ARG, "bad fixed/moving volume");
+        if (job->run_linear && (job->moving.dtype != REGB_U8 || (job->template_id < 0 && job->fixed.dtype != REGB_U8)))
+            throw Failure(REGB_ERR_ARG, "the affine stage takes uint8 volumes");
+        *id = e->e->submit(*job);
+        return REGB_OK;
+    });
+}
+
+regb_status regb_engine_poll(regb_engine* e, uint64_t id, regb_result* out)
+{
+    return eguard([&] { return e ? e->e->poll(id, out, false) : REGB_ERR_ARG; });
+}
+
+regb_status regb_engine_wait(regb_engine* e, uint64_t id, regb_result* out)
+{
+    return eguard([&] { return e ? e->e->poll(id, out, true) : REGB_ERR_ARG; });
+}
+
+regb_status regb_engine_cancel(regb_engine* e, uint64_t id)
+{
+    return eguard([&] { return e ? e->e->cancel(id) : REGB_ERR_ARG; });
+}
+
+regb_status regb_engine_release_job(regb_engine* e, uint64_t id)
+{
+    return eguard([&] {
+        if (!e)
+            return REGB_ERR_ARG;
+        e->e->forget(id);
+        return REGB_OK;
+    });
+}
+
+regb_status regb_engine_get_stats(regb_engine* e, regb_engine_stats* out)
+{
+    return eguard([&] {
+        if (!e || !out)
+            return REGB_ERR_ARG;
+        *out = e->e->stats();
+        return REGB_OK;
+    });
+}
+
+}  // extern "C"

@@ -137,14 +137,16 @@ struct LinearResult {
     long long evals = 0;
 };
 // The affine search of tipl::reg::linear on device-resident uint8 volumes.
+class AffineBatcher;
+class CdmScheduler;
 LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
                              const int* tdim, const float* to_vs, float* arg, const regb_linear_param& p,
-                             volatile const int* terminated, cudaStream_t st);
+                             volatile const int* terminated, cudaStream_t st, AffineBatcher* batcher = nullptr);
 
 // The CDM driver (reg/cdm.hpp:373-474) on device-resident images; d_field receives
 // the full-resolution field.  Returns REGB_OK, REGB_FALSE or REGB_CANCELLED.
 regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int pix, float* d_field,
                          const regb_cdm_param& p, volatile const int* terminated, cudaStream_t st,
-                         int* iterations = nullptr);
+                         int* iterations = nullptr, CdmScheduler* sched = nullptr);
 
 }  // namespace regb

@@ -107,5 +107,7 @@ cudaError_t launch_upsample_field_x2(const float* in, int iw, int ih, int id, fl
 // Sum of a segment's cost partials -> float mean (the reference's mean(cost_map)).
 cudaError_t launch_cost_mean(const CdmSeg* segs, int nseg, float* out, cudaStream_t st);
 int cdm_blocks_for(long long nvox);
+// out[i] = segs[i].ctl->done
+cudaError_t launch_cdm_status(const CdmSeg* segs, int nseg, int* out, cudaStream_t st);
 
 }  // namespace regb

@@ -311,7 +311,7 @@ public:
 
 LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
                              const int* tdim, const float* to_vs, float* arg, const regb_linear_param& p,
-                             volatile const int* terminated, cudaStream_t st)
+                             volatile const int* terminated, cudaStream_t st, AffineBatcher* batcher)
 {
     opt::Vec a(arg, arg + 12);
     LinearRunner R(a);
@@ -365,6 +365,7 @@ LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float
     for (auto& L : R.levels)
         pairs.push_back({L.from, Dim3{L.fd[0], L.fd[1], L.fd[2]}, L.to, Dim3{L.td[0], L.td[1], L.td[2]}});
     AffineEvaluator ev(pairs, p.cost_type, st);
+    ev.set_batcher(batcher);
     R.eval = &ev;
     R.set_bound(p.reg_type, bound, absolute);
     R.search_count = search_count;

@@ -1,0 +1,114 @@
+#include "scheduler.h"
+#include <algorithm>
+#include <cstring>
+
+namespace regb {
+
+CdmScheduler::CdmScheduler(int iters_per_round) : iters_(std::max(1, iters_per_round))
+{
+    REGB_CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    int dev = 0;
+    REGB_CK(cudaGetDevice(&dev));
+    th_ = std::thread([this, dev] {
+        cudaSetDevice(dev);
+        loop();
+    });
+}
+
+CdmScheduler::~CdmScheduler()
+{
+    {
+        std::lock_guard<std::mutex> g(m_);
+        stop_ = true;
+    }
+    cv_.notify_all();
+    if (th_.joinable())
+        th_.join();
+    segs_.reset();
+    status_.reset();
+    if (st_) {
+        cudaStreamSynchronize(st_);
+        cudaStreamDestroy(st_);
+    }
+}
+
+void CdmScheduler::run(CdmLevel& lvl, int gradient_type, volatile const int* terminated)
+{
+    Entry e{&lvl, gradient_type, terminated};
+    std::unique_lock<std::mutex> lk(m_);
+    active_.push_back(&e);
+    cv_.notify_all();
+    cv_done_.wait(lk, [&] { return e.done; });
+}
+
+void CdmScheduler::loop()
+{
+    std::unique_lock<std::mutex> lk(m_);
+    for (;;) {
+        cv_.wait(lk, [&] { return stop_ || !active_.empty(); });
+        if (stop_ && active_.empty())
+            return;
+        std::vector<Entry*> cur(active_);
+        lk.unlock();
+        bool failed = false;
+        try {
+            const int n = (int)cur.size();
+            if ((int)h_segs_.n < n) {
+                const int cap = std::max(n, 2 * (int)h_segs_.n);
+                h_segs_.alloc(cap);
+                h_status_.alloc(cap);
+                segs_.alloc(cap, st_);
+                status_.alloc(cap, st_);
+            }
+            // segments sorted into groups of one (pixel type, gradient type)
+            std::vector<int> order(n);
+            for (int i = 0; i < n; ++i)
+                order[i] = i;
+            auto key = [&](int i) { return cur[i]->lvl->pix * 256 + cur[i]->gtype; };
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
+            for (int i = 0; i < n; ++i)
+                h_segs_.p[i] = cur[order[i]]->lvl->seg;
+            REGB_CK(cudaMemcpyAsync(segs_.p, h_segs_.p, sizeof(CdmSeg) * n, cudaMemcpyHostToDevice, st_));
+            for (int it = 0; it < iters_; ++it) {
+                for (int g0 = 0; g0 < n;) {
+                    int g1 = g0;
+                    int blocks = 1;
+                    while (g1 < n && key(order[g1]) == key(order[g0])) {
+                        blocks = std::max(blocks, h_segs_.p[g1].nblk);
+                        ++g1;
+                    }
+                    const Entry* e = cur[order[g0]];
+                    launch_iteration(segs_.p + g0, g1 - g0, blocks, e->lvl->pix, e->gtype, st_);
+                    g0 = g1;
+                }
+            }
+            REGB_CK(launch_cdm_status(segs_.p, n, status_.p, st_));
+            REGB_CK(cudaMemcpyAsync(h_status_.p, status_.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
+            REGB_CK(cudaStreamSynchronize(st_));
+            lk.lock();
+            ++rounds_;
+            for (int i = 0; i < n; ++i) {
+                Entry* e = cur[order[i]];
+                if (h_status_.p[i] || (e->term && *e->term)) {
+                    e->done = true;
+                    active_.erase(std::find(active_.begin(), active_.end(), e));
+                }
+            }
+        } catch (...) {
+            failed = true;
+            lk.lock();
+        }
+        if (failed) {
+            // leave every level that was in the failed round; its job reads the state
+            for (Entry* e : cur) {
+                e->done = true;
+                auto it = std::find(active_.begin(), active_.end(), e);
+                if (it != active_.end())
+                    active_.erase(it);
+            }
+        }
+        cv_done_.notify_all();
+    }
+}
+
+}  // namespace regb
