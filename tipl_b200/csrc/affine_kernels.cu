@@ -174,22 +174,25 @@ __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __r
         xb.set(T, (two ? rb : r) % fd.h, (two ? rb : r) / fd.h);
         const uint8_t* __restrict__ fa = tk.fixed + (long long)r * fd.w;
         const uint8_t* __restrict__ fb = tk.fixed + (long long)(two ? rb : r) * fd.w;
+        // rows r and rb share every FP instruction (packed pairs)
+        const float2 yt0 = make_float2(xa.yt[0], xb.yt[0]), yt1 = make_float2(xa.yt[1], xb.yt[1]),
+                     yt2 = make_float2(xa.yt[2], xb.yt[2]);
+        const float2 zt0 = make_float2(xa.zt[0], xb.zt[0]), zt1 = make_float2(xa.zt[1], xb.zt[1]),
+                     zt2 = make_float2(xa.zt[2], xb.zt[2]);
+        const float2 s0 = bc2(cx.s[0]), s1 = bc2(cx.s[1]), s2 = bc2(cx.s[2]);
         float fx = (float)lane;
         for (int x = lane; x < fd.w; x += 32, fx += 32.0f) {
-            float px, py, pz;
-            U8Sample A, B;
-            xa.at(cx, fx, px, py, pz);
-            A.prepare(moving, g, px, py, pz);
-            xb.at(cx, fx, px, py, pz);
-            B.prepare(moving, g, px, py, pz);
-            B.ok = B.ok && two;
+            // x*T[3a] is the same in both rows: one scalar product (never contracted) per axis
+            const float2 px = add2(add2(add2(bc2(__fmul_rn(fx, cx.t0[0])), yt0), zt0), s0);
+            const float2 py = add2(add2(add2(bc2(__fmul_rn(fx, cx.t0[1])), yt1), zt1), s1);
+            const float2 pz = add2(add2(add2(bc2(__fmul_rn(fx, cx.t0[2])), yt2), zt2), s2);
             const uint32_t fva = __ldg(fa + x);
             const uint32_t fvb = two ? (uint32_t)__ldg(fb + x) : 0u;
-            A.load(g);
-            B.load(g);
-            mi_count(sh, (fva << 8) | A.finish());
+            uint32_t ta, tb;
+            sample_u8_pair(moving, g, px, py, pz, true, two, ta, tb);
+            mi_count(sh, (fva << 8) | ta);
             if (two)
-                mi_count(sh, (fvb << 8) | B.finish());
+                mi_count(sh, (fvb << 8) | tb);
         }
     }
     __syncthreads();
@@ -262,27 +265,52 @@ __global__ void __launch_bounds__(kCorrThreads) corr_kernel(const AffineTask* __
     ColXform cx;
     cx.set(T);
     uint32_t sy = 0, syy = 0, sxy = 0;
-    for (int r = r0 + (threadIdx.x >> 5); r < r1; r += nw) {
-        const int yy = r % fd.h, zz = r / fd.h;
-        RowXform rx;
-        rx.set(T, yy, zz);
-        const uint8_t* __restrict__ frow = tk.fixed + (long long)r * fd.w;
-        float fx = (float)lane;
-        for (int x = lane; x < fd.w; x += 32, fx += 32.0f) {
-            uint32_t v = 0;
-            if (tk.mode == 1) {
-                const int ax = x + tk.shift[0], ay = yy + tk.shift[1], az = zz + tk.shift[2];
-                if (ax >= 0 && ay >= 0 && az >= 0 && ax < md.w && ay < md.h && az < md.d)
+    auto acc = [&](uint32_t f, uint32_t v) {
+        sy += v;
+        syy += v * v;
+        sxy += f * v;
+    };
+    if (tk.mode == 1) {
+        // the CPU resample's integer-shift copy (numerical/resampling.hpp:1243-1262)
+        for (int r = r0 + (threadIdx.x >> 5); r < r1; r += nw) {
+            const int yy = r % fd.h, zz = r / fd.h;
+            const uint8_t* __restrict__ frow = tk.fixed + (long long)r * fd.w;
+            const int ay = yy + tk.shift[1], az = zz + tk.shift[2];
+            const bool rowin = ay >= 0 && az >= 0 && ay < md.h && az < md.d;
+            for (int x = lane; x < fd.w; x += 32) {
+                const int ax = x + tk.shift[0];
+                uint32_t v = 0;
+                if (rowin && ax >= 0 && ax < md.w)
                     v = __ldg(moving + (az * md.h + ay) * md.w + ax);
-            } else {
-                float px, py, pz;
-                rx.at(cx, fx, px, py, pz);
-                v = sample_u8(moving, g, px, py, pz);
+                acc(__ldg(frow + x), v);
             }
-            const uint32_t f = __ldg(frow + x);
-            sy += v;
-            syy += v * v;
-            sxy += f * v;
+        }
+    } else {
+        for (int r = r0 + (threadIdx.x >> 5); r < r1; r += 2 * nw) {
+            const int rb = r + nw;
+            const bool two = rb < r1;
+            RowXform xa, xb;
+            xa.set(T, r % fd.h, r / fd.h);
+            xb.set(T, (two ? rb : r) % fd.h, (two ? rb : r) / fd.h);
+            const uint8_t* __restrict__ fa = tk.fixed + (long long)r * fd.w;
+            const uint8_t* __restrict__ fb = tk.fixed + (long long)(two ? rb : r) * fd.w;
+            const float2 yt0 = make_float2(xa.yt[0], xb.yt[0]), yt1 = make_float2(xa.yt[1], xb.yt[1]),
+                         yt2 = make_float2(xa.yt[2], xb.yt[2]);
+            const float2 zt0 = make_float2(xa.zt[0], xb.zt[0]), zt1 = make_float2(xa.zt[1], xb.zt[1]),
+                         zt2 = make_float2(xa.zt[2], xb.zt[2]);
+            const float2 s0 = bc2(cx.s[0]), s1 = bc2(cx.s[1]), s2 = bc2(cx.s[2]);
+            float fx = (float)lane;
+            for (int x = lane; x < fd.w; x += 32, fx += 32.0f) {
+                // x*T[3a] is the same in both rows: one scalar product (never contracted) per axis
+                const float2 px = add2(add2(add2(bc2(__fmul_rn(fx, cx.t0[0])), yt0), zt0), s0);
+                const float2 py = add2(add2(add2(bc2(__fmul_rn(fx, cx.t0[1])), yt1), zt1), s1);
+                const float2 pz = add2(add2(add2(bc2(__fmul_rn(fx, cx.t0[2])), yt2), zt2), s2);
+                uint32_t va, vb;
+                sample_u8_pair(moving, g, px, py, pz, true, two, va, vb);
+                acc(__ldg(fa + x), va);
+                if (two)
+                    acc(__ldg(fb + x), vb);
+            }
         }
     }
     __shared__ unsigned long long red[32];

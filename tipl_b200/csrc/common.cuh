@@ -226,6 +226,93 @@ struct U8Sample {
     }
 };
 
+// ---- packed pairs: sm_100 executes two FP32 adds/multiplies as one instruction,
+// each lane rounded exactly like the scalar IEEE operation, so two voxels can
+// share arithmetic instructions without changing a bit of either result.
+// One rule keeps that true: a packed product must never feed a packed add or
+// subtract, because the assembler contracts that pair into a fused multiply-add
+// (explicit .rn does not stop it for the packed forms).  Products that feed sums
+// are formed with the scalar __fmul_rn, which is never contracted. ----
+#define REGB_F32X2_OP(name, op)                                                                  \
+    __device__ __forceinline__ float2 name(float2 a, float2 b)                                  \
+    {                                                                                            \
+        float2 r;                                                                                \
+        asm("{\n\t.reg .b64 ra, rb, rd;\n\t"                                                   \
+            "mov.b64 ra, {%2, %3};\n\t"                                                          \
+            "mov.b64 rb, {%4, %5};\n\t" op " rd, ra, rb;\n\t"                                  \
+            "mov.b64 {%0, %1}, rd;\n\t}"                                                         \
+            : "=f"(r.x), "=f"(r.y)                                                               \
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                           \
+        return r;                                                                                \
+    }
+REGB_F32X2_OP(add2, "add.rn.f32x2")
+REGB_F32X2_OP(sub2, "sub.rn.f32x2")
+REGB_F32X2_OP(mul2, "mul.rn.f32x2")
+REGB_F32X2_OP(addrz2, "add.rz.f32x2")
+#undef REGB_F32X2_OP
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+
+// Two uint8 trilinear estimates (the reference's interpolation of sample_u8) at
+// (px.x, py.x, pz.x) and (px.y, py.y, pz.y), sharing every FP instruction.
+// enA/enB disable a lane; a disabled or rejected lane returns 0 and loads
+// nothing outside the volume.
+__device__ __forceinline__ void sample_u8_pair(const uint8_t* __restrict__ I, const SampleGeo& g, float2 px,
+                                               float2 py, float2 pz, bool enA, bool enB, uint32_t& oA,
+                                               uint32_t& oB)
+{
+    const bool okA = enA && !(px.x < 0.0f || py.x < 0.0f || pz.x < 0.0f) && (px.x < g.wl) && (py.x < g.hl) &&
+                     (pz.x < g.dl);
+    const bool okB = enB && !(px.y < 0.0f || py.y < 0.0f || pz.y < 0.0f) && (px.y < g.wl) && (py.y < g.hl) &&
+                     (pz.y < g.dl);
+    const float2 t23 = bc2(kTwo23);
+    // 2^23 + floor, per lane with the scalar round-toward-zero add
+    const float2 rx = make_float2(__fadd_rz(px.x, kTwo23), __fadd_rz(px.y, kTwo23));
+    const float2 ry = make_float2(__fadd_rz(py.x, kTwo23), __fadd_rz(py.y, kTwo23));
+    const float2 rz = make_float2(__fadd_rz(pz.x, kTwo23), __fadd_rz(pz.y, kTwo23));
+    const float2 fx = sub2(rx, t23), fy = sub2(ry, t23), fz = sub2(rz, t23);
+    const float2 p0 = sub2(px, fx), p1 = sub2(py, fy), p2 = sub2(pz, fz);
+    const float2 one = bc2(1.0f);
+    const float2 n0 = sub2(one, p0), n1 = sub2(one, p1), n2 = sub2(one, p2);
+    const float2 n0n1 = mul2(n0, n1), p0n1 = mul2(p0, n1), n0p1 = mul2(n0, p1), p0p1 = mul2(p0, p1);
+    const int w = g.w, wh = g.wh;
+    const uint8_t* qa = okA ? I + (((__float_as_int(rz.x) - 0x4B000000) * g.h + (__float_as_int(ry.x) - 0x4B000000)) *
+                                       w + (__float_as_int(rx.x) - 0x4B000000))
+                            : I;
+    const uint8_t* qb = okB ? I + (((__float_as_int(rz.y) - 0x4B000000) * g.h + (__float_as_int(ry.y) - 0x4B000000)) *
+                                       w + (__float_as_int(rx.y) - 0x4B000000))
+                            : I;
+    uint32_t a[8], b[8];
+    a[0] = __ldg(qa);
+    b[0] = __ldg(qb);
+    a[1] = __ldg(qa + 1);
+    b[1] = __ldg(qb + 1);
+    a[2] = __ldg(qa + w);
+    b[2] = __ldg(qb + w);
+    a[3] = __ldg(qa + w + 1);
+    b[3] = __ldg(qb + w + 1);
+    a[4] = __ldg(qa + wh);
+    b[4] = __ldg(qb + wh);
+    a[5] = __ldg(qa + wh + 1);
+    b[5] = __ldg(qb + wh + 1);
+    a[6] = __ldg(qa + wh + w);
+    b[6] = __ldg(qb + wh + w);
+    a[7] = __ldg(qa + wh + w + 1);
+    b[7] = __ldg(qb + wh + w + 1);
+    const float2 wt[8] = {mul2(n0n1, n2), mul2(p0n1, n2), mul2(n0p1, n2), mul2(p0p1, n2),
+                          mul2(n0n1, p2), mul2(p0n1, p2), mul2(n0p1, p2), mul2(p0p1, p2)};
+    float2 acc;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float2 v = sub2(make_float2(__uint_as_float(0x4B000000u | a[k]), __uint_as_float(0x4B000000u | b[k])),
+                              t23);
+        const float2 m = make_float2(__fmul_rn(v.x, wt[k].x), __fmul_rn(v.y, wt[k].y));  // feeds a sum: scalar
+        acc = (k == 0) ? m : add2(acc, m);
+    }
+    const float2 tr = make_float2(__fadd_rz(acc.x, kTwo23), __fadd_rz(acc.y, kTwo23));
+    oA = (okA && acc.x > 0.0f) ? (uint32_t)(__float_as_int(tr.x) - 0x4B000000) : 0u;
+    oB = (okB && acc.y > 0.0f) ? (uint32_t)(__float_as_int(tr.y) - 0x4B000000) : 0u;
+}
+
 // Per-row part of the transform: for a fixed row (y, z), y*T[3a+1] and z*T[3a+2]
 // of each axis a; the per-voxel remainder ((x*T0 + yT1) + zT2) + s keeps the
 // reference's summation order.  The x column and the shift are held once (ColXform)
