@@ -190,6 +190,32 @@ regb_status regb_linear(const regb_volume* from, const float from_vs[3], const r
                         const float to_vs[3], float arg[12], const regb_linear_param* param,
                         volatile const int* terminated, float* cost_out, long long* cost_evals);
 
+/* The state of the reference's linear_reg_runner when its GPU implementation is
+ * entered: linear_reg_imp<out,mr,uint8,3>(std::true_type, runner, cost_type,
+ * terminated) (reg/linear.hpp:597-604, instantiated by reg/linear_cu.hpp:1-19).
+ * Bounds and stage list are the runner's fields (linear_reg_runner, reg/linear.hpp:
+ * 298-306); multi_resolution is the template flag mr. */
+typedef struct {
+    float arg_upper[12];
+    float arg_lower[12];
+    int reg_list[8];       /* DOF stages, e.g. {1, 5, 7, 15} */
+    int n_reg;
+    unsigned int search_count;
+    int multi_resolution;  /* 1 = optimize<cost, true> (pyramid above 96^3) */
+    int cost_type;         /* regb_cost_type */
+    double precision;      /* default 0.001 */
+    int max_iterations;    /* default 128 */
+} regb_runner_state;
+/* Fills the runner state tipl::reg::linear would set up for param (no mask-based
+ * initialisation; that stays with the caller). */
+regb_status regb_runner_state_from_param(const int from_dim[3], const float from_vs[3], const int to_dim[3],
+                                         const float to_vs[3], const float arg[12], const regb_linear_param* param,
+                                         regb_runner_state* out);
+/* Runs the runner from that state on one image pair: arg in/out, final cost out. */
+regb_status regb_linear_run(const regb_volume* from, const float from_vs[3], const regb_volume* to,
+                            const float to_vs[3], float arg[12], const regb_runner_state* state,
+                            volatile const int* terminated, float* cost_out, long long* cost_evals);
+
 /* ---- serving engine ---------------------------------------------------------------
  * No counterpart in the reference (which registers one pair per call): registration
  * jobs submitted as they arrive run concurrently on one GPU.  Their affine probe sets

@@ -1,0 +1,61 @@
+// Drop-in check: the reference's own tipl::reg::linear and tipl::reg::cdm_common,
+// compiled by the host compiler with -DTIPL_USE_CUDA, run their GPU branch through
+// include/tipl_b200/tipl_gpu.hpp (libregb200.so) or their CPU branch.
+//
+//   tipl_drop_in linear|cdm gpu|cpu w h d fixed.u8 moving.u8 out.bin
+// linear writes cost (float) + 12 params; cdm writes ok (int32) + the field.
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <vector>
+#include "reg/linear.hpp"
+#include "reg/cdm.hpp"
+#include "tipl_b200/tipl_gpu.hpp"
+
+static std::vector<unsigned char> read_all(const char* p, size_t n)
+{
+    std::vector<unsigned char> v(n);
+    std::ifstream f(p, std::ios::binary);
+    f.read((char*)v.data(), (std::streamsize)n);
+    if (!f)
+        throw std::runtime_error(std::string("cannot read ") + p);
+    return v;
+}
+
+int main(int argc, char** argv)
+{
+    if (argc != 9) {
+        std::fprintf(stderr, "usage: %s linear|cdm gpu|cpu w h d fixed moving out\n", argv[0]);
+        return 2;
+    }
+    const std::string what = argv[1];
+    const bool gpu = std::string(argv[2]) == "gpu";
+    const tipl::shape<3> sh(std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]));
+    auto fixed = read_all(argv[6], sh.size());
+    auto moving = read_all(argv[7], sh.size());
+    tipl::const_pointer_image<3, unsigned char> F(fixed.data(), sh), M(moving.data(), sh);
+    std::ofstream out(argv[8], std::ios::binary);
+    bool terminated = false;
+    if (what == "linear") {
+        tipl::affine_param<float, 3> arg;
+        tipl::reg::linear_reg_param param;
+        param.cuda = gpu;
+        float cost = tipl::reg::linear<void>(std::vector<tipl::const_pointer_image<3, unsigned char>>{F},
+                                             tipl::vector<3>(1, 1, 1),
+                                             std::vector<tipl::const_pointer_image<3, unsigned char>>{M},
+                                             tipl::vector<3>(1, 1, 1), arg, param, terminated);
+        out.write((const char*)&cost, 4);
+        out.write((const char*)arg.data(), 48);
+        std::printf("linear %s cost %.6f\n", gpu ? "gpu" : "cpu", cost);
+    } else {
+        tipl::image<3, tipl::vector<3>> dis;
+        bool ok = tipl::reg::cdm_common<void, unsigned char, 3>({F}, {M}, dis, terminated, tipl::reg::cdm_param(), gpu);
+        int32_t okv = ok ? 1 : 0;
+        out.write((const char*)&okv, 4);
+        if (ok)
+            out.write((const char*)&dis[0][0], (std::streamsize)(dis.size() * 12));
+        std::printf("cdm %s ok %d\n", gpu ? "gpu" : "cpu", okv);
+    }
+    return 0;
+}

@@ -1,0 +1,57 @@
+"""The drop-in boundary end to end: the reference's own tipl::reg::cdm_common and
+tipl::reg::linear (compiled with -DTIPL_USE_CUDA by the host compiler) take their GPU
+branch through include/tipl_b200/tipl_gpu.hpp on libregb200.so.  The GPU branch's CDM
+field must equal the reference CPU branch's bit for bit; the affine search, whose
+reference optimiser runs its line search and L-BFGS in racing threads, must reach a
+final cost within 1% of the CPU branch."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from tipl_b200 import phantom as ph
+
+pytestmark = pytest.mark.gpu
+BIN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cpp", "tipl_drop_in")
+
+
+@pytest.fixture(scope="module")
+def volumes(tmp_path_factory):
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    if not os.path.exists(BIN):
+        pytest.skip("drop-in binary not built (needs the reference headers at build time)")
+    d = tmp_path_factory.mktemp("dropin")
+    rng = np.random.default_rng(ph.seed_for(6, 0))
+    t, m, _ = ph.affine_pair((40, 44, 36), rng=rng)
+    f8, m8 = ph.normalize_to_u8(t), ph.normalize_to_u8(m)
+    f8.tofile(d / "f.u8")
+    m8.tofile(d / "m.u8")
+    return d, f8.shape
+
+
+def run(d, shape, what, where):
+    out = d / f"{what}_{where}.bin"
+    z, y, x = shape
+    r = subprocess.run([BIN, what, where, str(x), str(y), str(z), str(d / "f.u8"), str(d / "m.u8"), str(out)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    return np.fromfile(out, dtype=np.uint8)
+
+
+def test_cdm_common_gpu_branch_equals_cpu_branch(volumes):
+    d, shape = volumes
+    g = run(d, shape, "cdm", "gpu")
+    c = run(d, shape, "cdm", "cpu")
+    assert g[:4].view(np.int32)[0] == 1 and c[:4].view(np.int32)[0] == 1
+    assert np.array_equal(g, c)
+
+
+def test_linear_gpu_branch_close_to_cpu_branch(volumes):
+    d, shape = volumes
+    g = run(d, shape, "linear", "gpu").view(np.float32)
+    c = run(d, shape, "linear", "cpu").view(np.float32)
+    assert abs(g[0] - c[0]) <= 0.01 * abs(c[0]), (g[0], c[0])

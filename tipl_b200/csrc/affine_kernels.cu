@@ -165,9 +165,10 @@ __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __r
     const float* __restrict__ T = tk.T;
     ColXform cx;
     cx.set(T);
-    // two rows per warp at a time: the second row's corner loads overlap the first's
-    for (int r = r0 + (threadIdx.x >> 5); r < r1; r += 2 * nw) {
-        const int rb = r + nw;
+    // two adjacent rows per warp at a time: their loads overlap, and the second
+    // row's trilinear corners mostly fall on lines the first row just cached
+    for (int r = r0 + 2 * (threadIdx.x >> 5); r < r1; r += 2 * nw) {
+        const int rb = r + 1;
         const bool two = rb < r1;
         RowXform xa, xb;
         xa.set(T, r % fd.h, r / fd.h);
@@ -286,8 +287,8 @@ __global__ void __launch_bounds__(kCorrThreads) corr_kernel(const AffineTask* __
             }
         }
     } else {
-        for (int r = r0 + (threadIdx.x >> 5); r < r1; r += 2 * nw) {
-            const int rb = r + nw;
+        for (int r = r0 + 2 * (threadIdx.x >> 5); r < r1; r += 2 * nw) {
+            const int rb = r + 1;
             const bool two = rb < r1;
             RowXform xa, xb;
             xa.set(T, r % fd.h, r / fd.h);

@@ -555,4 +555,48 @@ regb_status regb_linear(const regb_volume* from, const float from_vs[3], const r
     });
 }
 
+regb_status regb_runner_state_from_param(const int from_dim[3], const float from_vs[3], const int to_dim[3],
+                                         const float to_vs[3], const float arg[12], const regb_linear_param* param,
+                                         regb_runner_state* out)
+{
+    return guarded([&] {
+        if (!from_dim || !from_vs || !to_dim || !to_vs || !arg || !out)
+            throw Failure(REGB_ERR_ARG, "null argument");
+        regb_linear_param p;
+        regb_linear_param_default(&p);
+        if (param)
+            p = *param;
+        runner_state_from_param(from_dim, from_vs, to_dim, to_vs, arg, p, *out);
+        return REGB_OK;
+    });
+}
+
+regb_status regb_linear_run(const regb_volume* from, const float from_vs[3], const regb_volume* to,
+                            const float to_vs[3], float arg[12], const regb_runner_state* state,
+                            volatile const int* terminated, float* cost_out, long long* cost_evals)
+{
+    return guarded([&] {
+        check_vol(from, "from");
+        check_vol(to, "to");
+        if (from->dtype != REGB_U8 || to->dtype != REGB_U8)
+            throw Failure(REGB_ERR_ARG, "linear takes uint8 volumes (reg/linear.hpp:622-629)");
+        if (!from_vs || !to_vs || !arg || !state)
+            throw Failure(REGB_ERR_ARG, "null voxel size / arg / state");
+        if (state->cost_type != REGB_COST_MI && state->cost_type != REGB_COST_CORR)
+            throw Failure(REGB_ERR_ARG, "cost_type must be MI or CORR");
+        Stream s;
+        Staged a, b;
+        a.in(from->ptr, nvox(from->dim), from->location, s.s, true);
+        b.in(to->ptr, nvox(to->dim), to->location, s.s, true);
+        LinearResult r = linear_register_state((const uint8_t*)a.d, from->dim, from_vs, (const uint8_t*)b.d, to->dim,
+                                               to_vs, arg, *state, terminated, s.s);
+        s.sync();
+        if (cost_out)
+            *cost_out = r.cost;
+        if (cost_evals)
+            *cost_evals = r.evals;
+        return (terminated && *terminated) ? REGB_CANCELLED : REGB_OK;
+    });
+}
+
 }  // extern "C"

@@ -143,6 +143,12 @@ LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float
                              const int* tdim, const float* to_vs, float* arg, const regb_linear_param& p,
                              volatile const int* terminated, cudaStream_t st, AffineBatcher* batcher = nullptr);
 
+LinearResult linear_register_state(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
+                                   const int* tdim, const float* to_vs, float* arg, const regb_runner_state& s,
+                                   volatile const int* terminated, cudaStream_t st);
+void runner_state_from_param(const int* fdim, const float* from_vs, const int* tdim, const float* to_vs,
+                             const float* arg, const regb_linear_param& p, regb_runner_state& s);
+
 // The CDM driver (reg/cdm.hpp:373-474) on device-resident images; d_field receives
 // the full-resolution field.  Returns REGB_OK, REGB_FALSE or REGB_CANCELLED.
 regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int pix, float* d_field,

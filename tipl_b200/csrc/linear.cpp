@@ -309,25 +309,26 @@ public:
     }
 };
 
-LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
-                             const int* tdim, const float* to_vs, float* arg, const regb_linear_param& p,
-                             volatile const int* terminated, cudaStream_t st, AffineBatcher* batcher)
+// Runs the runner from an explicit state: the reference runner's fields at the
+// point its GPU implementation is entered (reg/linear.hpp:597-604).
+static LinearResult run_state(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
+                              const int* tdim, const float* to_vs, float* arg, const regb_runner_state& s,
+                              volatile const int* terminated, cudaStream_t st, AffineBatcher* batcher)
 {
     opt::Vec a(arg, arg + 12);
     LinearRunner R(a);
     R.terminated = terminated;
-    R.cost_type = p.cost_type;
-    const float(*bound)[8] = kBound[(p.bound >= 0 && p.bound < 3) ? p.bound : 0];
-    const bool narrow = (p.bound == REGB_BOUND_NARROW);
-    bool absolute = p.absolute_bound != 0;
-    unsigned int search_count = p.search_count;
-    if (narrow) {  // reg/linear.hpp:645-651
-        absolute = false;
-        search_count = 0;
-    } else
-        absolute = true;
+    R.cost_type = s.cost_type;
+    R.arg_upper.assign(s.arg_upper, s.arg_upper + 12);
+    R.arg_lower.assign(s.arg_lower, s.arg_lower + 12);
+    R.reg_list.assign(s.reg_list, s.reg_list + std::max(0, std::min(s.n_reg, 8)));
+    if (R.reg_list.empty())
+        throw Failure(REGB_ERR_ARG, "empty reg_list");
+    R.search_count = s.search_count;
+    R.precision = s.precision;
+    R.max_iterations = s.max_iterations;
 
-    // pyramid: a level below while the fixed volume exceeds 96^3 (reg/linear.hpp:527-545)
+    // pyramid: a level below while the fixed volume exceeds 96^3 (reg/linear.hpp:309-322, 527-545)
     std::vector<DevBuf<uint8_t>> bufs;
     LinearRunner::Level L0;
     L0.from = d_from;
@@ -339,7 +340,7 @@ LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float
         L0.tvs[i] = to_vs[i];
     }
     R.levels.push_back(L0);
-    if (!narrow) {
+    if (s.multi_resolution) {
         for (;;) {
             const LinearRunner::Level& c = R.levels.back();
             const long long sz = (long long)c.fd[0] * c.fd[1] * c.fd[2];
@@ -364,22 +365,65 @@ LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float
     std::vector<AffineEvaluator::Pair> pairs;
     for (auto& L : R.levels)
         pairs.push_back({L.from, Dim3{L.fd[0], L.fd[1], L.fd[2]}, L.to, Dim3{L.td[0], L.td[1], L.td[2]}});
-    AffineEvaluator ev(pairs, p.cost_type, st);
+    AffineEvaluator ev(pairs, s.cost_type, st);
     ev.set_batcher(batcher);
     R.eval = &ev;
-    R.set_bound(p.reg_type, bound, absolute);
-    R.search_count = search_count;
-    double cost;
-    if (narrow) {
-        R.max_iterations = 128;
-        cost = R.run_optimize(0, 0);
-    } else
-        cost = R.run_optimize_mr(0);
+    // optimize<cost, mr> (reg/linear.hpp:552-560)
+    const double cost = s.multi_resolution ? R.run_optimize_mr(0) : R.run_optimize(0, 0);
     std::copy(a.begin(), a.end(), arg);
     LinearResult out;
     out.cost = (float)cost;
     out.evals = R.evals;
     return out;
+}
+
+// The runner state tipl::reg::linear sets up (reg/linear.hpp:631-651, 365-420):
+// bounds from the bound table around the identity (absolute) or around arg
+// (narrow), the DOF stage list of the registration type, and multi-resolution
+// with the line search except for the narrow bound.
+void runner_state_from_param(const int* fdim, const float* from_vs, const int* tdim, const float* to_vs,
+                             const float* arg, const regb_linear_param& p, regb_runner_state& s)
+{
+    opt::Vec a(arg, arg + 12);
+    LinearRunner R(a);
+    LinearRunner::Level L0{};
+    for (int i = 0; i < 3; ++i) {
+        L0.fd[i] = fdim[i];
+        L0.td[i] = tdim[i];
+        L0.fvs[i] = from_vs[i];
+        L0.tvs[i] = to_vs[i];
+    }
+    R.levels.push_back(L0);
+    const float(*bound)[8] = kBound[(p.bound >= 0 && p.bound < 3) ? p.bound : 0];
+    const bool narrow = (p.bound == REGB_BOUND_NARROW);
+    R.set_bound(p.reg_type, bound, narrow ? false : true);
+    std::memset(&s, 0, sizeof(s));
+    std::copy(R.arg_upper.begin(), R.arg_upper.end(), s.arg_upper);
+    std::copy(R.arg_lower.begin(), R.arg_lower.end(), s.arg_lower);
+    s.n_reg = (int)R.reg_list.size();
+    for (int i = 0; i < s.n_reg; ++i)
+        s.reg_list[i] = R.reg_list[i];
+    s.search_count = narrow ? 0 : p.search_count;
+    s.multi_resolution = narrow ? 0 : 1;
+    s.cost_type = p.cost_type;
+    s.precision = 0.001;
+    s.max_iterations = 128;
+}
+
+LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
+                             const int* tdim, const float* to_vs, float* arg, const regb_linear_param& p,
+                             volatile const int* terminated, cudaStream_t st, AffineBatcher* batcher)
+{
+    regb_runner_state s;
+    runner_state_from_param(fdim, from_vs, tdim, to_vs, arg, p, s);
+    return run_state(d_from, fdim, from_vs, d_to, tdim, to_vs, arg, s, terminated, st, batcher);
+}
+
+LinearResult linear_register_state(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
+                                   const int* tdim, const float* to_vs, float* arg, const regb_runner_state& s,
+                                   volatile const int* terminated, cudaStream_t st)
+{
+    return run_state(d_from, fdim, from_vs, d_to, tdim, to_vs, arg, s, terminated, st, nullptr);
 }
 
 }  // namespace regb
