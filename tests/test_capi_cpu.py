@@ -82,3 +82,32 @@ def test_param_defaults(L):
     L.regb_cdm_param_default(C.byref(q))
     assert (q.resolution, q.min_dimension, chr(q.gradient_type)) == (2.0, 16, "r")
     assert abs(q.speed - 0.3) < 1e-7 and abs(q.smoothing - 0.05) < 1e-7
+
+
+def test_runner_state_from_param(L):
+    """The runner state of tipl::reg::linear for an affine MI registration: the four DOF
+    stages, bounds around the identity from reg_bound (reg/linear.hpp:258-263, 370-420)."""
+    p = _lib.LinearParam()
+    L.regb_linear_param_default(C.byref(p))
+    s = _lib.RunnerState()
+    fd = np.array([182, 218, 182], np.int32)
+    vs = np.array([1, 1, 1], np.float32)
+    arg = np.array([0, 0, 0, 0, 0, 0, 1, 1, 1, 0, 0, 0], np.float32)
+    st = L.regb_runner_state_from_param(fd.ctypes.data_as(C.c_void_p), vs.ctypes.data_as(C.c_void_p),
+                                        fd.ctypes.data_as(C.c_void_p), vs.ctypes.data_as(C.c_void_p),
+                                        arg.ctypes.data_as(C.c_void_p), C.byref(p), C.byref(s))
+    assert st == 0
+    assert list(s.reg_list[: s.n_reg]) == [1, 5, 7, 15]
+    assert s.search_count == 16 and s.multi_resolution == 1 and s.max_iterations == 128
+    up = np.array(s.arg_upper[:], np.float32)
+    lo = np.array(s.arg_lower[:], np.float32)
+    assert up[0] == np.float32(np.float32(182 * 0.5) * np.float32(0.75))   # half extent * 0.75
+    assert up[1] == np.float32(np.float32(218 * 0.5) * np.float32(0.75))
+    assert up[3] == np.float32(0.0) + np.float32(1.57079632679) * np.float32(0.4)
+    assert up[6] == np.float32(1.5) and lo[6] == np.float32(0.7)
+    assert up[9] == np.float32(0.1) and lo[9] == np.float32(-0.1)
+    p.bound = 1  # narrow: around arg, no search, no pyramid
+    L.regb_runner_state_from_param(fd.ctypes.data_as(C.c_void_p), vs.ctypes.data_as(C.c_void_p),
+                                   fd.ctypes.data_as(C.c_void_p), vs.ctypes.data_as(C.c_void_p),
+                                   arg.ctypes.data_as(C.c_void_p), C.byref(p), C.byref(s))
+    assert s.search_count == 0 and s.multi_resolution == 0

@@ -49,6 +49,12 @@ class Stats(C.Structure):
                 ("corr_bytes", C.c_double), ("corr_ms", C.c_double)]
 
 
+class RunnerState(C.Structure):
+    _fields_ = [("arg_upper", C.c_float * 12), ("arg_lower", C.c_float * 12), ("reg_list", C.c_int * 8),
+                ("n_reg", C.c_int), ("search_count", C.c_uint), ("multi_resolution", C.c_int),
+                ("cost_type", C.c_int), ("precision", C.c_double), ("max_iterations", C.c_int)]
+
+
 class EngineConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_active", C.c_int), ("gather_us", C.c_int),
                 ("cdm_iters_per_round", C.c_int)]
@@ -113,6 +119,11 @@ _SIGS = {
     "regb_cdm_smooth": (C.c_int, [C.POINTER(Field), C.POINTER(Field), C.c_float, C.c_void_p]),
     "regb_cdm": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.POINTER(Field), C.POINTER(CdmParam),
                            C.c_void_p]),
+    "regb_runner_state_from_param": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.POINTER(LinearParam), C.POINTER(RunnerState)]),
+    "regb_linear_run": (C.c_int, [C.POINTER(Volume), C.c_void_p, C.POINTER(Volume), C.c_void_p, C.c_void_p,
+                                  C.POINTER(RunnerState), C.c_void_p, C.POINTER(C.c_float),
+                                  C.POINTER(C.c_longlong)]),
     "regb_engine_config_default": (None, [C.POINTER(EngineConfig)]),
     "regb_job_default": (None, [C.POINTER(Job)]),
     "regb_engine_create": (C.c_int, [C.POINTER(EngineConfig), C.POINTER(C.c_void_p)]),
