@@ -231,6 +231,22 @@ def run_served(args, rank, world, dist):
     subjects = make_subjects(f8, args.batch, seed=rank)
     dev_subj = [torch.from_numpy(m).cuda() for m in subjects]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    # the plain single-job path on the same subjects, one registration at a time
+    fdev = torch.from_numpy(f8).cuda()
+    t_plain = 0.0
+    if args.plain_steps:
+        tb.reg.linear(fdev, VS, dev_subj[0], VS)  # warm-up
+        for k in range(args.plain_steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            tb.reg.linear(fdev, VS, dev_subj[k % len(dev_subj)], VS)
+            b.record()
+            torch.cuda.synchronize()
+            t_plain += a.elapsed_time(b) / 1000.0
+    plain = args.plain_steps / t_plain if args.plain_steps else None
     eng = tb.Engine(max_active=max(args.batch, 1))
     tid = eng.add_template(torch.from_numpy(f8).cuda())
     lat, costs, evals = [], [], 0
@@ -279,17 +295,19 @@ def run_served(args, rank, world, dist):
     t_e2e, _ = timed(subjects, False)
     estats = eng.stats()
     eng.close()
-    return t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects
+    return t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects, plain
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="plain", choices=["plain", "served"])
+    ap.add_argument("--mode", default="served", choices=["plain", "served"])
     ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--plain-steps", type=int, default=3,
+                    help="served mode: plain single-job registrations timed afterwards for the served/plain ratio")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel-case", choices=["mi", "corr"], default=None,
                     help="run only K-candidate cost batches of the full-size pair (for profiler captures)")
@@ -408,7 +426,7 @@ def main():
 
 
 def served_line(args, rank, world, dist, torch):
-    t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects = run_served(args, rank, world, dist)
+    t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects, plain = run_served(args, rank, world, dist)
 
     def maxall(x):
         if not dist:
@@ -449,6 +467,8 @@ def served_line(args, rank, world, dist, torch):
                            "latency_ms": {"p50": pct(0.50), "p95": pct(0.95), "p99": pct(0.99)},
                            "engine": {"affine_launches": estats["affine_launches"],
                                       "affine_tasks": estats["affine_tasks"]},
+                           "plain_single_job_registrations_per_s": plain,
+                           "served_over_plain": (regs / t_dev / world) / plain if plain else None,
                            "parallelism": f"replicas x{world}"},
                 "roofline": {"bound": "hbm", "kernel": "mi_kernel", "achieved": achieved, "peak": hbm,
                              "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,

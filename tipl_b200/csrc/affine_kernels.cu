@@ -167,6 +167,7 @@ __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __r
     cx.set(T);
     // two adjacent rows per warp at a time: their loads overlap, and the second
     // row's trilinear corners mostly fall on lines the first row just cached
+    // (neighbouring warps work on neighbouring pairs at the same time)
     for (int r = r0 + 2 * (threadIdx.x >> 5); r < r1; r += 2 * nw) {
         const int rb = r + 1;
         const bool two = rb < r1;
