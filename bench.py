@@ -39,6 +39,10 @@ SHAPE = (182, 218, 182)  # numpy (z, y, x) = 182 x 218 x 182 voxels
 VS = (1.0, 1.0, 1.0)
 METRIC = "registrations/s (affine 12-DOF MI, 182x218x182 uint8, 1 mm)"
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) per voxel evaluation of mi_kernel, from one ncu capture of a
+# 12-candidate launch on the 182x218x182 pair (profiles/mi_kernel_affine_182x218x182.md:
+# 17.613568 MB / 86.65 M voxel evaluations); scaled to each bench launch by its voxels.
+MI_DRAM_BYTES_PER_VOXEL_EVAL = 17.613568e6 / (12 * 7221032)
 
 
 def env_rank():
@@ -411,7 +415,9 @@ def main():
                            "final_cost_mean": float(np.mean(costs)), "cost_evals_per_registration":
                                evals / max(1, args.steps), "parallelism": f"replicas x{world}"},
                 "roofline": {"bound": "hbm", "kernel": "mi_kernel", "achieved": achieved, "peak": hbm,
-                             "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                             "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
+                             "traffic": MI_DRAM_BYTES_PER_VOXEL_EVAL * st.mi_voxels / max(1, st.mi_launches),
+                             "traffic_note": "ncu DRAM bytes per voxel evaluation x this run's voxels per launch",
                              "launches": st.mi_launches, "avg_launch_ms": st.mi_ms / max(1, st.mi_launches),
                              "bytes_per_launch": st.mi_bytes / max(1, st.mi_launches)},
                 "cpu_baseline": cpu,
@@ -471,7 +477,9 @@ def served_line(args, rank, world, dist, torch):
                            "served_over_plain": (regs / t_dev / world) / plain if plain else None,
                            "parallelism": f"replicas x{world}"},
                 "roofline": {"bound": "hbm", "kernel": "mi_kernel", "achieved": achieved, "peak": hbm,
-                             "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                             "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
+                             "traffic": MI_DRAM_BYTES_PER_VOXEL_EVAL * st.mi_voxels / max(1, st.mi_launches),
+                             "traffic_note": "ncu DRAM bytes per voxel evaluation x this run's voxels per launch",
                              "launches": st.mi_launches, "avg_launch_ms": st.mi_ms / max(1, st.mi_launches),
                              "bytes_per_launch": st.mi_bytes / max(1, st.mi_launches)},
                 "cpu_baseline": cpu,
