@@ -167,6 +167,38 @@ def run_reference(args):
     return 0
 
 
+def cdm_case(args):
+    """CDM registrations of a 182x218x182 uint8 pair (template vs the template warped by a
+    smooth field, max 4 voxels), min_dimension 32: levels 23/46/91 iterate."""
+    import torch
+
+    import tipl_b200 as tb
+    from tipl_b200 import _lib
+    from tipl_b200 import phantom as ph
+
+    rng = np.random.default_rng(ph.seed_for(4, 0))
+    t = ph.class_phantom(SHAPE, rng)
+    d = ph.smooth_field(SHAPE, rng, 6.0, 4.0)
+    m = ph.rician(ph.warp(t, d), rng)
+    It = torch.from_numpy(ph.normalize_to_u8(t)).cuda()
+    Is = torch.from_numpy(ph.normalize_to_u8(m)).cuda()
+    p = tb.reg.cdm_param(min_dimension=32)
+    field, ok = tb.reg.cdm(It, Is, p)  # warm-up
+    L = _lib.lib()
+    L.regb_stats_reset(0)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    field, ok = tb.reg.cdm(It, Is, p, out=field)
+    b.record()
+    torch.cuda.synchronize()
+    st = _lib.Stats()
+    L.regb_stats_get(st)
+    print(json.dumps({"kernel_case": "cdm", "ok": bool(ok), "ms": a.elapsed_time(b), "launches": st.launches,
+                      "field_rms": float(field.float().pow(2).sum(-1).sqrt().mean())}))
+    return 0
+
+
 def kernel_case(args):
     """Three launches of one cost kernel on the full-size pair, K candidates each."""
     import torch
@@ -313,12 +345,14 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=3,
                     help="served mode: plain single-job registrations timed afterwards for the served/plain ratio")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel-case", choices=["mi", "corr"], default=None,
+    ap.add_argument("--kernel-case", choices=["mi", "corr", "cdm"], default=None,
                     help="run only K-candidate cost batches of the full-size pair (for profiler captures)")
     ap.add_argument("--k", type=int, default=12)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernel_case == "cdm":
+        return cdm_case(args)
     if args.kernel_case:
         return kernel_case(args)
 

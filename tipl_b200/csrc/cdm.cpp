@@ -8,8 +8,8 @@
 // most 1 (reg/cdm.hpp:400-405).
 //
 // Each iteration is the kernel sequence of cdm_kernels.cu; the loop decisions run
-// on the device (CdmCtl), and this plain, single-job driver reads the done flag
-// back after every iteration, as the reference reads its cost back.
+// on the device (CdmCtl).  This single-job driver replays the iterations through
+// a CUDA graph and reads the done flag back once per graph launch.
 #include <algorithm>
 #include <cfloat>
 #include <cstring>
@@ -17,8 +17,54 @@
 #include "cdm_level.h"
 #include "host.h"
 #include "scheduler.h"
+#include "stats.h"
 
 namespace regb {
+
+void GraphExec::capture(const std::function<void(cudaStream_t)>& body)
+{
+    reset();
+    cudaStream_t cs;
+    REGB_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    const long long before = g_launches.load();
+    if (e == cudaSuccess) {
+        try {
+            body(cs);
+        } catch (...) {
+            cudaStreamEndCapture(cs, &graph);
+            if (graph)
+                cudaGraphDestroy(graph);
+            cudaStreamDestroy(cs);
+            throw;
+        }
+        e = cudaStreamEndCapture(cs, &graph);
+    }
+    // captured launches are counted when the graph runs, once per replay
+    nodes = g_launches.load() - before;
+    g_launches.fetch_sub(nodes);
+    if (e == cudaSuccess)
+        e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph)
+        cudaGraphDestroy(graph);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess)
+        throw_cuda(e, "graph capture");
+}
+
+void GraphExec::launch(cudaStream_t st)
+{
+    REGB_CK(cudaGraphLaunch(exec, st));
+    count_launch(nodes);
+}
+
+void GraphExec::reset()
+{
+    if (exec)
+        cudaGraphExecDestroy(exec);
+    exec = nullptr;
+}
 
 void CdmLevel::init(const void* It_, const void* Is_, int w, int h, int d, int pix_, const regb_cdm_param& p,
                     float* best, cudaStream_t st)
@@ -65,11 +111,8 @@ void CdmLevel::init(const void* It_, const void* Is_, int w, int h, int d, int p
 void launch_iteration(const CdmSeg* d_segs, int nseg, int blocks, int pix, int gradient_type, cudaStream_t st)
 {
     REGB_CK(launch_cdm_compose(d_segs, nseg, blocks, pix, st));
-    REGB_CK(launch_cdm_gradient(d_segs, nseg, blocks, pix, gradient_type, st));
-    REGB_CK(launch_cdm_control(d_segs, nseg, blocks, st));
-    REGB_CK(launch_cdm_best_copy(d_segs, nseg, blocks, st));
-    REGB_CK(launch_cdm_poisson(d_segs, nseg, blocks, 12, st));
-    REGB_CK(launch_cdm_theta(d_segs, nseg, blocks, st));
+    REGB_CK(launch_cdm_gradient(d_segs, nseg, blocks, pix, gradient_type, st));  // + loop decisions
+    REGB_CK(launch_cdm_poisson(d_segs, nseg, blocks, 12, st));                    // + best_d copy, theta
     REGB_CK(launch_cdm_accumulate(d_segs, nseg, blocks, st));
     REGB_CK(launch_cdm_smooth(d_segs, nseg, blocks, st));
 }
@@ -146,16 +189,26 @@ regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int
             if (terminated && *terminated && !run.h_ctl.done)
                 status = REGB_CANCELLED;
         }
-        for (int it = 0; !sched && it < 201; ++it) {
-            if (terminated && *terminated) {
-                status = REGB_CANCELLED;
-                break;
+        if (!sched) {
+            // kIters iterations per graph launch; the loop decisions live on the
+            // device, so iterations launched after the loop has ended are no-ops
+            constexpr int kIters = 4;
+            GraphExec g;
+            g.capture([&](cudaStream_t cs) {
+                for (int k = 0; k < kIters; ++k)
+                    launch_iteration(run.d_seg.p, 1, run.seg.nblk, pix, p.gradient_type, cs);
+            });
+            for (int it = 0; it < 201; it += kIters) {
+                if (terminated && *terminated) {
+                    status = REGB_CANCELLED;
+                    break;
+                }
+                g.launch(st);
+                REGB_CK(cudaMemcpyAsync(&run.h_ctl, run.ctl.p, sizeof(CdmCtl), cudaMemcpyDeviceToHost, st));
+                REGB_CK(cudaStreamSynchronize(st));
+                if (run.h_ctl.done)
+                    break;
             }
-            launch_iteration(run.d_seg.p, 1, run.seg.nblk, pix, p.gradient_type, st);
-            REGB_CK(cudaMemcpyAsync(&run.h_ctl, run.ctl.p, sizeof(CdmCtl), cudaMemcpyDeviceToHost, st));
-            REGB_CK(cudaStreamSynchronize(st));
-            if (run.h_ctl.done)
-                break;
         }
         iters += run.h_ctl.iters_run;
         if (run.h_ctl.done == 2)

@@ -3,12 +3,12 @@
 // level (CdmSeg), blockIdx.x < seg.nblk strides over its voxels.
 //
 // One iteration of a level (reg/cdm.hpp:418-470) is the launch sequence
-//   compose -> gradient -> control -> best_copy -> poisson -> theta -> accumulate -> smooth
+//   compose -> gradient (+ loop decisions in its last block) -> 12 Poisson sweeps
+//   (the first also saves/restores best_d, the last forms theta) -> accumulate -> smooth
 // The reference's host-side decisions (cost bookkeeping, cdm_improved, the
-// smoothing schedule, best_d restore, theta, the iteration cap) run in the control
-// and theta kernels against CdmCtl, so a level runs without any host round trip;
-// every later kernel of an iteration reads ctl->done and returns once a level has
-// left its loop.
+// smoothing schedule, best_d save/restore, theta, the iteration cap) run on the
+// device against CdmCtl, so a level runs without any host round trip; every
+// kernel of an iteration reads ctl->done and returns once a level has left its loop.
 #include <cfloat>
 #include "common.cuh"
 #include "stats.h"
@@ -67,6 +67,9 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_compose_kernel(const CdmSeg* 
         Js[i] = v;
     }
 }
+
+__device__ void control_block(const CdmSeg& S);
+__device__ __forceinline__ bool last_block_of_segment(const CdmSeg& S);
 
 // ------------------------------------------------------------------ gradient
 // Window sums of linear_regression over the clipped 5^3 window
@@ -239,6 +242,8 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_gradient_kernel(const CdmSeg*
     csum = block_sum(csum, red);
     if (threadIdx.x == 0)
         S.cost_part[blockIdx.x] = csum;
+    if (last_block_of_segment(S))
+        control_block(S);
 }
 
 // ------------------------------------------------------------------ control
@@ -294,16 +299,11 @@ __device__ float seg_cost_mean(const CdmSeg& S)
 }
 
 // The body of the reference's iteration loop between the gradient and the
-// Poisson solve (reg/cdm.hpp:418-460).  One block per segment.
-__global__ void cdm_control_kernel(const CdmSeg* __restrict__ segs)
+// Poisson solve (reg/cdm.hpp:418-460), run by one block of the segment (the
+// gradient kernel's last block).
+__device__ void control_block(const CdmSeg& S)
 {
-    const CdmSeg& S = segs[blockIdx.y];
     CdmCtl* c = S.ctl;
-    if (c->done) {
-        if (threadIdx.x == 0)
-            c->save_best = c->restore = 0;
-        return;
-    }
     const float mean_cost = seg_cost_mean(S);
     if (threadIdx.x != 0)
         return;
@@ -341,65 +341,127 @@ __global__ void cdm_control_kernel(const CdmSeg* __restrict__ segs)
     ++c->iters_run;
 }
 
-// best_d = cur_d when the cost improved (reg/cdm.hpp:447-452); otherwise, on a
-// stall, cur_d = best_d (reg/cdm.hpp:457).  Runs even on the iteration that
-// leaves the loop, as the reference saves best_d before its break.
-__global__ void __launch_bounds__(kCdmThreads) cdm_best_copy_kernel(const CdmSeg* __restrict__ segs)
+// Completion ticket of a segment's blocks: true in the one block that finishes
+// last (all other blocks' global writes are visible to it).
+__device__ __forceinline__ bool last_block_of_segment(const CdmSeg& S)
 {
-    SEG_BEGIN
-    const CdmCtl* c = S.ctl;
-    const float* src;
-    float* dst;
-    if (c->save_best) {
-        src = S.cur_d;
-        dst = S.best_d;
-    } else if (c->restore) {
-        src = S.best_d;
-        dst = S.cur_d;
-    } else
-        return;
-    for (long long i = first; i < 3 * n; i += stride)
-        dst[i] = src[i];
+    __shared__ unsigned int last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        last = (atomicAdd(&S.ctl->ticket, 1u) == (unsigned)S.nblk - 1u);
+        if (last)
+            S.ctl->ticket = 0u;
+    }
+    __syncthreads();
+    if (last)
+        __threadfence();
+    return last;
 }
 
 // ------------------------------------------------------------------ Poisson
 // cdm_solve_poisson (reg/cdm.hpp:158-253): s0 = new_d * (-1/6); then Jacobi sweeps
 // s' = (new_d - s[-1] - s[+1] - s[-w] - s[+w] - s[-wh] - s[+wh]) * (-1/6) with the
 // neighbours taken by flat index, bounds on the flat index only.
-__global__ void __launch_bounds__(kCdmThreads) cdm_poisson_init_kernel(const CdmSeg* __restrict__ segs)
+// mode 0: the first sweep, reading s0 = new_d * (-1/6) formed on the fly (the same
+//         float product the reference stores), writing B; it also applies this
+//         iteration's best_d save / restore (reg/cdm.hpp:447-457), which the
+//         reference performs before its Poisson solve -- even on the iteration
+//         that leaves the loop;
+// mode 1: a middle sweep, parity picks A->B or B->A;
+// mode 2: the last sweep (B->A) with the first-iteration max |result| (theta,
+//         reg/cdm.hpp:463-467) formed from the values it writes.
+__device__ __forceinline__ void poisson_point(const float* __restrict__ s, const float* __restrict__ rhs, long long p,
+                                              long long n, long long w, long long wh, bool scale_s, float* v)
 {
-    SEG_BEGIN
-    if (S.ctl->done)
-        return;
-    const float c = -0.5f / 3.0f;
-    for (long long i = first; i < 3 * n; i += stride)
-        S.aux_d[i] = S.new_d[i] * c;
+    const float c6 = -0.5f / 3.0f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float acc = rhs[3 * p + c];
+        if (scale_s) {
+            if (p >= 1) acc -= s[3 * (p - 1) + c] * c6;
+            if (p < n - 1) acc -= s[3 * (p + 1) + c] * c6;
+            if (p >= w) acc -= s[3 * (p - w) + c] * c6;
+            if (p < n - w) acc -= s[3 * (p + w) + c] * c6;
+            if (p >= wh) acc -= s[3 * (p - wh) + c] * c6;
+            if (p < n - wh) acc -= s[3 * (p + wh) + c] * c6;
+        } else {
+            if (p >= 1) acc -= s[3 * (p - 1) + c];
+            if (p < n - 1) acc -= s[3 * (p + 1) + c];
+            if (p >= w) acc -= s[3 * (p - w) + c];
+            if (p < n - w) acc -= s[3 * (p + w) + c];
+            if (p >= wh) acc -= s[3 * (p - wh) + c];
+            if (p < n - wh) acc -= s[3 * (p + wh) + c];
+        }
+        acc *= c6;
+        v[c] = acc;
+    }
 }
 
-__global__ void __launch_bounds__(kCdmThreads) cdm_poisson_sweep_kernel(const CdmSeg* __restrict__ segs, int parity)
+__global__ void __launch_bounds__(kCdmThreads) cdm_poisson_kernel(const CdmSeg* __restrict__ segs, int mode,
+                                                                  int parity)
 {
     SEG_BEGIN
-    if (S.ctl->done)
+    CdmCtl* c = S.ctl;
+    if (mode == 0) {
+        const float* src = nullptr;
+        float* dst = nullptr;
+        if (c->save_best) {
+            src = S.cur_d;
+            dst = S.best_d;
+        } else if (c->restore) {
+            src = S.best_d;
+            dst = S.cur_d;
+        }
+        if (dst)
+            for (long long i = first; i < 3 * n; i += stride)
+                dst[i] = src[i];
+    }
+    if (c->done)
         return;
-    const float* __restrict__ s = parity ? S.tmp_d : S.aux_d;
-    float* __restrict__ o = parity ? S.aux_d : S.tmp_d;
     const float* __restrict__ rhs = S.new_d;
+    const float* __restrict__ in;
+    float* __restrict__ out;
+    if (mode == 0) {
+        in = rhs;
+        out = S.tmp_d;
+    } else if (mode == 2) {
+        in = S.tmp_d;
+        out = S.aux_d;
+    } else {
+        in = parity ? S.tmp_d : S.aux_d;
+        out = parity ? S.aux_d : S.tmp_d;
+    }
     const long long w = D.w, wh = D.wh();
-    const float inv_d2 = -0.5f / 3.0f;
+    const bool want_theta = (mode == 2) && (c->theta == 0.0f);
+    float m = 0.0f;
     for (long long p = first; p < n; p += stride) {
-        float v[3] = {rhs[3 * p], rhs[3 * p + 1], rhs[3 * p + 2]};
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            if (p >= 1) v[c] -= s[3 * (p - 1) + c];
-            if (p < n - 1) v[c] -= s[3 * (p + 1) + c];
-            if (p >= w) v[c] -= s[3 * (p - w) + c];
-            if (p < n - w) v[c] -= s[3 * (p + w) + c];
-            if (p >= wh) v[c] -= s[3 * (p - wh) + c];
-            if (p < n - wh) v[c] -= s[3 * (p + wh) + c];
-            v[c] *= inv_d2;
-            o[3 * p + c] = v[c];
+        float v[3];
+        poisson_point(in, rhs, p, n, w, wh, mode == 0, v);
+        out[3 * p] = v[0];
+        out[3 * p + 1] = v[1];
+        out[3 * p + 2] = v[2];
+        if (want_theta) {
+            // cdm_max_displacement_length: sqrt(double(x*x + y*y + z*z)) as float
+            const float l2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+            m = fmaxf(m, (float)sqrt((double)l2));
         }
     }
+    if (!want_theta)
+        return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0)
+        atomicMax(&c->theta_bits, __float_as_uint(m));
+    if (!last_block_of_segment(S) || threadIdx.x != 0)
+        return;
+    const float theta = __uint_as_float(atomicAdd(&c->theta_bits, 0u));
+    c->theta = theta;
+    if (theta == 0.0f)
+        c->done = 1;
+    else
+        c->scale = c->speed / theta;
 }
 
 // ------------------------------------------------------------------ theta
@@ -425,17 +487,9 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_theta_kernel(const CdmSeg* __
         m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0)
         atomicMax(&c->theta_bits, __float_as_uint(m));
-    __threadfence();
-    __syncthreads();
-    __shared__ unsigned int last;
-    if (threadIdx.x == 0)
-        last = (atomicAdd(&c->ticket, 1u) == (unsigned)S.nblk - 1u);
-    __syncthreads();
-    if (!last || threadIdx.x != 0)
+    if (!last_block_of_segment(S) || threadIdx.x != 0)
         return;
-    __threadfence();
     const float theta = __uint_as_float(atomicAdd(&c->theta_bits, 0u));
-    c->ticket = 0u;
     c->theta = theta;
     if (theta == 0.0f)
         c->done = 1;
@@ -698,27 +752,14 @@ cudaError_t launch_cdm_gradient(const CdmSeg* segs, int nseg, int blocks, int pi
     return cudaGetLastError();
 }
 
-cudaError_t launch_cdm_control(const CdmSeg* segs, int nseg, int, cudaStream_t st)
-{
-    cdm_control_kernel<<<dim3(1, nseg), 256, 0, st>>>(segs);
-    count_launch();
-    return cudaGetLastError();
-}
-
-cudaError_t launch_cdm_best_copy(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st)
-{
-    cdm_best_copy_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
-    count_launch();
-    return cudaGetLastError();
-}
-
 cudaError_t launch_cdm_poisson(const CdmSeg* segs, int nseg, int blocks, int sweeps, cudaStream_t st)
 {
-    cdm_poisson_init_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
-    for (int k = 0; k < sweeps; ++k)
-        cdm_poisson_sweep_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs, k & 1);
+    // sweeps is 12 (reg/cdm.hpp:165): first (B), 10 middle (B->A, A->B, ...), last (B->A)
+    cdm_poisson_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs, 0, 0);
+    for (int k = 1; k < sweeps - 1; ++k)
+        cdm_poisson_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs, 1, k & 1);
+    cdm_poisson_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs, 2, 1);
     count_launch(sweeps);
-    count_launch();
     return cudaGetLastError();
 }
 

@@ -1,8 +1,22 @@
 // Device state of one CDM level of one job (fields, scratch, control block).
 #pragma once
+#include <functional>
 #include "host.h"
 
 namespace regb {
+
+// An instantiated CUDA graph of work captured from a stream.
+struct GraphExec {
+    cudaGraphExec_t exec = nullptr;
+    long long nodes = 0;  // kernels per replay
+    GraphExec() = default;
+    GraphExec(const GraphExec&) = delete;
+    GraphExec& operator=(const GraphExec&) = delete;
+    ~GraphExec() { reset(); }
+    void capture(const std::function<void(cudaStream_t)>& body);
+    void launch(cudaStream_t st);
+    void reset();
+};
 
 struct CdmLevel {
     int pix = 0;

@@ -91,10 +91,10 @@ cudaError_t launch_fixed_stats(const uint8_t* f, long long n, int32_t* hist, uns
 // CDM passes.  pix: 0 = uint8, 1 = float.  segs is a device array of nseg segments;
 // blocks is gridDim.x per segment.
 cudaError_t launch_cdm_compose(const CdmSeg* segs, int nseg, int blocks, int pix, cudaStream_t st);
+// The gradient's last block of each segment also runs the loop decisions.
 cudaError_t launch_cdm_gradient(const CdmSeg* segs, int nseg, int blocks, int pix, int gradient_type,
                                 cudaStream_t st);
-cudaError_t launch_cdm_control(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st);
-cudaError_t launch_cdm_best_copy(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st);
+// 12 sweeps; the first also applies best_d save/restore, the last forms theta.
 cudaError_t launch_cdm_poisson(const CdmSeg* segs, int nseg, int blocks, int sweeps, cudaStream_t st);
 cudaError_t launch_cdm_theta(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st);
 cudaError_t launch_cdm_accumulate(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st);
