@@ -9,6 +9,7 @@
 // smoothing schedule, best_d save/restore, theta, the iteration cap) run on the
 // device against CdmCtl, so a level runs without any host round trip; every
 // kernel of an iteration reads ctl->done and returns once a level has left its loop.
+#include <atomic>
 #include <cfloat>
 #include "common.cuh"
 #include "stats.h"
@@ -246,6 +247,139 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_gradient_kernel(const CdmSeg*
         control_block(S);
 }
 
+// Tiled uint8 'r' gradient.  For integer pixels the regression's window sums
+// (sum Js, sum It, sum Js^2, sum It^2, sum Js*It over the clipped 5^3 window) are
+// exact integers, so they are formed here as separable 5-tap box sums over a
+// shared-memory tile (zero outside the volume, the window size m from the clipped
+// extents) -- the same integers the reference sums voxel by voxel, hence
+// bit-identical results at a fraction of the loads.
+constexpr int kTX = 32, kTY = 4, kTZ = 4, kBoxThreads = 128;
+constexpr int kHX = kTX + 4, kHY = kTY + 4, kHZ = kTZ + 4;
+struct BoxSmem {
+    uint8_t J[kHZ][kHY][kHX];
+    uint8_t I[kHZ][kHY][kHX];
+    int p1[5][kHZ][kHY][kTX];  // x-summed
+    int p2[5][kHZ][kTY][kTX];  // x,y-summed
+};
+
+__global__ void __launch_bounds__(kBoxThreads) cdm_gradient_box_u8_kernel(const CdmSeg* __restrict__ segs)
+{
+    const CdmSeg& S = segs[blockIdx.y];
+    if ((int)blockIdx.x >= S.nblk)
+        return;
+    if (S.ctl->done)
+        return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    BoxSmem& sm = *reinterpret_cast<BoxSmem*>(smraw);
+    const Dim3 D{S.w, S.h, S.d};
+    const uint8_t* __restrict__ Js = (const uint8_t*)S.Js;
+    const uint8_t* __restrict__ It = (const uint8_t*)S.It;
+    float* __restrict__ nd = S.new_d;
+    const int ntx = (D.w + kTX - 1) / kTX, nty = (D.h + kTY - 1) / kTY, ntz = (D.d + kTZ - 1) / kTZ;
+    const int ntiles = ntx * nty * ntz;
+    const long long wl = D.w, whl = D.wh();
+    double csum = 0.0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += S.nblk) {
+        const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
+        const int x0 = tx * kTX, y0 = ty * kTY, z0 = tz * kTZ;
+        __syncthreads();  // the previous tile's readers are done with the buffers
+        for (int k = threadIdx.x; k < kHZ * kHY * kHX; k += blockDim.x) {
+            const int hx = k % kHX, hy = (k / kHX) % kHY, hz = k / (kHX * kHY);
+            const int gx = x0 + hx - 2, gy = y0 + hy - 2, gz = z0 + hz - 2;
+            uint8_t a = 0, b = 0;
+            if (gx >= 0 && gy >= 0 && gz >= 0 && gx < D.w && gy < D.h && gz < D.d) {
+                const long long gi = (gz * whl) + gy * wl + gx;
+                a = Js[gi];
+                b = It[gi];
+            }
+            sm.J[hz][hy][hx] = a;
+            sm.I[hz][hy][hx] = b;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < kHZ * kHY * kTX; k += blockDim.x) {
+            const int xo = k % kTX, hy = (k / kTX) % kHY, hz = k / (kTX * kHY);
+            int s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+#pragma unroll
+            for (int dx = 0; dx < 5; ++dx) {
+                const int a = sm.J[hz][hy][xo + dx], b = sm.I[hz][hy][xo + dx];
+                s0 += a;
+                s1 += b;
+                s2 += a * a;
+                s3 += b * b;
+                s4 += a * b;
+            }
+            sm.p1[0][hz][hy][xo] = s0;
+            sm.p1[1][hz][hy][xo] = s1;
+            sm.p1[2][hz][hy][xo] = s2;
+            sm.p1[3][hz][hy][xo] = s3;
+            sm.p1[4][hz][hy][xo] = s4;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < kHZ * kTY * kTX; k += blockDim.x) {
+            const int xo = k % kTX, yo = (k / kTX) % kTY, hz = k / (kTX * kTY);
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                int v = 0;
+#pragma unroll
+                for (int dy = 0; dy < 5; ++dy)
+                    v += sm.p1[c][hz][yo + dy][xo];
+                sm.p2[c][hz][yo][xo] = v;
+            }
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < kTZ * kTY * kTX; k += blockDim.x) {
+            const int xo = k % kTX, yo = (k / kTX) % kTY, zo = k / (kTX * kTY);
+            const int x = x0 + xo, y = y0 + yo, z = z0 + zo;
+            if (x >= D.w || y >= D.h || z >= D.d)
+                continue;
+            const long long i = (z * whl) + y * wl + x;
+            const int js = sm.J[zo + 2][yo + 2][xo + 2], it = sm.I[zo + 2][yo + 2][xo + 2];
+            float3 out = make_float3(0.0f, 0.0f, 0.0f);
+            float cost = 0.0f;
+            if (!(js == 0 || it == 0)) {
+                int t[5];
+#pragma unroll
+                for (int c = 0; c < 5; ++c) {
+                    int v = 0;
+#pragma unroll
+                    for (int dz = 0; dz < 5; ++dz)
+                        v += sm.p2[c][zo + dz][yo][xo];
+                    t[c] = v;
+                }
+                const int m = (min(D.w - 1, x + 2) - max(0, x - 2) + 1) * (min(D.h - 1, y + 2) - max(0, y - 2) + 1) *
+                              (min(D.d - 1, z + 2) - max(0, z - 2) + 1);
+                Reg r;
+                regress_finish((double)t[0], (double)t[1], (double)t[2], (double)t[3], (double)t[4], m, r);
+                if (r.a > 0.0f) {
+                    // gradient_at from the tile (neighbours are inside the halo)
+                    float3 g;
+                    g.x = (x + 1 < D.w && x) ? (float)((int)sm.J[zo + 2][yo + 2][xo + 3] - (int)sm.J[zo + 2][yo + 2][xo + 1]) : 0.0f;
+                    g.y = (y + 1 < D.h && y) ? (float)((int)sm.J[zo + 2][yo + 3][xo + 2] - (int)sm.J[zo + 2][yo + 1][xo + 2]) : 0.0f;
+                    g.z = (z + 1 < D.d && z) ? (float)((int)sm.J[zo + 3][yo + 2][xo + 2] - (int)sm.J[zo + 1][yo + 2][xo + 2]) : 0.0f;
+                    const float sc = r.r2 * ((float)js * r.a + r.b - (float)it);
+                    g.x *= sc;
+                    g.y *= sc;
+                    g.z *= sc;
+                    out.x = 0.0f + g.x;
+                    out.y = 0.0f + g.y;
+                    out.z = 0.0f + g.z;
+                    cost = -r.r2;
+                }
+            }
+            nd[3 * i] = out.x;
+            nd[3 * i + 1] = out.y;
+            nd[3 * i + 2] = out.z;
+            csum += (double)cost;
+        }
+    }
+    __shared__ double red[32];
+    csum = block_sum(csum, red);
+    if (threadIdx.x == 0)
+        S.cost_part[blockIdx.x] = csum;
+    if (last_block_of_segment(S))
+        control_block(S);
+}
+
 // ------------------------------------------------------------------ control
 // cdm_improved (reg/cdm.hpp:19-34): regression of the last costs on their index
 // (int x, float y; statistics.hpp:694-713); a positive slope means "not improved".
@@ -433,7 +567,37 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_poisson_kernel(const CdmSeg* 
         out = parity ? S.aux_d : S.tmp_d;
     }
     const long long w = D.w, wh = D.wh();
-    const bool want_theta = (mode == 2) && (c->theta == 0.0f);
+    if (mode != 2) {
+        // one float of the interleaved xyz array per thread: the component's
+        // neighbours at voxel offsets 1, w, wh are float offsets 3, 3w, 3wh, and
+        // the reference's flat-index bounds p >= k / p < n - k are f >= 3k / f < 3(n - k)
+        // -- every tap is a coalesced load, the arithmetic per component unchanged
+        const float c6 = -0.5f / 3.0f;
+        const long long N3 = 3 * n, w3 = 3 * w, wh3 = 3 * wh;
+        const bool sc = (mode == 0);
+        for (long long f = first; f < N3; f += stride) {
+            float acc = rhs[f];
+            if (sc) {
+                if (f >= 3) acc -= in[f - 3] * c6;
+                if (f < N3 - 3) acc -= in[f + 3] * c6;
+                if (f >= w3) acc -= in[f - w3] * c6;
+                if (f < N3 - w3) acc -= in[f + w3] * c6;
+                if (f >= wh3) acc -= in[f - wh3] * c6;
+                if (f < N3 - wh3) acc -= in[f + wh3] * c6;
+            } else {
+                if (f >= 3) acc -= in[f - 3];
+                if (f < N3 - 3) acc -= in[f + 3];
+                if (f >= w3) acc -= in[f - w3];
+                if (f < N3 - w3) acc -= in[f + w3];
+                if (f >= wh3) acc -= in[f - wh3];
+                if (f < N3 - wh3) acc -= in[f + wh3];
+            }
+            acc *= c6;
+            out[f] = acc;
+        }
+        return;
+    }
+    const bool want_theta = (c->theta == 0.0f);
     float m = 0.0f;
     for (long long p = first; p < n; p += stride) {
         float v[3];
@@ -577,20 +741,18 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_smooth_kernel(const CdmSeg* _
     const float w_1 = 1.0f - sm;
     const float* __restrict__ d = S.tmp_d;
     float* __restrict__ dd = S.cur_d;
-    const long long w = D.w, wh = D.wh();
-    for (long long p = first; p < n; p += stride) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            float v = 0.0f;
-            if (p + 1 < n) v += d[3 * (p + 1) + k];
-            if (p >= 1) v += d[3 * (p - 1) + k];
-            if (p + w < n) v += d[3 * (p + w) + k];
-            if (p >= w) v += d[3 * (p - w) + k];
-            if (p + wh < n) v += d[3 * (p + wh) + k];
-            if (p >= wh) v += d[3 * (p - wh) + k];
-            v *= w_6;
-            dd[3 * p + k] = d[3 * p + k] * w_1 + v;
-        }
+    // one float of the interleaved array per thread (see the Poisson sweep)
+    const long long N3 = 3 * n, w3 = 3 * (long long)D.w, wh3 = 3 * (long long)D.wh();
+    for (long long f = first; f < N3; f += stride) {
+        float v = 0.0f;
+        if (f + 3 < N3) v += d[f + 3];
+        if (f >= 3) v += d[f - 3];
+        if (f + w3 < N3) v += d[f + w3];
+        if (f >= w3) v += d[f - w3];
+        if (f + wh3 < N3) v += d[f + wh3];
+        if (f >= wh3) v += d[f - wh3];
+        v *= w_6;
+        dd[f] = d[f] * w_1 + v;
     }
 }
 
@@ -744,7 +906,22 @@ cudaError_t launch_cdm_compose(const CdmSeg* segs, int nseg, int blocks, int pix
 cudaError_t launch_cdm_gradient(const CdmSeg* segs, int nseg, int blocks, int pix, int gradient_type,
                                 cudaStream_t st)
 {
-    if (pix == 0)
+    if (pix == 0 && gradient_type == 'r') {
+        static std::atomic<unsigned long long> attr_set{0};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess)
+            return e;
+        const unsigned long long bit = 1ull << (dev & 63);
+        if (!(attr_set.load() & bit)) {
+            e = cudaFuncSetAttribute(cdm_gradient_box_u8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(BoxSmem));
+            if (e != cudaSuccess)
+                return e;
+            attr_set.fetch_or(bit);
+        }
+        cdm_gradient_box_u8_kernel<<<SEG_GRID, kBoxThreads, sizeof(BoxSmem), st>>>(segs);
+    } else if (pix == 0)
         cdm_gradient_kernel<uint8_t><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, gradient_type);
     else
         cdm_gradient_kernel<float><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, gradient_type);
