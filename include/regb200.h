@@ -116,6 +116,24 @@ regb_status regb_affine_to_matrix_f64(const double param[12], const int from_dim
                                       const int to_dim[3], const double to_vs[3], double T[12]);
 /* transformation_matrix::inverse (numerical/transformation.hpp:820-832); REGB_FALSE if singular. */
 regb_status regb_matrix_inverse(float T[12]);
+/* transformation_matrix::to_affine_param(from, from_vs, to, to_vs)
+ * (numerical/transformation.hpp:703-741): the 12 parameters (translocation, rotation,
+ * scaling, affine) of a from-voxel -> to-voxel matrix. */
+regb_status regb_matrix_to_affine_param(const float T[12], const int from_dim[3], const float from_vs[3],
+                                        const int to_dim[3], const float to_vs[3], float param[12]);
+
+/* ---- mask-moment initialisation of linear() (reg/linear.hpp:658-684) --------------- */
+/* has_mask(img) (numerical/basic_op.hpp:811-830) of a uint8 volume: *out = 1 when more
+ * than a fifth of its voxels are 0 or its non-zero voxels' bounding box lies inside the
+ * volume on some axis. */
+regb_status regb_has_mask(const regb_volume* img, int* out);
+/* estimate_affine_param(source, source_vs, target, target_vs, arg)
+ * (numerical/transformation.hpp:933-1021) on uint8 volumes: parameters that map the
+ * centroid and principal axes of source's voxels > 0 onto target's.  REGB_FALSE (param =
+ * identity) when either volume has no voxel > 0.  The moments are formed from exact
+ * per-line voxel counts made on the device; regb_linear runs this step itself. */
+regb_status regb_estimate_affine_param(const regb_volume* source, const float source_vs[3],
+                                       const regb_volume* target, const float target_vs[3], float param[12]);
 
 /* ---- resample ------------------------------------------------------------------- */
 /* tipl::resample<linear>(from, to, trans) (numerical/resampling.hpp:1239-1298):

@@ -52,14 +52,45 @@ def _u8(a):
 
 
 class _Lib:
+    _pfx = ""
+
     def __init__(self, path: str):
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         self.lib = C.CDLL(path)
 
+    def _fn(self, name):
+        return getattr(self.lib, self._pfx + name)
+
+    # -- mask-moment initialisation of linear() (reg/linear.hpp:658-684)
+    def has_mask(self, img) -> bool:
+        return bool(self._fn("has_mask" if self._pfx == "tiplref_" else "has_mask_u8")(_ptr(_u8(img)),
+                                                                                        _ptr(_dims(img.shape))))
+
+    def estimate_affine_param(self, src, src_vs, tgt, tgt_vs) -> np.ndarray:
+        a = np.zeros(12, np.float32)
+        self._fn("estimate_affine_param" + ("" if self._pfx == "tiplref_" else "_u8"))(
+            _ptr(_u8(src)), _ptr(_dims(src.shape)), _ptr(_f32(src_vs)), _ptr(_u8(tgt)), _ptr(_dims(tgt.shape)),
+            _ptr(_f32(tgt_vs)), _ptr(a))
+        return a
+
+    def matrix_to_affine_param(self, T, from_shape, from_vs, to_shape, to_vs) -> np.ndarray:
+        a = np.zeros(12, np.float32)
+        self._fn("matrix_to_affine_param")(_ptr(_f32(T)), _ptr(_dims(from_shape)), _ptr(_f32(from_vs)),
+                                           _ptr(_dims(to_shape)), _ptr(_f32(to_vs)), _ptr(a))
+        return a
+
+    def eigen_sym3(self, A):
+        A = np.ascontiguousarray(A, np.float64).reshape(9)
+        V, d = np.zeros(9), np.zeros(3)
+        self._fn("eigen_sym3")(_ptr(A), _ptr(V), _ptr(d))
+        return V, d
+
 
 class Oracle(_Lib):
     """Plain-C restatement.  Volumes are numpy arrays shaped (z, y, x); fields (z, y, x, 3)."""
+
+    _pfx = "orc_"
 
     def __init__(self, path: str = ORACLE_SO):
         super().__init__(path)
@@ -215,12 +246,15 @@ class Oracle(_Lib):
 class Reference(_Lib):
     """The reference's own CPU implementation (compiled from its headers)."""
 
+    _pfx = "tiplref_"
+
     def __init__(self, path: str = REF_SO):
         super().__init__(path)
         L = self.lib
         for n in ("tiplref_mi_cost", "tiplref_corr_cost"):
             getattr(L, n).restype = C.c_double
-        for n in ("tiplref_cdm_gradient_u8", "tiplref_cdm_gradient_f32", "tiplref_cdm_max_len", "tiplref_linear"):
+        for n in ("tiplref_cdm_gradient_u8", "tiplref_cdm_gradient_f32", "tiplref_cdm_max_len", "tiplref_linear",
+                  "tiplref_linear_bound"):
             getattr(L, n).restype = C.c_float
         L.tiplref_cdm_smooth.argtypes = [_P, _P, _P, C.c_float]
         for n in ("tiplref_cdm_u8", "tiplref_cdm_f32"):
@@ -330,6 +364,14 @@ class Reference(_Lib):
         c = self.lib.tiplref_linear(_ptr(_u8(fixed)), _ptr(_dims(fixed.shape)), _ptr(_f32(fixed_vs)),
                                     _ptr(_u8(moving)), _ptr(_dims(moving.shape)), _ptr(_f32(moving_vs)), _ptr(a),
                                     int(reg_type), int(cost_type))
+        return float(c), a
+
+    def linear_bound(self, fixed, fixed_vs, moving, moving_vs, arg=None, reg_type=15, cost_type=1, bound=0):
+        """tipl::reg::linear with bound table 0 reg, 1 narrow (single-threaded L-BFGS from arg), 2 large."""
+        a = np.array([0, 0, 0, 0, 0, 0, 1, 1, 1, 0, 0, 0], np.float32) if arg is None else _f32(arg).copy()
+        c = self.lib.tiplref_linear_bound(_ptr(_u8(fixed)), _ptr(_dims(fixed.shape)), _ptr(_f32(fixed_vs)),
+                                          _ptr(_u8(moving)), _ptr(_dims(moving.shape)), _ptr(_f32(moving_vs)),
+                                          _ptr(a), int(reg_type), int(cost_type), int(bound))
         return float(c), a
 
     def normalize_to_u8(self, img, upper=255.999):

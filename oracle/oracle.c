@@ -245,6 +245,9 @@ int orc_is_integer_shift(const float* T, int* shift)
 #undef PIX
 #undef R
 
+/* ---- mask-moment initialisation of linear() ------------------------------- */
+#include "oracle_mask.h"
+
 /* ---- affine costs ---------------------------------------------------------- */
 
 /* histogram(img, hist, 0, 255, 256) (numerical/basic_op.hpp:1293-1311): bin =

@@ -63,6 +63,13 @@ int orc_cdm_level_f32(const float* It, const float* Is, const int* dim, float* b
 int orc_cdm_level_f64(const double* It, const double* Is, const int* dim, double* best_d, float resolution,
                       float speed, float smoothing, unsigned int min_dimension, int gradient_type, int* iters_out);
 
+int orc_has_mask_u8(const uint8_t* img, const int* dim);
+void orc_eigen_sym3(const double* A, double* V, double* d);
+void orc_estimate_affine_param_u8(const uint8_t* src, const int* sdim, const float* svs, const uint8_t* tgt,
+                                  const int* tdim, const float* tvs, float* arg);
+void orc_matrix_to_affine_param(const float* T, const int* from_dim, const float* from_vs, const int* to_dim,
+                                const float* to_vs, float* arg);
+
 #ifdef __cplusplus
 }
 #endif

@@ -245,6 +245,54 @@ float tiplref_linear(const u8* from, const int* from_dim, const float* from_vs, 
     return c;
 }
 
+// has_mask(img) (numerical/basic_op.hpp:811-830)
+int tiplref_has_mask(const u8* img, const int* dim) { return tipl::has_mask(cview(img, dim)) ? 1 : 0; }
+
+// estimate_affine_param(source, source_vs, target, target_vs, arg) (numerical/transformation.hpp:933-1021)
+void tiplref_estimate_affine_param(const u8* src, const int* sdim, const float* svs, const u8* tgt, const int* tdim,
+                                   const float* tvs, float* arg)
+{
+    tipl::affine_param<float, 3> a;
+    tipl::estimate_affine_param(cview(src, sdim), tipl::vector<3>(svs), cview(tgt, tdim), tipl::vector<3>(tvs), a);
+    std::copy(a.begin(), a.end(), arg);
+}
+
+// transformation_matrix::to_affine_param(from, from_vs, to, to_vs) (numerical/transformation.hpp:703-741)
+void tiplref_matrix_to_affine_param(const float* T, const int* from_dim, const float* from_vs, const int* to_dim,
+                                    const float* to_vs, float* arg)
+{
+    auto a = to_matrix(T).to_affine_param(shp(from_dim), tipl::vector<3>(from_vs), shp(to_dim),
+                                          tipl::vector<3>(to_vs));
+    std::copy(a.begin(), a.end(), arg);
+}
+
+// eigen_decomposition_sym, 3x3 double (numerical/matrix.hpp:1830-1955)
+void tiplref_eigen_sym3(const double* A, double* V, double* d)
+{
+    tipl::mat::eigen_decomposition_sym(A, V, d, tipl::dim<3, 3>());
+}
+
+// linear<void> with an explicit bound table: 0 reg_bound, 1 narrow_bound, 2 large_bound
+// (reg/linear.hpp:258-266); the narrow bound takes the single-threaded L-BFGS path.
+float tiplref_linear_bound(const u8* from, const int* from_dim, const float* from_vs, const u8* to,
+                           const int* to_dim, const float* to_vs, float* arg_inout, int reg_type, int cost_type,
+                           int bound)
+{
+    tipl::affine_param<float, 3> arg(arg_inout);
+    tipl::reg::linear_reg_param p;
+    p.reg_type = tipl::reg::reg_type(reg_type);
+    p.cost_type = tipl::reg::cost_type(cost_type);
+    p.bound = bound == 1 ? tipl::reg::narrow_bound : (bound == 2 ? tipl::reg::large_bound : tipl::reg::reg_bound);
+    p.cuda = false;
+    bool terminated = false;
+    float c = tipl::reg::linear<void>(std::vector<tipl::const_pointer_image<3, u8>>{cview(from, from_dim)},
+                                      tipl::vector<3>(from_vs),
+                                      std::vector<tipl::const_pointer_image<3, u8>>{cview(to, to_dim)},
+                                      tipl::vector<3>(to_vs), arg, p, terminated);
+    std::copy(arg.begin(), arg.end(), arg_inout);
+    return c;
+}
+
 // normalize_upper_lower2(in, out, upper) (numerical/numerical.hpp:909-927): float -> uint8
 void tiplref_normalize_to_u8(const float* in, const int* dim, u8* out, float upper)
 {

@@ -31,10 +31,86 @@ def save(name, **arrays):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=os.environ.get("TIPL_REF_ROOT", oracle.DEFAULT_REF_ROOT))
+    ap.add_argument("--only", default=None, help="make one fixture group: core | mask_init")
     args = ap.parse_args()
     oracle.build(args.ref_root, with_ref=True)
     R = oracle.Reference()
     R.set_threads(1)
+    if args.only in (None, "core"):
+        core(R)
+    if args.only in (None, "mask_init"):
+        mask_init(R)
+
+
+def mask_init(R):
+    """has_mask, estimate_affine_param, to_affine_param and linear() with the mask start."""
+    rng = np.random.default_rng(ph.seed_for(0, 9))
+    vols = []
+    for shp in [(30, 34, 28), (27, 31, 35)]:
+        vols.append(ph.normalize_to_u8(ph.class_phantom(shp, rng)))              # zero background
+    vols.append((rng.random((20, 22, 18)) * 200 + 20).astype(np.uint8))          # no zero voxel
+    b = np.full((20, 22, 18), 7, np.uint8)
+    b[:, :, 0] = 0
+    b[:, :, -1] = 0
+    vols.append(b)                                                                # box inside along x only
+    vols.append(np.zeros((9, 10, 11), np.uint8))                                  # empty
+    c = np.zeros((16, 18, 14), np.uint8)
+    c[3:11, 5:9, 2:12] = 90
+    vols.append(c)                                                                # axis-aligned box
+    has = np.array([R.has_mask(v) for v in vols], np.int32)
+    flat = np.concatenate([v.ravel() for v in vols])
+    shapes = np.array([v.shape for v in vols], np.int32)
+    pairs, vss, est = [], [], []
+    for (i, j) in [(0, 1), (1, 0), (0, 0), (5, 0), (0, 5), (4, 0), (3, 1)]:
+        for vs_pair in [((1, 1, 1), (1, 1, 1)), (tuple(rng.uniform(0.8, 2.0, 3)), tuple(rng.uniform(0.8, 2.0, 3)))]:
+            svs, tvs = (np.array(v, np.float32) for v in vs_pair)
+            pairs.append((i, j))
+            vss.append(np.concatenate([svs, tvs]))
+            est.append(R.estimate_affine_param(vols[i], svs, vols[j], tvs))
+    Ts, tshapes, tvss, to_param = [], [], [], []
+    for k in range(24):
+        fs = tuple(int(v) for v in rng.integers(5, 60, 3))
+        ts = tuple(int(v) for v in rng.integers(5, 60, 3))
+        fvs = rng.uniform(0.7, 2.2, 3).astype(np.float32)
+        tvs = rng.uniform(0.7, 2.2, 3).astype(np.float32)
+        if k % 4 == 0:
+            fvs[:] = 1.0
+            tvs[:] = 1.0
+        p = ph.random_affine(rng, rot_deg=25, trans_vox=8, vs=fvs)
+        p[9:] = rng.uniform(-0.08, 0.08, 3)
+        T = R.affine_to_matrix(p, fs, fvs, ts, tvs)
+        Ts.append(T)
+        tshapes.append(np.array(fs + ts, np.int32))
+        tvss.append(np.concatenate([fvs, tvs]))
+        to_param.append(R.matrix_to_affine_param(T, fs, fvs, ts, tvs))
+    # linear() on a masked pair: the moving volume keeps a zero background
+    t = ph.class_phantom((44, 52, 48), rng)
+    T = R.affine_to_matrix(ph.random_affine(rng, rot_deg=8, trans_vox=3), t.shape, (1, 1, 1), t.shape, (1, 1, 1))
+    f8 = ph.normalize_to_u8(t)
+    m8 = R.resample(f8, t.shape, T)
+    # the reference's line search and L-BFGS race in two threads: record several runs
+    lin_costs = []
+    for th in (1, 4, 8, 16):
+        R.set_threads(th)
+        c, a = R.linear(f8, (1, 1, 1), m8, (1, 1, 1))
+        lin_costs.append(c)
+        if th == 8:
+            lin_cost, lin_arg = c, a
+    # narrow bound: one thread, L-BFGS from the given start, reproducible
+    starts = np.array([[0, 0, 0, 0, 0, 0, 1, 1, 1, 0, 0, 0],
+                       [1, 0.5, -0.5, 0.05, 0.02, -0.03, 1.02, 0.97, 1.0, 0.01, 0, -0.01]], np.float32)
+    narrow = [R.linear_bound(f8, (1, 1, 1), m8, (1, 1, 1), arg=st, bound=1, cost_type=ct)
+              for st in starts for ct in (1, 2)]
+    R.set_threads(1)
+    save("mask_init", vols=flat, shapes=shapes, has=has, pairs=np.array(pairs, np.int32),
+         vs=np.array(vss, np.float32), est=np.array(est, np.float32), T=np.array(Ts, np.float32),
+         tshapes=np.array(tshapes), tvs=np.array(tvss, np.float32), to_param=np.array(to_param, np.float32),
+         lin_fixed=f8, lin_moving=m8, lin_cost=np.float32(lin_cost), lin_arg=lin_arg,
+         lin_costs=np.array(lin_costs, np.float32), narrow_start=starts,
+         narrow_cost=np.array([n[0] for n in narrow], np.float32), narrow_arg=np.array([n[1] for n in narrow]))
+
+
+def core(R):
     rng = np.random.default_rng(ph.seed_for(0, 1))
 
     # transformation_matrix(affine_param, ...) and its inverse

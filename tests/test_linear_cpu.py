@@ -1,0 +1,60 @@
+"""The library's affine search driven on the CPU (tests/cpp/linear_cpu: the
+LinearRunner of tipl_b200/csrc/linear_runner.h with the oracle's costs in place of
+the device evaluator) against the reference's own tipl::reg::linear.
+
+* narrow bound: the reference takes its single-threaded path (L-BFGS from the given
+  start, reg/linear.hpp:645-651) -- final cost and parameters must be bit-identical;
+* reg bound with the mask start: the reference races its line search against L-BFGS
+  in two threads, so its result varies from run to run; ours (the same two searches
+  on a virtual clock) must be no worse than the worst of the recorded reference runs
+  by more than 1 %, and must be reproducible."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "tests", "cpp", "linear_cpu")
+
+
+@pytest.fixture(scope="module")
+def harness(orc):
+    if not os.path.exists(os.path.join(ROOT, "tipl_b200", "libregb200.so")):
+        pytest.skip("libregb200.so not built")
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "tests", "cpp"), "linear_cpu"])
+    return EXE
+
+
+def run(exe, tmp_path, f8, m8, cost, bound, start=None):
+    fp, mp, op = tmp_path / "f.u8", tmp_path / "m.u8", tmp_path / "o.bin"
+    f8.tofile(fp)
+    m8.tofile(mp)
+    z, y, x = f8.shape
+    z2, y2, x2 = m8.shape
+    cmd = [exe, str(x), str(y), str(z), str(fp), str(x2), str(y2), str(z2), str(mp), str(cost), str(bound), str(op)]
+    if start is not None:
+        cmd += [repr(float(v)) for v in start]
+    subprocess.run(cmd, check=True, capture_output=True, timeout=600)
+    o = np.fromfile(op, np.uint8)
+    return o[:4].view(np.float32)[0], o[4:52].view(np.float32).copy()
+
+
+def test_narrow_bound_bit_exact(harness, golden, tmp_path):
+    g = golden("mask_init")
+    k = 0
+    for st in g["narrow_start"]:
+        for cost in (1, 2):
+            c, a = run(harness, tmp_path, g["lin_fixed"], g["lin_moving"], cost, 1, st)
+            assert c.view(np.uint32) == g["narrow_cost"][k].view(np.uint32), (cost, c, g["narrow_cost"][k])
+            assert np.array_equal(a.view(np.uint32), g["narrow_arg"][k].view(np.uint32))
+            k += 1
+
+
+def test_reg_bound_mask_start_within_reference_runs(harness, golden, tmp_path):
+    g = golden("mask_init")
+    c1, a1 = run(harness, tmp_path, g["lin_fixed"], g["lin_moving"], 1, 0)
+    c2, a2 = run(harness, tmp_path, g["lin_fixed"], g["lin_moving"], 1, 0)
+    assert c1 == c2 and np.array_equal(a1, a2), "not reproducible"
+    worst = float(np.max(g["lin_costs"]))
+    assert c1 <= worst * 1.01, (c1, g["lin_costs"])

@@ -126,6 +126,33 @@ def matrix_inverse(T) -> np.ndarray:
     return M
 
 
+def matrix_to_affine_param(T, from_shape, from_vs, to_shape, to_vs) -> np.ndarray:
+    """transformation_matrix::to_affine_param: the 12 parameters of a from -> to matrix."""
+    M = np.ascontiguousarray(T, np.float32)
+    a = np.zeros(12, np.float32)
+    fd = np.array(list(_dims(from_shape)), np.int32)
+    td = np.array(list(_dims(to_shape)), np.int32)
+    _lib.check(_lib.lib().regb_matrix_to_affine_param(_fptr(M), _fptr(fd), _fptr(np.asarray(from_vs, np.float32)),
+                                                      _fptr(td), _fptr(np.asarray(to_vs, np.float32)), _fptr(a)))
+    return a
+
+
+def has_mask(img) -> bool:
+    """tipl::has_mask of a uint8 volume (numpy or device tensor)."""
+    out = C.c_int(0)
+    _lib.check(_lib.lib().regb_has_mask(C.byref(_vol(img)), C.byref(out)))
+    return bool(out.value)
+
+
+def estimate_affine_param(source, source_vs, target, target_vs) -> np.ndarray:
+    """tipl::estimate_affine_param: initial parameters from the masks' centroids and axes."""
+    a = np.zeros(12, np.float32)
+    _lib.check(_lib.lib().regb_estimate_affine_param(C.byref(_vol(source)), _fptr(np.asarray(source_vs, np.float32)),
+                                                     C.byref(_vol(target)), _fptr(np.asarray(target_vs, np.float32)),
+                                                     _fptr(a)), allow=(_lib.REGB_OK, _lib.REGB_FALSE))
+    return a
+
+
 # ---------------------------------------------------------------- resample / costs
 def resample(src, out_shape, T, allow_shift_copy=True, out=None, stream=None):
     """tipl::resample<linear>(src, out_shape, T)."""

@@ -101,6 +101,9 @@ _SIGS = {
     "regb_affine_to_matrix": (C.c_int, [C.c_void_p] * 6),
     "regb_affine_to_matrix_f64": (C.c_int, [C.c_void_p] * 6),
     "regb_matrix_inverse": (C.c_int, [C.c_void_p]),
+    "regb_matrix_to_affine_param": (C.c_int, [C.c_void_p] * 6),
+    "regb_has_mask": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "regb_estimate_affine_param": (C.c_int, [C.c_void_p] * 5),
     "regb_resample": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p]),
     "regb_mi_cost": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p,
                                C.c_void_p, C.c_void_p]),

@@ -7,6 +7,7 @@
 #include "affine_eval.h"
 #include "cdm_level.h"
 #include "host.h"
+#include "mask_init.h"
 
 namespace regb {
 const std::string& last_error();
@@ -205,6 +206,54 @@ regb_status regb_matrix_inverse(float T[12])
     if (!T)
         return REGB_ERR_ARG;
     return matrix_inverse(T) ? REGB_OK : REGB_FALSE;
+}
+
+regb_status regb_matrix_to_affine_param(const float T[12], const int from_dim[3], const float from_vs[3],
+                                        const int to_dim[3], const float to_vs[3], float param[12])
+{
+    return guarded([&] {
+        if (!T || !from_dim || !from_vs || !to_dim || !to_vs || !param)
+            throw Failure(REGB_ERR_ARG, "null argument");
+        matrix_to_affine_param(T, from_dim, from_vs, to_dim, to_vs, param);
+        return REGB_OK;
+    });
+}
+
+regb_status regb_has_mask(const regb_volume* img, int* out)
+{
+    return guarded([&] {
+        check_vol(img, "img");
+        if (img->dtype != REGB_U8 || !out)
+            throw Failure(REGB_ERR_ARG, "has_mask takes a uint8 volume and an output");
+        Stream s;
+        Staged a;
+        a.in(img->ptr, nvox(img->dim), img->location, s.s, true);
+        MaskCounts c;
+        mask_counts((const uint8_t*)a.d, img->dim, c, s.s);
+        *out = has_mask(c) ? 1 : 0;
+        return REGB_OK;
+    });
+}
+
+regb_status regb_estimate_affine_param(const regb_volume* source, const float source_vs[3],
+                                       const regb_volume* target, const float target_vs[3], float param[12])
+{
+    return guarded([&] {
+        check_vol(source, "source");
+        check_vol(target, "target");
+        if (source->dtype != REGB_U8 || target->dtype != REGB_U8)
+            throw Failure(REGB_ERR_ARG, "estimate_affine_param takes uint8 volumes");
+        if (!source_vs || !target_vs || !param)
+            throw Failure(REGB_ERR_ARG, "null voxel size / param");
+        Stream s;
+        Staged a, b;
+        a.in(source->ptr, nvox(source->dim), source->location, s.s, true);
+        b.in(target->ptr, nvox(target->dim), target->location, s.s, true);
+        MaskCounts cs, ct;
+        mask_counts((const uint8_t*)a.d, source->dim, cs, s.s);
+        mask_counts((const uint8_t*)b.d, target->dim, ct, s.s);
+        return estimate_affine_param(cs, source_vs, ct, target_vs, param) ? REGB_OK : REGB_FALSE;
+    });
 }
 
 regb_status regb_resample(const regb_volume* from, regb_volume* to, const float T[12], int allow_shift_copy,

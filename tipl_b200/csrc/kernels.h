@@ -110,4 +110,8 @@ int cdm_blocks_for(long long nvox);
 // out[i] = segs[i].ctl->done
 cudaError_t launch_cdm_status(const CdmSeg* segs, int nseg, int* out, cudaStream_t st);
 
+// Voxels > 0 per (x, y), (x, z), (y, z) line of a uint8 volume (zeroes the tables first).
+cudaError_t launch_mask_counts(const uint8_t* v, Dim3 dim, uint32_t* xy, uint32_t* xz, uint32_t* yz,
+                               cudaStream_t st);
+
 }  // namespace regb

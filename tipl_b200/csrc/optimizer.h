@@ -192,9 +192,14 @@ inline void lbfgs(Vec& x, const float* up, const float* lo, const BatchFn& fun, 
 // line_search (numerical/optimization.hpp:272-512): per active axis a grid of
 // grid_samples steps (linear spacing for translations, cubic for the rest), then
 // a search along the resultant of the best steps; two rounds with a shrinking
-// range.  Each grid is one evaluation set; results are applied in sample order.
+// range.  Each grid is one evaluation set.  The reference runs the samples as
+// parallel tasks that each check for termination (the caller's check also
+// exchanges best points with the other search thread) and then apply their cost;
+// here the results are applied task by task in sample order, each after
+// is_terminated() and tick() (the time one evaluation takes).
 inline void line_search(Vec& x, const float* up, const float* lo, const std::vector<int>& strategy,
-                        const BatchFn& fun, double& optimal_value, int grid_samples, const StopFn& is_terminated)
+                        const BatchFn& fun, double& optimal_value, int grid_samples, const StopFn& is_terminated,
+                        const std::function<void()>& tick = [] {})
 {
     const size_t size = x.size();
     const double ftol = 0.05;
@@ -242,7 +247,7 @@ inline void line_search(Vec& x, const float* up, const float* lo, const std::vec
         std::vector<double> costs(size * grid_samples, fp), steps(size * grid_samples, 0.0);
         {
             std::vector<Vec> cand;
-            std::vector<int> where;
+            std::vector<int> where;  // per task: its candidate, or -1 (zero step)
             for (size_t a = 0; a < active.size(); ++a)
                 for (int s = 0; s < grid_samples; ++s) {
                     const int i = active[a];
@@ -258,24 +263,34 @@ inline void line_search(Vec& x, const float* up, const float* lo, const std::vec
                         trial = (v > 0.0) ? (v * cu[i]) : (v * -cl[i]);
                     }
                     steps[li] = trial;
-                    if (std::abs(trial) < 1e-8)
+                    if (std::abs(trial) < 1e-8) {
+                        where.push_back(-1);
                         continue;
+                    }
                     Vec t(p);
                     for (size_t j = 0; j < size; ++j)
                         t[j] = std::min<float>(up[j], std::max<float>(lo[j], (float)(p[j] + trial * xi[i][j])));
+                    where.push_back((int)cand.size());
                     cand.push_back(std::move(t));
-                    where.push_back(li);
                 }
-            if (!cand.empty()) {
-                auto r = fun(cand);
-                for (size_t k = 0; k < r.size(); ++k) {
-                    costs[where[k]] = r[k];
+            std::vector<double> r;
+            if (!cand.empty())
+                r = fun(cand);
+            size_t task = 0;
+            for (size_t a = 0; a < active.size(); ++a)
+                for (int s = 0; s < grid_samples; ++s, ++task) {
+                    if (is_terminated())
+                        continue;
+                    const int k = where[task];
+                    if (k < 0)
+                        continue;
+                    tick();
+                    costs[active[a] * grid_samples + s] = r[k];
                     if (r[k] < optimal_value) {
                         optimal_value = r[k];
                         x = cand[k];
                     }
                 }
-            }
         }
         if (is_terminated())
             return;
@@ -321,22 +336,32 @@ inline void line_search(Vec& x, const float* up, const float* lo, const std::vec
                 const double st = (bp - bn) / (grid_samples - 1);
                 if (st > 1e-8) {
                     std::vector<Vec> cand;
+                    std::vector<int> where;
                     for (int s = 0; s < grid_samples; ++s) {
                         const double trial = bn + s * st;
                         if (std::abs(trial) > 1e-8) {
                             Vec t(p);
                             for (size_t j = 0; j < size; ++j)
                                 t[j] = std::min<float>(up[j], std::max<float>(lo[j], (float)(p[j] + trial * dir[j])));
+                            where.push_back((int)cand.size());
                             cand.push_back(std::move(t));
-                        }
+                        } else
+                            where.push_back(-1);
                     }
-                    if (!cand.empty()) {
-                        auto r = fun(cand);
-                        for (size_t k = 0; k < r.size(); ++k)
-                            if (r[k] < optimal_value) {
-                                optimal_value = r[k];
-                                x = cand[k];
-                            }
+                    std::vector<double> r;
+                    if (!cand.empty())
+                        r = fun(cand);
+                    for (int s = 0; s < grid_samples; ++s) {
+                        if (is_terminated())
+                            continue;
+                        const int k = where[s];
+                        if (k < 0)
+                            continue;
+                        tick();
+                        if (r[k] < optimal_value) {
+                            optimal_value = r[k];
+                            x = cand[k];
+                        }
                     }
                 }
             }
