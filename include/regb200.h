@@ -122,6 +122,17 @@ regb_status regb_matrix_inverse(float T[12]);
 regb_status regb_matrix_to_affine_param(const float T[12], const int from_dim[3], const float from_vs[3],
                                         const int to_dim[3], const float to_vs[3], float param[12]);
 
+/* ---- storage conversions ------------------------------------------------------------ */
+/* normalize_upper_lower2(in, out, upper) (numerical/numerical.hpp:909-927) on the device:
+ * out = uint8((in - min) * (upper / (max - min))) for a U8, F32, U16 or BF16 volume, in
+ * the reference's float arithmetic.  The reference's callers quantise this way, with
+ * upper = 255.999, before tipl::reg::linear.  REGB_FALSE (out untouched) when the volume
+ * is constant, as the reference then returns without writing. */
+regb_status regb_normalize_to_u8(const regb_volume* in, regb_volume* out, float upper, void* stream);
+/* Exact widening of a U8, U16 or BF16 volume to F32 (BF16 = the upper 16 bits of an IEEE
+ * float); the FP32 nonlinear path runs on volumes stored this way. */
+regb_status regb_widen_to_f32(const regb_volume* in, regb_volume* out, void* stream);
+
 /* ---- mask-moment initialisation of linear() (reg/linear.hpp:658-684) --------------- */
 /* has_mask(img) (numerical/basic_op.hpp:811-830) of a uint8 volume: *out = 1 when more
  * than a fifth of its voxels are 0 or its non-zero voxels' bounding box lies inside the

@@ -98,6 +98,8 @@ class Oracle(_Lib):
         L.orc_mi_cost_from_hist.restype = C.c_double
         L.orc_mi_cost_u8.restype = C.c_double
         L.orc_corr_cost_u8.restype = C.c_double
+        L.orc_mi_cost_u8_f64.restype = C.c_double
+        L.orc_corr_cost_u8_f64.restype = C.c_double
         for n in ("orc_cdm_gradient_u8", "orc_cdm_gradient_f32", "orc_cdm_max_len_f32"):
             getattr(L, n).restype = C.c_float
         for n in ("orc_cdm_gradient_f64", "orc_cdm_max_len_f64"):
@@ -107,6 +109,16 @@ class Oracle(_Lib):
         for sfx in ("u8", "f32", "f64"):
             getattr(L, f"orc_cdm_level_{sfx}").argtypes = [_P, _P, _P, _P, C.c_float, C.c_float, C.c_float,
                                                           C.c_uint, C.c_int, _P]
+
+    def normalize_to_u8(self, img, upper=255.999):
+        """normalize_upper_lower2 of a float32 or uint16 volume; (out, ok)."""
+        out = np.zeros(img.shape, np.uint8)
+        if img.dtype == np.uint16:
+            ok = self.lib.orc_normalize_to_u8_u16(_ptr(np.ascontiguousarray(img)), C.c_longlong(img.size), _ptr(out),
+                                                  C.c_float(upper))
+        else:
+            ok = self.lib.orc_normalize_to_u8_f32(_ptr(_f32(img)), C.c_longlong(img.size), _ptr(out), C.c_float(upper))
+        return out, bool(ok)
 
     # -- transforms
     def affine_to_matrix(self, param, from_shape, from_vs, to_shape, to_vs) -> np.ndarray:
@@ -158,6 +170,15 @@ class Oracle(_Lib):
     def mi_cost(self, fixed, moving, T) -> float:
         return self.lib.orc_mi_cost_u8(_ptr(_u8(fixed)), _ptr(_dims(fixed.shape)), _ptr(_u8(moving)),
                                        _ptr(_dims(moving.shape)), _ptr(_f32(T)))
+
+    def mi_cost_f64(self, fixed, moving, T64) -> float:
+        """MI cost with the transform and interpolation in double (error reporting)."""
+        return self.lib.orc_mi_cost_u8_f64(_ptr(_u8(fixed)), _ptr(_dims(fixed.shape)), _ptr(_u8(moving)),
+                                           _ptr(_dims(moving.shape)), _ptr(np.ascontiguousarray(T64, np.float64)))
+
+    def corr_cost_f64(self, fixed, moving, T64) -> float:
+        return self.lib.orc_corr_cost_u8_f64(_ptr(_u8(fixed)), _ptr(_dims(fixed.shape)), _ptr(_u8(moving)),
+                                             _ptr(_dims(moving.shape)), _ptr(np.ascontiguousarray(T64, np.float64)))
 
     def corr_cost(self, fixed, moving, T) -> float:
         return self.lib.orc_corr_cost_u8(_ptr(_u8(fixed)), _ptr(_dims(fixed.shape)), _ptr(_u8(moving)),
@@ -373,6 +394,12 @@ class Reference(_Lib):
                                           _ptr(_u8(moving)), _ptr(_dims(moving.shape)), _ptr(_f32(moving_vs)),
                                           _ptr(a), int(reg_type), int(cost_type), int(bound))
         return float(c), a
+
+    def normalize_u16_to_u8(self, img, upper=255.999):
+        out = np.zeros(img.shape, np.uint8)
+        self.lib.tiplref_normalize_u16_to_u8(_ptr(np.ascontiguousarray(img, np.uint16)), _ptr(_dims(img.shape)),
+                                             _ptr(out), C.c_float(upper))
+        return out
 
     def normalize_to_u8(self, img, upper=255.999):
         out = np.zeros(img.shape, np.uint8)

@@ -245,6 +245,34 @@ int orc_is_integer_shift(const float* T, int* shift)
 #undef PIX
 #undef R
 
+/* ---- quantisation to uint8 ------------------------------------------------ */
+
+/* normalize_upper_lower2(in, out, upper) (numerical/numerical.hpp:909-927): float
+ * min/max, out = uint8((v - min) * (upper / (max - min))) truncated; returns 0 and
+ * leaves out untouched for a constant volume. */
+#define ORC_NORMALIZE(NAME, T)                                                  \
+    int NAME(const T* in, long long n, uint8_t* out, float upper)               \
+    {                                                                           \
+        if (n <= 0)                                                             \
+            return 0;                                                           \
+        float mn = (float)in[0], mx = (float)in[0];                             \
+        for (long long i = 1; i < n; ++i) {                                     \
+            const float v = (float)in[i];                                       \
+            if (v < mn) mn = v;                                                 \
+            if (v > mx) mx = v;                                                 \
+        }                                                                       \
+        const float range = mx - mn;                                            \
+        if (range == 0.0f)                                                      \
+            return 0;                                                           \
+        upper /= range;                                                         \
+        for (long long i = 0; i < n; ++i)                                       \
+            out[i] = (uint8_t)(((float)in[i] - mn) * upper);                    \
+        return 1;                                                               \
+    }
+ORC_NORMALIZE(orc_normalize_to_u8_f32, float)
+ORC_NORMALIZE(orc_normalize_to_u8_u16, uint16_t)
+#undef ORC_NORMALIZE
+
 /* ---- mask-moment initialisation of linear() ------------------------------- */
 #include "oracle_mask.h"
 
@@ -312,6 +340,80 @@ double orc_mi_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, c
     double c = orc_mi_cost_from_hist(hist, fh);
     free(hist);
     return c;
+}
+
+/* ---- FP64 restatement of the affine costs (error reporting only) ----------
+ * The same algorithm as orc_mi_cost_u8 / orc_corr_cost_u8 with every float step in
+ * double: the transform (given in double), the trilinear weights and the weighted
+ * sum; the uint8 quantisation of the sampled value stays (it is part of the
+ * algorithm: the joint histogram bins and the resampled volume are uint8). */
+static int trilinear_u8_f64(const uint8_t* I, const int* dim, double x, double y, double z, uint8_t* out)
+{
+    if (x < 0 || y < 0 || z < 0)
+        return 0;
+    size_t ix = (size_t)x, iy = (size_t)y, iz = (size_t)z;
+    size_t w = (size_t)dim[0];
+    if (ix + 1 >= w || iy + 1 >= (size_t)dim[1] || iz + 1 >= (size_t)dim[2])
+        return 0;
+    double p0 = x - (double)ix, p1 = y - (double)iy, p2 = z - (double)iz;
+    double n0 = 1 - p0, n1 = 1 - p1, n2 = 1 - p2;
+    size_t wh = w * (size_t)dim[1];
+    size_t d0 = iz * wh + iy * w + ix;
+    size_t d[8] = {d0, d0 + 1, d0 + w, d0 + w + 1, d0 + wh, d0 + 1 + wh, d0 + w + wh, d0 + w + 1 + wh};
+    double r[8] = {n0 * n1 * n2, p0 * n1 * n2, n0 * p1 * n2, p0 * p1 * n2,
+                   n0 * n1 * p2, p0 * n1 * p2, n0 * p1 * p2, p0 * p1 * p2};
+    double acc = 0.0;
+    for (int i = 0; i < 8; ++i)
+        acc += (double)I[d[i]] * r[i];
+    *out = (uint8_t)(acc <= 0.0 ? 0 : (unsigned)acc);
+    return 1;
+}
+
+double orc_mi_cost_u8_f64(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const double* T)
+{
+    int32_t* hist = (int32_t*)calloc(65536, sizeof(int32_t));
+    int32_t fh[256];
+    orc_histogram_u8(from, (long long)fdim[0] * fdim[1] * fdim[2], fh);
+    size_t i = 0;
+    for (int z = 0; z < fdim[2]; ++z)
+        for (int y = 0; y < fdim[1]; ++y)
+            for (int x = 0; x < fdim[0]; ++x, ++i) {
+                const double px = x * T[0] + y * T[1] + z * T[2] + T[9];
+                const double py = x * T[3] + y * T[4] + z * T[5] + T[10];
+                const double pz = x * T[6] + y * T[7] + z * T[8] + T[11];
+                uint8_t v = 0;
+                trilinear_u8_f64(to, tdim, px, py, pz, &v);
+                ++hist[((uint32_t)from[i] << 8) + v];
+            }
+    double c = orc_mi_cost_from_hist(hist, fh);
+    free(hist);
+    return c;
+}
+
+/* correlation in FP64 on the fixed grid (no role swap, no integer-shift copy): r from
+ * the template and the double-interpolated, uint8-quantised moving volume; 1 - r^2. */
+double orc_corr_cost_u8_f64(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const double* T)
+{
+    long long nf = (long long)fdim[0] * fdim[1] * fdim[2];
+    double sx = 0, sy = 0, sxx = 0, syy = 0, sxy = 0;
+    size_t i = 0;
+    for (int z = 0; z < fdim[2]; ++z)
+        for (int y = 0; y < fdim[1]; ++y)
+            for (int x = 0; x < fdim[0]; ++x, ++i) {
+                const double px = x * T[0] + y * T[1] + z * T[2] + T[9];
+                const double py = x * T[3] + y * T[4] + z * T[5] + T[10];
+                const double pz = x * T[6] + y * T[7] + z * T[8] + T[11];
+                uint8_t v = 0;
+                trilinear_u8_f64(to, tdim, px, py, pz, &v);
+                const double a = from[i], b = v;
+                sx += a; sy += b; sxx += a * a; syy += b * b; sxy += a * b;
+            }
+    const double n = (double)nf, mx = sx / n, my = sy / n;
+    const double vx = sxx / n - mx * mx, vy = syy / n - my * my;
+    if (vx <= 0 || vy <= 0)
+        return 1.0;
+    const double r = (sxy / n - mx * my) / sqrt(vx) / sqrt(vy);
+    return 1.0 - r * r;
 }
 
 /* correlation functor CPU (reg/linear.hpp:23-37): the smaller volume is the

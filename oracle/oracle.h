@@ -34,6 +34,8 @@ void orc_mi_hist_u8(const uint8_t* from, const int* fdim, const uint8_t* to, con
 double orc_mi_cost_from_hist(const int32_t* hist, const int32_t* from_hist);
 double orc_mi_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T);
 double orc_corr_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T);
+double orc_mi_cost_u8_f64(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const double* T);
+double orc_corr_cost_u8_f64(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const double* T);
 
 void orc_compose_u8(const uint8_t* Is, const int* dim, const float* dis, uint8_t* Js);
 void orc_compose_f32(const float* Is, const int* dim, const float* dis, float* Js);
@@ -63,6 +65,8 @@ int orc_cdm_level_f32(const float* It, const float* Is, const int* dim, float* b
 int orc_cdm_level_f64(const double* It, const double* Is, const int* dim, double* best_d, float resolution,
                       float speed, float smoothing, unsigned int min_dimension, int gradient_type, int* iters_out);
 
+int orc_normalize_to_u8_f32(const float* in, long long n, uint8_t* out, float upper);
+int orc_normalize_to_u8_u16(const uint16_t* in, long long n, uint8_t* out, float upper);
 int orc_has_mask_u8(const uint8_t* img, const int* dim);
 void orc_eigen_sym3(const double* A, double* V, double* d);
 void orc_estimate_affine_param_u8(const uint8_t* src, const int* sdim, const float* svs, const uint8_t* tgt,

@@ -302,4 +302,13 @@ void tiplref_normalize_to_u8(const float* in, const int* dim, u8* out, float upp
         std::copy(o.begin(), o.end(), out);
 }
 
+// normalize_upper_lower2 of a uint16 volume (numerical/numerical.hpp:909-927)
+void tiplref_normalize_u16_to_u8(const unsigned short* in, const int* dim, u8* out, float upper)
+{
+    tipl::image<3, u8> o;
+    tipl::normalize_upper_lower2(cview(in, dim), o, upper);
+    if (o.size() == size_t(dim[0]) * dim[1] * dim[2])
+        std::copy(o.begin(), o.end(), out);
+}
+
 }  // extern "C"

@@ -40,6 +40,18 @@ def main():
         core(R)
     if args.only in (None, "mask_init"):
         mask_init(R)
+    if args.only in (None, "precision"):
+        precision(R)
+
+
+def precision(R):
+    """normalize_upper_lower2 of float32 and uint16 volumes (the quantisation before linear())."""
+    rng = np.random.default_rng(ph.seed_for(4, 9))
+    t = ph.class_phantom((26, 30, 22), rng)                       # float32 in [0, 4095]
+    u = np.round(t + rng.normal(0, 20, t.shape)).clip(0, 4095).astype(np.uint16)
+    neg = (t - 1000.0 + rng.normal(0, 5, t.shape)).astype(np.float32)  # negative values too
+    save("precision", f32=t, u16=u, neg=neg, q_f32=R.normalize_to_u8(t), q_u16=R.normalize_u16_to_u8(u),
+         q_neg=R.normalize_to_u8(neg), q_f32_200=R.normalize_to_u8(t, 200.0))
 
 
 def mask_init(R):

@@ -49,12 +49,38 @@ def _dims(shape):
     return arr
 
 
+class BF16(np.ndarray):
+    """A host volume stored as BF16: a uint16 array holding the upper 16 bits of each
+    float32 value (make one with to_bf16).  Device volumes use torch.bfloat16."""
+
+    def __new__(cls, bits):
+        return np.ascontiguousarray(bits, dtype=np.uint16).view(cls)
+
+
+def to_bf16(a) -> BF16:
+    """float32 -> BF16 storage, rounding to nearest even."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return BF16(r.astype(np.uint16))
+
+
+def from_bf16(b) -> np.ndarray:
+    """BF16 storage -> the float32 values it holds (exact)."""
+    return (np.asarray(b, dtype=np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
 def _dtype_code(a) -> int:
+    if isinstance(a, BF16):
+        return _lib.BF16
     name = str(a.dtype)
     if name in ("uint8", "torch.uint8"):
         return _lib.U8
     if name in ("float32", "torch.float32"):
         return _lib.F32
+    if name in ("uint16", "torch.uint16"):
+        return _lib.U16
+    if name == "torch.bfloat16":
+        return _lib.BF16
     raise TypeError(f"unsupported dtype {a.dtype}")
 
 
@@ -135,6 +161,34 @@ def matrix_to_affine_param(T, from_shape, from_vs, to_shape, to_vs) -> np.ndarra
     _lib.check(_lib.lib().regb_matrix_to_affine_param(_fptr(M), _fptr(fd), _fptr(np.asarray(from_vs, np.float32)),
                                                       _fptr(td), _fptr(np.asarray(to_vs, np.float32)), _fptr(a)))
     return a
+
+
+def normalize_to_u8(img, upper=255.999, out=None, stream=None):
+    """normalize_upper_lower2(img, out, upper) on the device: uint8 of (v - min) * upper / (max - min).
+    Returns (out, ok); ok is False (out untouched) for a constant volume."""
+    if out is None:
+        if _is_dev(img):
+            import torch
+
+            out = torch.zeros(tuple(img.shape), dtype=torch.uint8, device=img.device)
+        else:
+            out = np.zeros(img.shape, np.uint8)
+    st = _lib.check(_lib.lib().regb_normalize_to_u8(C.byref(_vol(img)), C.byref(_vol(out)), float(upper),
+                                                    _stream(stream)), allow=(_lib.REGB_OK, _lib.REGB_FALSE))
+    return out, st == _lib.REGB_OK
+
+
+def widen_to_f32(img, out=None, stream=None):
+    """Exact widening of a uint8 / uint16 / BF16 volume to float32."""
+    if out is None:
+        if _is_dev(img):
+            import torch
+
+            out = torch.zeros(tuple(img.shape), dtype=torch.float32, device=img.device)
+        else:
+            out = np.zeros(img.shape, np.float32)
+    _lib.check(_lib.lib().regb_widen_to_f32(C.byref(_vol(img)), C.byref(_vol(out)), _stream(stream)))
+    return out
 
 
 def has_mask(img) -> bool:

@@ -8,6 +8,7 @@
 #include "cdm_level.h"
 #include "host.h"
 #include "mask_init.h"
+#include "stats.h"
 
 namespace regb {
 const std::string& last_error();
@@ -215,6 +216,55 @@ regb_status regb_matrix_to_affine_param(const float T[12], const int from_dim[3]
         if (!T || !from_dim || !from_vs || !to_dim || !to_vs || !param)
             throw Failure(REGB_ERR_ARG, "null argument");
         matrix_to_affine_param(T, from_dim, from_vs, to_dim, to_vs, param);
+        return REGB_OK;
+    });
+}
+
+regb_status regb_normalize_to_u8(const regb_volume* in, regb_volume* out, float upper, void* stream)
+{
+    return guarded([&] {
+        check_vol(in, "in", false);
+        check_vol(out, "out");
+        if (!pix_size(in->dtype) || out->dtype != REGB_U8 || !same_dims(in->dim, out->dim))
+            throw Failure(REGB_ERR_ARG, "normalize: in U8/F32/U16/BF16, out U8 of the same shape");
+        const bool dev = in->location == REGB_DEVICE && out->location == REGB_DEVICE;
+        Stream own;
+        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : own.s;
+        const size_t n = nvox(in->dim);
+        Staged a, b;
+        a.in(in->ptr, n * pix_size(in->dtype), in->location, st, true);
+        b.in(out->ptr, n, out->location, st, true);
+        DevBuf<unsigned> mm(2, st);
+        REGB_CK(launch_normalize_to_u8(a.d, in->dtype, (long long)n, upper, (uint8_t*)b.d, mm.p, st));
+        count_launch(2);
+        b.out(out->ptr, st);
+        unsigned h[2];
+        REGB_CK(cudaMemcpyAsync(h, mm.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        REGB_CK(cudaStreamSynchronize(st));
+        return h[0] == h[1] ? REGB_FALSE : REGB_OK;
+    });
+}
+
+regb_status regb_widen_to_f32(const regb_volume* in, regb_volume* out, void* stream)
+{
+    return guarded([&] {
+        check_vol(in, "in", false);
+        check_vol(out, "out");
+        if (!pix_size(in->dtype) || in->dtype == REGB_F32 || out->dtype != REGB_F32 ||
+            !same_dims(in->dim, out->dim))
+            throw Failure(REGB_ERR_ARG, "widen: in U8/U16/BF16, out F32 of the same shape");
+        const bool dev = in->location == REGB_DEVICE && out->location == REGB_DEVICE;
+        Stream own;
+        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : own.s;
+        const size_t n = nvox(in->dim);
+        Staged a, b;
+        a.in(in->ptr, n * pix_size(in->dtype), in->location, st, true);
+        b.in(out->ptr, n * 4, out->location, st, false);
+        REGB_CK(launch_widen_to_f32(a.d, in->dtype, (long long)n, (float*)b.d, st));
+        count_launch();
+        b.out(out->ptr, st);
+        if (!dev || !stream)
+            REGB_CK(cudaStreamSynchronize(st));
         return REGB_OK;
     });
 }

@@ -25,6 +25,8 @@
 #include <thread>
 #include "batcher.h"
 #include "host.h"
+#include "kernels.h"
+#include "stats.h"
 #include "scheduler.h"
 
 using Clock = std::chrono::steady_clock;
@@ -32,11 +34,36 @@ using Clock = std::chrono::steady_clock;
 namespace regb {
 
 struct EngineTemplate {
-    DevBuf<uint8_t> data;
+    DevBuf<uint8_t> data;  // as given (U8, F32, U16 or BF16)
+    DevBuf<uint8_t> u8;    // normalize_upper_lower2(data, 255.999) when data is not U8
+    DevBuf<float> f32;     // data widened to float when it is U16 or BF16
     int dim[3];
     int dtype;
     float vs[3];
+    const uint8_t* as_u8() const { return dtype == REGB_U8 ? data.p : u8.p; }
+    const float* as_f32() const { return dtype == REGB_F32 ? (const float*)data.p : f32.p; }
 };
+
+// The affine stage quantises a volume that is not uint8 the way the reference's
+// callers do before tipl::reg::linear: normalize_upper_lower2(v, 255.999)
+// (numerical/numerical.hpp:909-927).
+constexpr float kQuantUpper = 255.999f;
+
+void to_u8(const void* d, int dtype, size_t n, DevBuf<uint8_t>& out, cudaStream_t st)
+{
+    DevBuf<unsigned> mm(2, st);
+    out.alloc(n, st);
+    REGB_CK(cudaMemsetAsync(out.p, 0, n, st));
+    REGB_CK(launch_normalize_to_u8(d, dtype, (long long)n, kQuantUpper, out.p, mm.p, st));
+    count_launch(2);
+}
+
+void to_f32(const void* d, int dtype, size_t n, DevBuf<float>& out, cudaStream_t st)
+{
+    out.alloc(n, st);
+    REGB_CK(launch_widen_to_f32(d, dtype, (long long)n, out.p, st));
+    count_launch();
+}
 
 struct EngineJob {
     uint64_t id = 0;
@@ -83,6 +110,11 @@ public:
         t->data.alloc(n, util_.s);
         REGB_CK(cudaMemcpyAsync(t->data.p, v.ptr, n, v.location == REGB_HOST ? cudaMemcpyHostToDevice
                                                                               : cudaMemcpyDeviceToDevice, util_.s));
+        const size_t nv = (size_t)v.dim[0] * v.dim[1] * v.dim[2];
+        if (v.dtype != REGB_U8)
+            to_u8(t->data.p, v.dtype, nv, t->u8, util_.s);
+        if (v.dtype == REGB_U16 || v.dtype == REGB_BF16)
+            to_f32(t->data.p, v.dtype, nv, t->f32, util_.s);
         util_.sync();
         std::memcpy(t->dim, v.dim, sizeof(t->dim));
         t->dtype = v.dtype;
@@ -185,10 +217,17 @@ private:
         if (j.template_id < 0)
             b += nf * ps;
         b += nm * (double)pix_size(j.moving.dtype);
+        const bool float_cdm = ftype != REGB_U8 || j.moving.dtype != REGB_U8;
+        if (j.moving.dtype != REGB_U8)
+            b += nm;                          // uint8 copy for the affine stage
+        if (j.template_id < 0 && ftype != REGB_U8)
+            b += nf;
+        if (j.run_cdm && float_cdm)
+            b += 4.0 * (nm + (j.template_id < 0 ? nf : 0.0));  // float copies for CDM
         if (j.run_linear)
             b += 0.15 * (nf + nm);
         if (j.run_cdm) {
-            b += nf * ps + 12.0 * nf;  // resampled subject, output field
+            b += nf * (float_cdm ? 4.0 : ps) + 12.0 * nf;  // resampled subject, output field
             // the largest iterated level: 5 fields + composed image
             int w = fd[0], h = fd[1], d = fd[2];
             float res = j.cdm.resolution;
@@ -259,10 +298,13 @@ private:
         Stream st;
         // fixed volume: resident template or the job's own
         const void* d_fixed;
+        const uint8_t* fixed_u8 = nullptr;  // the affine stage's view
+        const float* fixed_f32 = nullptr;   // the float CDM stage's view
         int fdim[3];
         int fdtype;
         float fvs[3];
-        DevBuf<uint8_t> own_fixed, own_moving;
+        DevBuf<uint8_t> own_fixed, own_moving, fixed_q, moving_q;
+        DevBuf<float> fixed_w, moving_w;
         if (s.template_id >= 0) {
             const EngineTemplate* t;
             {
@@ -270,6 +312,8 @@ private:
                 t = templates_.at(s.template_id).get();
             }
             d_fixed = t->data.p;
+            fixed_u8 = t->as_u8();
+            fixed_f32 = t->as_f32();
             std::memcpy(fdim, t->dim, sizeof(fdim));
             fdtype = t->dtype;
             std::memcpy(fvs, t->vs, sizeof(fvs));
@@ -285,12 +329,47 @@ private:
             fdtype = s.fixed.dtype;
             std::memcpy(fvs, s.fixed_vs, sizeof(fvs));
         }
-        const size_t mb = (size_t)s.moving.dim[0] * s.moving.dim[1] * s.moving.dim[2] * pix_size(s.moving.dtype);
+        const size_t nm = (size_t)s.moving.dim[0] * s.moving.dim[1] * s.moving.dim[2];
+        const size_t nfx = (size_t)fdim[0] * fdim[1] * fdim[2];
+        const size_t mb = nm * pix_size(s.moving.dtype);
         const void* d_moving = s.moving.ptr;
         if (s.moving.location == REGB_HOST) {
             own_moving.alloc(mb, st.s);
             REGB_CK(cudaMemcpyAsync(own_moving.p, s.moving.ptr, mb, cudaMemcpyHostToDevice, st.s));
             d_moving = own_moving.p;
+        }
+        if (s.template_id < 0) {
+            if (fdtype == REGB_U8)
+                fixed_u8 = (const uint8_t*)d_fixed;
+            else if (s.run_linear) {
+                to_u8(d_fixed, fdtype, nfx, fixed_q, st.s);
+                fixed_u8 = fixed_q.p;
+            }
+        }
+        const uint8_t* moving_u8 = (const uint8_t*)d_moving;
+        if (s.moving.dtype != REGB_U8 && s.run_linear) {
+            to_u8(d_moving, s.moving.dtype, nm, moving_q, st.s);
+            moving_u8 = moving_q.p;
+        }
+        // CDM runs on uint8 when both volumes are uint8 (the reference GPU path's type),
+        // otherwise in float on the volumes widened exactly from their storage type
+        const bool float_cdm = fdtype != REGB_U8 || s.moving.dtype != REGB_U8;
+        const float* moving_f32 = nullptr;
+        if (s.run_cdm && float_cdm) {
+            if (!fixed_f32 || s.template_id < 0) {
+                if (fdtype == REGB_F32)
+                    fixed_f32 = (const float*)d_fixed;
+                else {
+                    to_f32(d_fixed, fdtype, nfx, fixed_w, st.s);
+                    fixed_f32 = fixed_w.p;
+                }
+            }
+            if (s.moving.dtype == REGB_F32)
+                moving_f32 = (const float*)d_moving;
+            else {
+                to_f32(d_moving, s.moving.dtype, nm, moving_w, st.s);
+                moving_f32 = moving_w.p;
+            }
         }
         st.sync();
         r.status = REGB_OK;
@@ -298,8 +377,8 @@ private:
             batcher_.add_client();
             LinearResult lr;
             try {
-                lr = linear_register((const uint8_t*)d_fixed, fdim, fvs, (const uint8_t*)d_moving, s.moving.dim,
-                                     s.moving_vs, r.arg, s.linear, &j->cancel, st.s, &batcher_);
+                lr = linear_register(fixed_u8, fdim, fvs, moving_u8, s.moving.dim, s.moving_vs, r.arg, s.linear,
+                                     &j->cancel, st.s, &batcher_);
             } catch (...) {
                 batcher_.remove_client();
                 throw;
@@ -315,8 +394,8 @@ private:
         if (s.run_cdm) {
             // the subject resampled onto the template grid with the affine found
             // (the mm_reg pipeline, reg/mm_reg.hpp:379-416)
-            const int pix = (fdtype == REGB_F32) ? 1 : 0;
-            const size_t nf = (size_t)fdim[0] * fdim[1] * fdim[2];
+            const int pix = float_cdm ? 1 : 0;
+            const size_t nf = nfx;
             DevBuf<uint8_t> Is(nf * (pix ? 4 : 1), st.s);
             float T[12];
             affine_to_matrix(r.arg, fdim, fvs, s.moving.dim, s.moving_vs, T);
@@ -324,12 +403,13 @@ private:
             const int* sh = integer_shift(T, shift) ? shift : nullptr;
             const Dim3 md{s.moving.dim[0], s.moving.dim[1], s.moving.dim[2]}, fdd{fdim[0], fdim[1], fdim[2]};
             if (pix)
-                REGB_CK(launch_resample<float>((const float*)d_moving, md, (float*)Is.p, fdd, T, sh, st.s));
+                REGB_CK(launch_resample<float>(moving_f32, md, (float*)Is.p, fdd, T, sh, st.s));
             else
                 REGB_CK(launch_resample<uint8_t>((const uint8_t*)d_moving, md, Is.p, fdd, T, sh, st.s));
             DevBuf<float> field(3 * nf, st.s);
             int iters = 0;
-            regb_status cs = cdm_register(d_fixed, Is.p, fdim, pix, field.p, s.cdm, &j->cancel, st.s, &iters, &sched_);
+            regb_status cs = cdm_register(pix ? (const void*)fixed_f32 : d_fixed, Is.p, fdim, pix, field.p, s.cdm,
+                                          &j->cancel, st.s, &iters, &sched_);
             r.cdm_ok = (cs == REGB_OK) ? 1 : 0;
             r.cdm_iterations = iters;
             if (cs == REGB_CANCELLED)
@@ -386,7 +466,7 @@ bool vol_ok(const regb_volume& v)
 {
     return v.ptr && v.dim[0] > 0 && v.dim[1] > 0 && v.dim[2] > 0 &&
            (long long)v.dim[0] * v.dim[1] * v.dim[2] < (1LL << 31) && pix_size(v.dtype) &&
-           (v.dtype == REGB_U8 || v.dtype == REGB_F32) && (v.location == REGB_HOST || v.location == REGB_DEVICE);
+           (v.location == REGB_HOST || v.location == REGB_DEVICE);
 }
 }  // namespace
 
@@ -459,8 +539,6 @@ regb_status regb_engine_submit(regb_engine* e, const regb_job* job, uint64_t* id
             throw Failure(REGB_ERR_ARG, "null argument");
         if (!vol_ok(job->moving) || (job->template_id < 0 && !vol_ok(job->fixed)))
             throw Failure(REGB_ERR_ARG, "bad fixed/moving volume");
-        if (job->run_linear && (job->moving.dtype != REGB_U8 || (job->template_id < 0 && job->fixed.dtype != REGB_U8)))
-            throw Failure(REGB_ERR_ARG, "the affine stage takes uint8 volumes");
         *id = e->e->submit(*job);
         return REGB_OK;
     });

@@ -110,6 +110,14 @@ int cdm_blocks_for(long long nvox);
 // out[i] = segs[i].ctl->done
 cudaError_t launch_cdm_status(const CdmSeg* segs, int nseg, int* out, cudaStream_t st);
 
+// normalize_upper_lower2 to uint8 of a U8 / F32 / U16 / BF16 volume (dtype codes of
+// regb_dtype); mm is 2 words of device scratch; out is untouched when max == min
+// (then mm[0] == mm[1] afterwards).
+cudaError_t launch_normalize_to_u8(const void* in, int dtype, long long n, float upper, uint8_t* out, unsigned* mm,
+                                   cudaStream_t st);
+// Exact widening of a U8 / F32 / U16 / BF16 volume to float.
+cudaError_t launch_widen_to_f32(const void* in, int dtype, long long n, float* out, cudaStream_t st);
+
 // Voxels > 0 per (x, y), (x, z), (y, z) line of a uint8 volume (zeroes the tables first).
 cudaError_t launch_mask_counts(const uint8_t* v, Dim3 dim, uint32_t* xy, uint32_t* xz, uint32_t* yz,
                                cudaStream_t st);
