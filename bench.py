@@ -35,6 +35,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from tipl_b200 import replicas  # noqa: E402  (loads no library)
+
 SHAPE = (182, 218, 182)  # numpy (z, y, x) = 182 x 218 x 182 voxels
 VS = (1.0, 1.0, 1.0)
 METRIC = "registrations/s (affine 12-DOF MI, 182x218x182 uint8, 1 mm)"
@@ -46,8 +48,7 @@ MI_DRAM_BYTES_PER_VOXEL_EVAL = 17.613568e6 / (12 * 7221032)
 
 
 def env_rank():
-    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
-            int(os.environ.get("WORLD_SIZE", "1")))
+    return replicas.env_rank()
 
 
 def make_pair(job: int):
@@ -196,6 +197,87 @@ def cdm_case(args):
     L.regb_stats_get(st)
     print(json.dumps({"kernel_case": "cdm", "ok": bool(ok), "ms": a.elapsed_time(b), "launches": st.launches,
                       "field_rms": float(field.float().pow(2).sum(-1).sqrt().mean())}))
+    return 0
+
+
+def precision_report(args):
+    """The mixed-precision workload: a 182x218x182 template and a subject (random affine,
+    smooth displacement up to 4 voxels, 2% Rician-like noise) stored as uint16 and as
+    BF16, registered by one served job each (affine MI on the device-quantised uint8
+    volumes, then 3-level CDM in FP32 on the widened volumes).  Reports, per storage
+    type, the job's device time, the final MI against the FP64 restatement at the same
+    parameters, whether the joint-histogram counts equal the FP32 restatement's, and the
+    displacement-field RMS error against the FP64 CDM of the oracle on the same inputs."""
+    import time
+
+    import torch
+
+    import oracle
+    import tipl_b200 as tb
+    from tipl_b200 import phantom as ph
+
+    orc = oracle.Oracle()
+    rng = np.random.default_rng(ph.seed_for(4, 100))
+    t = ph.class_phantom(SHAPE, rng)
+    p_true = ph.random_affine(rng)
+    Tm = tb.affine_to_matrix(p_true, SHAPE, VS, SHAPE, VS)
+    m = tb.resample(torch.from_numpy(t).cuda(), SHAPE, Tm, allow_shift_copy=False).cpu().numpy()
+    m = ph.rician(ph.warp(m, ph.smooth_field(SHAPE, rng, 6.0, 4.0)), rng)
+    cdm_p = tb.reg.cdm_param(min_dimension=32)
+    out = {"report": "precision", "workload": "affine MI + 3-level CDM (levels 23/46/91 iterate), 182x218x182, 1 mm",
+           "data": "synthetic", "storage": {}}
+    for kind in ("u16", "bf16"):
+        if kind == "u16":
+            ts, ms = (np.round(np.clip(x, 0, 4095)).astype(np.uint16) for x in (t, m))
+            tw, mw = ts.astype(np.float32), ms.astype(np.float32)
+        else:
+            ts, ms = tb.to_bf16(t), tb.to_bf16(m)
+            tw, mw = tb.from_bf16(ts), tb.from_bf16(ms)
+        field = torch.zeros(SHAPE + (3,), dtype=torch.float32, device="cuda")
+        with tb.Engine() as eng:
+            tid = eng.add_template(ts)
+            eng.wait(eng.submit(ms, template=tid, cdm=True, cdm_param=cdm_p, field_out=field))  # warm-up
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            r = eng.wait(eng.submit(ms, template=tid, cdm=True, cdm_param=cdm_p, field_out=field))
+            b.record()
+            torch.cuda.synchronize()
+        ms_job = a.elapsed_time(b)
+        q_t, _ = tb.normalize_to_u8(ts)
+        q_m, _ = tb.normalize_to_u8(ms)
+        arg = r["arg"]
+        T = tb.affine_to_matrix(arg, SHAPE, VS, SHAPE, VS)
+        T64 = orc.affine_to_matrix_f64(arg.astype(np.float64), SHAPE, VS, SHAPE, VS)
+        mi32, hist = tb.mi_cost(q_t, q_m, T[None], return_hist=True)
+        t0 = time.time()
+        mi64 = orc.mi_cost_f64(q_t, q_m, T64)
+        hist_exact = bool(np.array_equal(hist[0], orc.mi_hist(q_t, q_m, T)))
+        # FP64 nonlinear stage on the same inputs: the widened subject resampled in double
+        Is64 = np.zeros(SHAPE, np.float64)
+        orc.lib.orc_resample_f64(oracle._ptr(mw.astype(np.float64)), oracle._ptr(oracle._dims(SHAPE)),
+                                 oracle._ptr(Is64), oracle._ptr(oracle._dims(SHAPE)), oracle._ptr(T), 1)
+        d64, ok64, it64 = orc.cdm(tw.astype(np.float64), Is64, min_dimension=32)
+        d32 = field.cpu().numpy().astype(np.float64)
+        err = np.sqrt(((d32 - d64) ** 2).sum(-1))
+
+        def warped_corr(d):
+            # Pearson r (double) between the template and the subject warped by field d
+            w = np.zeros(SHAPE, np.float64)
+            orc.lib.orc_compose_f64(oracle._ptr(Is64), oracle._ptr(oracle._dims(SHAPE)),
+                                    oracle._ptr(np.ascontiguousarray(d, np.float64)), oracle._ptr(w))
+            return float(np.corrcoef(tw.astype(np.float64).ravel(), w.ravel())[0, 1])
+        out["storage"][kind] = {
+            "job_ms": ms_job, "linear_cost": r["linear_cost"], "cdm_ok": bool(r["cdm_ok"]),
+            "cdm_iterations": r["cdm_iterations"], "mi_fp32": float(mi32[0]), "mi_fp64": float(mi64),
+            "mi_rel_err": abs(float(mi32[0]) - mi64) / abs(mi64), "hist_counts_bit_exact": hist_exact,
+            "field_rms_err_vox": float(np.sqrt((err ** 2).mean())), "field_max_err_vox": float(err.max()),
+            "field_rms_vox": float(np.sqrt((d64 ** 2).sum(-1).mean())), "fp64_cdm_ok": bool(ok64),
+            "fp64_cdm_iterations": it64, "warped_corr_fp32": warped_corr(d32), "warped_corr_fp64": warped_corr(d64),
+            "warped_corr_none": warped_corr(np.zeros_like(d64)),
+            "oracle_s": time.time() - t0}
+    print(json.dumps(out))
     return 0
 
 
@@ -348,7 +430,11 @@ def main():
     ap.add_argument("--kernel-case", choices=["mi", "corr", "cdm"], default=None,
                     help="run only K-candidate cost batches of the full-size pair (for profiler captures)")
     ap.add_argument("--k", type=int, default=12)
+    ap.add_argument("--precision-report", action="store_true",
+                    help="uint16 / BF16 storage: errors of the FP32 path against the FP64 oracle (config 4)")
     args = ap.parse_args()
+    if args.precision_report:
+        return precision_report(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.kernel_case == "cdm":
@@ -417,15 +503,8 @@ def main():
     clocks = clk.stop()
     t_e2e, _, _, _ = timed(f8, m8, False)  # host numpy buffers: the library copies them in each step
 
-    def maxall(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    t_dev = maxall(t_dev)
-    t_e2e = maxall(t_e2e)
+    t_dev = replicas.max_over_ranks(t_dev, dist)
+    t_e2e = replicas.max_over_ranks(t_e2e, dist)
     regs = args.steps * world
     value = regs / t_dev
     e2e = regs / t_e2e
@@ -467,16 +546,12 @@ def main():
 
 def served_line(args, rank, world, dist, torch):
     t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects, plain = run_served(args, rank, world, dist)
+    lat = replicas.gather_lists(lat, dist)  # every rank's per-job latencies
+    costs = replicas.gather_lists(costs, dist)
+    evals = replicas.sum_over_ranks(evals, dist)
 
-    def maxall(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    t_dev = maxall(t_dev)
-    t_e2e = maxall(t_e2e)
+    t_dev = replicas.max_over_ranks(t_dev, dist)
+    t_e2e = replicas.max_over_ranks(t_e2e, dist)
     regs = args.steps * args.batch * world
     hbm, hbm_kind = peaks()
     achieved = (st.mi_bytes / st.mi_launches) / (st.mi_ms / st.mi_launches / 1000.0) / 1e9 if st.mi_launches else 0

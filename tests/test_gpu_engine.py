@@ -92,3 +92,71 @@ def test_budget_admission_and_cancel(data):
         ra = eng.wait(a)
         assert rb["status"] == _lib.REGB_CANCELLED
         assert ra["status"] == 0
+
+
+def _plain_mixed(tmpl, mov):
+    """The plain calls a served job of any storage type stands for: the affine search on
+    the device-quantised uint8 volumes, then CDM on uint8 (both uint8) or in float on
+    the widened volumes."""
+    q = lambda v: v if v.dtype == np.uint8 and not isinstance(v, tb.BF16) else tb.normalize_to_u8(v)[0]
+    cost, arg, evals = tb.reg.linear(q(tmpl), (1, 1, 1), q(mov), (1, 1, 1))
+    T = tb.affine_to_matrix(arg, tmpl.shape, (1, 1, 1), mov.shape, (1, 1, 1))
+    both_u8 = all(v.dtype == np.uint8 and not isinstance(v, tb.BF16) for v in (tmpl, mov))
+    if both_u8:
+        field, ok = tb.reg.cdm(tmpl, tb.resample(mov, tmpl.shape, T, allow_shift_copy=True))
+    else:
+        w = lambda v: v if v.dtype == np.float32 and not isinstance(v, tb.BF16) else tb.widen_to_f32(v)
+        field, ok = tb.reg.cdm(w(tmpl), tb.resample(w(mov), tmpl.shape, T, allow_shift_copy=True))
+    return cost, arg, evals, field, ok
+
+
+def test_poisson_arrivals_templates_and_storage_types():
+    """Jobs arriving at random (Poisson) times against three resident templates of
+    different shapes and storage types, subjects of random shape stored as uint8,
+    uint16, float32 or BF16, affine then CDM, under a budget that makes some queue:
+    every result equals the plain single-job calls."""
+    import threading
+    import time
+
+    rng = np.random.default_rng(ph.seed_for(5, 7))
+    store = {
+        "u8": lambda a: ph.normalize_to_u8(a),
+        "u16": lambda a: np.round(np.clip(a, 0, 4095)).astype(np.uint16),
+        "f32": lambda a: a.astype(np.float32),
+        "bf16": lambda a: tb.to_bf16(a),
+    }
+    tshapes = [((26, 30, 24), "u8"), ((36, 40, 34), "u16"), ((32, 32, 32), "f32")]
+    templates = [(store[k](ph.class_phantom(s, rng)), k) for s, k in tshapes]
+    jobs = []
+    for k in range(10):
+        ti = int(rng.integers(0, len(templates)))
+        s = tuple(int(v) for v in rng.integers(24, 44, 3))
+        base = ph.class_phantom(s, rng)
+        p = ph.random_affine(rng, rot_deg=6, trans_vox=2)
+        T = ph.affine_matrix_f32(p, s, (1, 1, 1), s, (1, 1, 1))
+        kind = ["u8", "u16", "f32", "bf16"][k % 4]
+        jobs.append((ti, store[kind](ph.rician(ph.apply_matrix(base, T, s), rng))))
+    want = [_plain_mixed(templates[ti][0], m) for ti, m in jobs]
+    arrivals = np.cumsum(rng.exponential(1.0 / 200.0, len(jobs)))
+    fields = [np.zeros(templates[ti][0].shape + (3,), np.float32) for ti, _ in jobs]
+    ids = [None] * len(jobs)
+    with tb.Engine(hbm_budget_bytes=24 << 20, max_active=4) as eng:
+        tids = [eng.add_template(t) for t, _ in templates]
+
+        def feed():
+            t0 = time.perf_counter()
+            for k, (ti, m) in enumerate(jobs):
+                dt = arrivals[k] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                ids[k] = eng.submit(m, template=tids[ti], cdm=True, field_out=fields[k])
+
+        th = threading.Thread(target=feed)
+        th.start()
+        th.join()
+        res = [eng.wait(i) for i in ids]
+    for r, (cost, arg, evals, field, ok), f in zip(res, want, fields):
+        assert r["status"] == 0
+        assert r["linear_cost"] == np.float32(cost) and np.array_equal(r["arg"].view(np.uint32), arg.view(np.uint32))
+        assert r["cdm_ok"] == ok
+        assert np.array_equal(f.view(np.uint32), field.view(np.uint32))
