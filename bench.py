@@ -135,6 +135,54 @@ def cpu_baseline_linear(fixed, moving, threads: int):
     return dt, cost, arg
 
 
+def ref_gpu_sample(args):
+    """Child process: the reference's own CUDA path (oracle/_ref/libtipl_ref_gpu.so) on the
+    volumes in args.ref_gpu_sample -- one warm-up and one timed call -- printed as JSON.
+    It runs in its own process so that the product's measurements cannot be disturbed."""
+    import oracle
+
+    z = np.load(args.ref_gpu_sample)
+    G = oracle.ReferenceGPU()
+    G.set_threads(os.cpu_count() or 1)
+    out = {}
+    if "fixed" in z:
+        G.linear(z["fixed"], VS, z["moving"], VS)
+        t0 = time.perf_counter()
+        cost, _ = G.linear(z["fixed"], VS, z["moving"], VS)
+        out["linear_s"], out["linear_cost"] = time.perf_counter() - t0, cost
+    if "It" in z:
+        md = int(z["min_dimension"])
+        G.cdm(z["It"], z["Is"], min_dimension=md)
+        t0 = time.perf_counter()
+        d, ok = G.cdm(z["It"], z["Is"], min_dimension=md)
+        out["cdm_s"], out["cdm_ok"] = time.perf_counter() - t0, ok
+        out["cdm_field_rms"] = float(np.sqrt((d.astype(np.float64) ** 2).sum(-1)).mean())
+    print(json.dumps(out))
+    return 0
+
+
+def reference_gpu(**arrays):
+    """Times the reference's CUDA path in a child process; None when it was not built or failed."""
+    import subprocess
+    import tempfile
+
+    import oracle
+
+    if not os.path.exists(oracle.REF_GPU_SO):
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "sample.npz")
+        np.savez(path, **arrays)
+        try:
+            r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-gpu-sample", path],
+                               capture_output=True, text=True, timeout=600)
+        except subprocess.TimeoutExpired:
+            return None
+        if r.returncode != 0 or not r.stdout.strip():
+            return None
+        return json.loads(r.stdout.strip().splitlines()[-1])
+
+
 def run_reference(args):
     rank, local, world = env_rank()
     if rank != 0:
@@ -195,8 +243,14 @@ def cdm_case(args):
     torch.cuda.synchronize()
     st = _lib.Stats()
     L.regb_stats_get(st)
-    print(json.dumps({"kernel_case": "cdm", "ok": bool(ok), "ms": a.elapsed_time(b), "launches": st.launches,
-                      "field_rms": float(field.float().pow(2).sum(-1).sqrt().mean())}))
+    line = {"kernel_case": "cdm", "ok": bool(ok), "ms": a.elapsed_time(b), "launches": st.launches,
+            "field_rms": float(field.float().pow(2).sum(-1).sqrt().mean())}
+    if args.steps > 1:
+        g = reference_gpu(It=It.cpu().numpy(), Is=Is.cpu().numpy(), min_dimension=np.int64(32))
+        if g:
+            line["reference_gpu_ms"] = 1000.0 * g["cdm_s"]
+            line["reference_gpu_field_rms"] = g["cdm_field_rms"]
+    print(json.dumps(line))
     return 0
 
 
@@ -432,7 +486,10 @@ def main():
     ap.add_argument("--k", type=int, default=12)
     ap.add_argument("--precision-report", action="store_true",
                     help="uint16 / BF16 storage: errors of the FP32 path against the FP64 oracle (config 4)")
+    ap.add_argument("--ref-gpu-sample", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.ref_gpu_sample:
+        return ref_gpu_sample(args)
     if args.precision_report:
         return precision_report(args)
     if args.impl == "reference":
@@ -563,6 +620,13 @@ def served_line(args, rank, world, dist, torch):
             cpu = {"value": 1.0 / r[0], "unit": "registrations/s", "cores": threads, "kind": "reference",
                    "sample": "one full tipl::reg::linear (MI) registration of the first subject (oracle/_ref)",
                    "final_cost": r[1]}
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        g = reference_gpu(fixed=f8, moving=subjects[0])
+        if g:
+            ref_gpu = {"value": 1.0 / g["linear_s"], "unit": "registrations/s", "final_cost": g["linear_cost"],
+                       "kind": "the reference's own CUDA path (tipl::reg::linear, cuda = true) built for sm_100a",
+                       "sample": "one registration of the first subject from host buffers, wall clock"}
     if rank == 0:
         lat_s = sorted(lat)
 
@@ -592,6 +656,7 @@ def served_line(args, rank, world, dist, torch):
                              "launches": st.mi_launches, "avg_launch_ms": st.mi_ms / max(1, st.mi_launches),
                              "bytes_per_launch": st.mi_bytes / max(1, st.mi_launches)},
                 "cpu_baseline": cpu,
+                "reference_gpu": ref_gpu,
                 "e2e": {"value": regs / t_e2e, "unit": "registrations/s",
                         "h2d_bytes_per_step": int(sum(m.nbytes for m in subjects)),
                         "d2h_bytes_per_step": 56 * args.batch},

@@ -4,6 +4,8 @@
   hot path (oracle/oracle.c + oracle_core.h/oracle_field.h/oracle_cdm.h).
 * ``Reference`` -- oracle/_ref/libtipl_ref.so, the reference's own header-only C++
   compiled from its sources by oracle/Makefile (present only where it was built).
+* ``ReferenceGPU`` -- oracle/_ref/libtipl_ref_gpu.so, the reference's own CUDA path
+  (nvcc, sm_100a), timed by bench.py as a secondary figure.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this
 package; the product path (tipl_b200) never does.
@@ -19,6 +21,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libtipl_ref.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libtipl_ref_gpu.so")
 DEFAULT_REF_ROOT = "/root/reference"
 
 
@@ -27,7 +30,7 @@ def build(ref_root: str | None = None, with_ref: bool = True) -> None:
     subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
     root = ref_root or os.environ.get("TIPL_REF_ROOT", DEFAULT_REF_ROOT)
     if with_ref and os.path.isdir(os.path.join(root, "reg")):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_ROOT={root}"])
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", "refgpu", f"REF_ROOT={root}"])
 
 
 _P = C.c_void_p
@@ -405,3 +408,31 @@ class Reference(_Lib):
         out = np.zeros(img.shape, np.uint8)
         self.lib.tiplref_normalize_to_u8(_ptr(_f32(img)), _ptr(_dims(img.shape)), _ptr(out), upper)
         return out
+
+
+class ReferenceGPU(_Lib):
+    """The reference's own CUDA path (tipl::reg::linear / cdm_common with cuda = true)."""
+
+    _pfx = "tiplrefgpu_"
+
+    def __init__(self, path: str = REF_GPU_SO):
+        super().__init__(path)
+        L = self.lib
+        L.tiplrefgpu_linear.restype = C.c_float
+        L.tiplrefgpu_cdm.argtypes = [_P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_uint]
+
+    def set_threads(self, n: int) -> None:
+        self.lib.tiplrefgpu_set_threads(int(n))
+
+    def linear(self, fixed, fixed_vs, moving, moving_vs, arg=None, reg_type=15, cost_type=1):
+        a = np.array([0, 0, 0, 0, 0, 0, 1, 1, 1, 0, 0, 0], np.float32) if arg is None else _f32(arg).copy()
+        c = self.lib.tiplrefgpu_linear(_ptr(_u8(fixed)), _ptr(_dims(fixed.shape)), _ptr(_f32(fixed_vs)),
+                                       _ptr(_u8(moving)), _ptr(_dims(moving.shape)), _ptr(_f32(moving_vs)), _ptr(a),
+                                       int(reg_type), int(cost_type))
+        return float(c), a
+
+    def cdm(self, It, Is, resolution=2.0, speed=0.3, smoothing=0.05, min_dimension=16):
+        d = np.zeros(It.shape + (3,), np.float32)
+        ok = self.lib.tiplrefgpu_cdm(_ptr(_u8(It)), _ptr(_u8(Is)), _ptr(_dims(It.shape)), _ptr(d), resolution, speed,
+                                     smoothing, min_dimension)
+        return d, bool(ok)
