@@ -65,6 +65,39 @@ class _Lib:
     def _fn(self, name):
         return getattr(self.lib, self._pfx + name)
 
+    # -- subject preprocessing of the mm_reg pipeline (reg/mm_reg.hpp:14-20)
+    def gaussian(self, img, bandwidth=1):
+        out = np.ascontiguousarray(img, np.float32).copy()
+        self._fn("gaussian" if self._pfx == "tiplref_" else "gaussian_f32")(_ptr(out), _ptr(_dims(out.shape)),
+                                                                           C.c_int(bandwidth))
+        return out
+
+    def subject_image_pre(self, img):
+        out = np.zeros(img.shape, np.uint8)
+        self._fn("subject_image_pre" if self._pfx == "tiplref_" else "subject_image_pre_f32")(
+            _ptr(np.ascontiguousarray(img, np.float32)), _ptr(_dims(img.shape)), _ptr(out))
+        return out
+
+    def otsu_threshold(self, img):
+        a = np.ascontiguousarray(img, np.float32)
+        if self._pfx == "tiplref_":
+            f = self.lib.tiplref_otsu_threshold
+            f.restype = C.c_float
+            return f(_ptr(a), _ptr(_dims(a.shape)))
+        f = self.lib.orc_otsu_threshold_f32
+        f.restype = C.c_float
+        return f(_ptr(a), C.c_longlong(a.size))
+
+    def otsu_median(self, img):
+        a = np.ascontiguousarray(img, np.float32)
+        if self._pfx == "tiplref_":
+            f = self.lib.tiplref_otsu_median
+            f.restype = C.c_float
+            return f(_ptr(a), _ptr(_dims(a.shape)))
+        f = self.lib.orc_otsu_median_f32
+        f.restype = C.c_float
+        return f(_ptr(a), C.c_longlong(a.size))
+
     # -- mask-moment initialisation of linear() (reg/linear.hpp:658-684)
     def has_mask(self, img) -> bool:
         return bool(self._fn("has_mask" if self._pfx == "tiplref_" else "has_mask_u8")(_ptr(_u8(img)),

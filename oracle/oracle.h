@@ -67,6 +67,12 @@ int orc_cdm_level_f64(const double* It, const double* Is, const int* dim, double
 
 int orc_normalize_to_u8_f32(const float* in, long long n, uint8_t* out, float upper);
 int orc_normalize_to_u8_u16(const uint16_t* in, long long n, uint8_t* out, float upper);
+void orc_gaussian_f32(float* img, const int* dim, int bandwidth);
+float orc_otsu_threshold_f32(const float* img, long long n);
+float orc_median_f32(const float* v, long long n);
+float orc_otsu_median_f32(const float* img, long long n);
+void orc_normalize_otsu_median_f32(float* img, long long n, float upper);
+void orc_subject_image_pre_f32(const float* in, const int* dim, uint8_t* out);
 int orc_has_mask_u8(const uint8_t* img, const int* dim);
 void orc_eigen_sym3(const double* A, double* V, double* d);
 void orc_estimate_affine_param_u8(const uint8_t* src, const int* sdim, const float* svs, const uint8_t* tgt,

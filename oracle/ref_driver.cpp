@@ -13,6 +13,7 @@
 #include <cstdint>
 #include "reg/linear.hpp"
 #include "reg/cdm.hpp"
+#include "reg/mm_reg.hpp"
 
 namespace {
 using u8 = unsigned char;
@@ -300,6 +301,31 @@ void tiplref_normalize_to_u8(const float* in, const int* dim, u8* out, float upp
     tipl::normalize_upper_lower2(cview(in, dim), o, upper);
     if (o.size() == size_t(dim[0]) * dim[1] * dim[2])
         std::copy(o.begin(), o.end(), out);
+}
+
+// filter::gaussian(I, bandwidth) on a float image (filter/gaussian.hpp:84-96), in place
+void tiplref_gaussian(float* img, const int* dim, int bandwidth)
+{
+    tipl::image<3> I(img, shp(dim));
+    tipl::filter::gaussian(I, (unsigned int)bandwidth);
+    std::copy(I.begin(), I.end(), img);
+}
+
+// segmentation::otsu_threshold / otsu_median (numerical/otsu.hpp:59-100)
+float tiplref_otsu_threshold(const float* img, const int* dim)
+{
+    return tipl::segmentation::otsu_threshold(tipl::image<3>(img, shp(dim)));
+}
+float tiplref_otsu_median(const float* img, const int* dim)
+{
+    return tipl::segmentation::otsu_median(tipl::image<3>(img, shp(dim)));
+}
+
+// reg::subject_image_pre (reg/mm_reg.hpp:14-20): float image -> uint8
+void tiplref_subject_image_pre(const float* img, const int* dim, u8* out)
+{
+    auto o = tipl::reg::subject_image_pre(tipl::image<3>(img, shp(dim)));
+    std::copy(o.begin(), o.end(), out);
 }
 
 // normalize_upper_lower2 of a uint16 volume (numerical/numerical.hpp:909-927)

@@ -42,6 +42,25 @@ def main():
         mask_init(R)
     if args.only in (None, "precision"):
         precision(R)
+    if args.only in (None, "preprocess"):
+        preprocess(R)
+
+
+def preprocess(R):
+    """subject_image_pre of the mm_reg pipeline (gaussian, Otsu median, uint8) and its parts."""
+    rng = np.random.default_rng(ph.seed_for(4, 11))
+    out = {}
+    # shapes: one under the median's 2048-value chunking threshold above Otsu, the rest over
+    for k, shp in enumerate([(9, 11, 13), (30, 34, 28), (41, 37, 45), (1, 20, 24)]):
+        t = ph.rician(ph.class_phantom(shp, rng), rng) if shp[0] > 1 else rng.random(shp).astype(np.float32) * 90
+        g = R.gaussian(t)
+        out[f"c{k}_in"] = t
+        out[f"c{k}_gauss"] = g
+        out[f"c{k}_gauss2"] = R.gaussian(t, 2)
+        out[f"c{k}_otsu"] = np.float32(R.otsu_threshold(g))
+        out[f"c{k}_median"] = np.float32(R.otsu_median(g))
+        out[f"c{k}_pre"] = R.subject_image_pre(t)
+    save("preprocess", **out)
 
 
 def precision(R):
