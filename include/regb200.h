@@ -133,6 +133,18 @@ regb_status regb_normalize_to_u8(const regb_volume* in, regb_volume* out, float 
  * float); the FP32 nonlinear path runs on volumes stored this way. */
 regb_status regb_widen_to_f32(const regb_volume* in, regb_volume* out, void* stream);
 
+/* ---- subject preprocessing of the mm_reg pipeline (reg/mm_reg.hpp:14-20) ----------- */
+/* filter::gaussian(I, bandwidth) (filter/gaussian.hpp:18-96) of an F32 volume: bandwidth
+ * rounds of the separable [1 2 1] x, y, z passes with the edge sample repeated, then the
+ * scale 2^-(6 * bandwidth).  in and out are distinct F32 volumes of one shape. */
+regb_status regb_gaussian(const regb_volume* in, regb_volume* out, int bandwidth, void* stream);
+/* reg::subject_image_pre (reg/mm_reg.hpp:14-20): gaussian (bandwidth 1), then
+ * segmentation::normalize_otsu_median(I, 255.99) (numerical/otsu.hpp:110-136), then the
+ * float -> uint8 conversion.  in: F32, or U8 / U16 / BF16 widened exactly to float
+ * first; out: U8 of the same shape.  Synchronises the stream (the Otsu threshold and
+ * median are decided on the host). */
+regb_status regb_subject_image_pre(const regb_volume* in, regb_volume* out, void* stream);
+
 /* ---- mask-moment initialisation of linear() (reg/linear.hpp:658-684) --------------- */
 /* has_mask(img) (numerical/basic_op.hpp:811-830) of a uint8 volume: *out = 1 when more
  * than a fifth of its voxels are 0 or its non-zero voxels' bounding box lies inside the

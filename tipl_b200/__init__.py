@@ -191,6 +191,27 @@ def widen_to_f32(img, out=None, stream=None):
     return out
 
 
+def gaussian(img, bandwidth=1, out=None, stream=None):
+    """filter::gaussian of a float32 volume (separable [1 2 1], bandwidth rounds)."""
+    if out is None:
+        out = _like(img, img.shape)
+    _lib.check(_lib.lib().regb_gaussian(C.byref(_vol(img)), C.byref(_vol(out)), int(bandwidth), _stream(stream)))
+    return out
+
+
+def subject_image_pre(img, out=None, stream=None):
+    """reg::subject_image_pre: gaussian, Otsu-median normalisation to [0, 255.99], uint8."""
+    if out is None:
+        if _is_dev(img):
+            import torch
+
+            out = torch.zeros(tuple(img.shape), dtype=torch.uint8, device=img.device)
+        else:
+            out = np.zeros(img.shape, np.uint8)
+    _lib.check(_lib.lib().regb_subject_image_pre(C.byref(_vol(img)), C.byref(_vol(out)), _stream(stream)))
+    return out
+
+
 def has_mask(img) -> bool:
     """tipl::has_mask of a uint8 volume (numpy or device tensor)."""
     out = C.c_int(0)

@@ -105,6 +105,8 @@ _SIGS = {
     "regb_has_mask": (C.c_int, [C.c_void_p, C.c_void_p]),
     "regb_normalize_to_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p]),
     "regb_widen_to_f32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "regb_gaussian": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "regb_subject_image_pre": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "regb_estimate_affine_param": (C.c_int, [C.c_void_p] * 5),
     "regb_resample": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p]),
     "regb_mi_cost": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p,

@@ -8,6 +8,7 @@
 #include "cdm_level.h"
 #include "host.h"
 #include "mask_init.h"
+#include "preprocess.h"
 #include "stats.h"
 
 namespace regb {
@@ -265,6 +266,60 @@ regb_status regb_widen_to_f32(const regb_volume* in, regb_volume* out, void* str
         b.out(out->ptr, st);
         if (!dev || !stream)
             REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_gaussian(const regb_volume* in, regb_volume* out, int bandwidth, void* stream)
+{
+    return guarded([&] {
+        check_vol(in, "in");
+        check_vol(out, "out");
+        if (in->dtype != REGB_F32 || out->dtype != REGB_F32 || !same_dims(in->dim, out->dim) || bandwidth < 0 ||
+            bandwidth > 64)
+            throw Failure(REGB_ERR_ARG, "gaussian: F32 in and out of one shape, bandwidth 0..64");
+        if (in->ptr == out->ptr)
+            throw Failure(REGB_ERR_ARG, "gaussian: in and out must be distinct");
+        const bool dev = in->location == REGB_DEVICE && out->location == REGB_DEVICE;
+        Stream own;
+        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : own.s;
+        const size_t n = nvox(in->dim);
+        Staged a, b;
+        a.in(in->ptr, n * 4, in->location, st, true);
+        b.in(out->ptr, n * 4, out->location, st, false);
+        gaussian((const float*)a.d, in->dim, bandwidth, (float*)b.d, st);
+        b.out(out->ptr, st);
+        if (!dev || !stream)
+            REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_subject_image_pre(const regb_volume* in, regb_volume* out, void* stream)
+{
+    return guarded([&] {
+        check_vol(in, "in", false);
+        check_vol(out, "out");
+        if (!pix_size(in->dtype) || out->dtype != REGB_U8 || !same_dims(in->dim, out->dim))
+            throw Failure(REGB_ERR_ARG, "subject_image_pre: in U8/F32/U16/BF16, out U8 of the same shape");
+        const bool dev = in->location == REGB_DEVICE && out->location == REGB_DEVICE;
+        Stream own;
+        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : own.s;
+        const size_t n = nvox(in->dim);
+        Staged a, b;
+        a.in(in->ptr, n * pix_size(in->dtype), in->location, st, true);
+        b.in(out->ptr, n, out->location, st, false);
+        DevBuf<float> wide;
+        const float* f = (const float*)a.d;
+        if (in->dtype != REGB_F32) {
+            wide.alloc(n, st);
+            REGB_CK(launch_widen_to_f32(a.d, in->dtype, (long long)n, wide.p, st));
+            count_launch();
+            f = wide.p;
+        }
+        subject_image_pre(f, in->dim, (uint8_t*)b.d, st);
+        b.out(out->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
         return REGB_OK;
     });
 }

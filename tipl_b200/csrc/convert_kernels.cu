@@ -121,6 +121,24 @@ cudaError_t launch_normalize_to_u8(const void* in, int dtype, long long n, float
     return cudaGetLastError();
 }
 
+cudaError_t launch_minmax(const void* in, int dtype, long long n, unsigned* mm, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(mm, 0xff, sizeof(unsigned), st);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(mm + 1, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess)
+        return e;
+    const int g = grid_for(n);
+    switch (dtype) {
+    case 0: minmax_kernel<0><<<g, kThreads, 0, st>>>(in, n, mm); break;
+    case 1: minmax_kernel<1><<<g, kThreads, 0, st>>>(in, n, mm); break;
+    case 2: minmax_kernel<2><<<g, kThreads, 0, st>>>(in, n, mm); break;
+    case 3: minmax_kernel<3><<<g, kThreads, 0, st>>>(in, n, mm); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_widen_to_f32(const void* in, int dtype, long long n, float* out, cudaStream_t st)
 {
     const int g = grid_for(n);

@@ -115,8 +115,29 @@ cudaError_t launch_cdm_status(const CdmSeg* segs, int nseg, int* out, cudaStream
 // (then mm[0] == mm[1] afterwards).
 cudaError_t launch_normalize_to_u8(const void* in, int dtype, long long n, float upper, uint8_t* out, unsigned* mm,
                                    cudaStream_t st);
+// Exact min / max of a U8 / F32 / U16 / BF16 volume as order-preserving float keys:
+// mm[0] = key(min), mm[1] = key(max), key(f) = f >= 0 ? bits | 2^31 : ~bits.
+cudaError_t launch_minmax(const void* in, int dtype, long long n, unsigned* mm, cudaStream_t st);
 // Exact widening of a U8 / F32 / U16 / BF16 volume to float.
 cudaError_t launch_widen_to_f32(const void* in, int dtype, long long n, float* out, cudaStream_t st);
+
+// Subject preprocessing (preprocess_kernels.cu).  One round of the separable [1 2 1]
+// Gaussian (x, y, z passes), optionally times scale.
+cudaError_t launch_gaussian_round(const float* in, float* out, int w, int h, int d, float scale, int apply_scale,
+                                  cudaStream_t st);
+// 256-bin histogram of floor((v - mn) * range), clamped to [0, 255] (zeroes hist first).
+cudaError_t launch_otsu_hist(const float* v, long long n, float mn, float range, unsigned* hist, cudaStream_t st);
+// The values > ot in voxel order into out; counts holds compact_tiles(n) + 1 words and
+// receives the total in its last word.
+long long compact_tiles(long long n);
+cudaError_t launch_compact_above(const float* v, long long n, float ot, unsigned* counts, float* out, cudaStream_t st);
+// The 256 chunk middles of median() over m >= 2048 values.
+cudaError_t launch_chunk_medians(const float* v, long long m, float* med, cudaStream_t st);
+// count of v * s > 0 (zeroes cnt first)
+cudaError_t launch_positive_count(const float* v, long long n, float s, unsigned long long* cnt, cudaStream_t st);
+// out = uint8(clamp(v * s - (shift ? c : 0), 0, upper))
+cudaError_t launch_otsu_normalize(const float* v, long long n, float s, int shift, float c, float upper, uint8_t* out,
+                                  cudaStream_t st);
 
 // Voxels > 0 per (x, y), (x, z), (y, z) line of a uint8 volume (zeroes the tables first).
 cudaError_t launch_mask_counts(const uint8_t* v, Dim3 dim, uint32_t* xy, uint32_t* xz, uint32_t* yz,
