@@ -292,6 +292,10 @@ typedef struct {
     regb_cdm_param cdm;
     float* field_out;          /* optional: receives the CDM field (template dims x 3 floats) */
     int field_location;        /* REGB_HOST or REGB_DEVICE for field_out */
+    int subject_pre;           /* 0: subject quantised like a template (normalize_upper_lower2,
+                                  255.999) unless already uint8; 1: subject_image_pre (gaussian +
+                                  Otsu-median normalisation, reg/mm_reg.hpp:14-20) -- then the whole
+                                  job runs on uint8 like the mm_reg pipeline */
 } regb_job;
 
 typedef struct {

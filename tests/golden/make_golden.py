@@ -44,6 +44,41 @@ def main():
         precision(R)
     if args.only in (None, "preprocess"):
         preprocess(R)
+    if args.only in (None, "linear_runs"):
+        linear_runs(R)
+
+
+def linear_pairs():
+    """Six seeded 30x34x28 phantom pairs: template, its exact affine resample (masked,
+    even k) or that resample with Rician noise (no mask, odd k)."""
+    R = oracle.Reference()
+    out = []
+    for seed in range(6):
+        rng = np.random.default_rng(3000 + seed)
+        shape = (30, 34, 28)
+        f8 = ph.normalize_to_u8(ph.class_phantom(shape, rng))
+        T = R.affine_to_matrix(ph.random_affine(rng, rot_deg=10, trans_vox=3), shape, (1, 1, 1), shape, (1, 1, 1))
+        m8 = R.resample(f8, shape, T)
+        if seed % 2:
+            m8 = ph.normalize_to_u8(ph.rician(m8.astype(np.float32), rng))
+        out.append((f8, m8))
+    return out
+
+
+def linear_runs(R):
+    """The reference linear() (MI) on each pair, four runs with 1, 4, 8 and 16 threads:
+    its line search and L-BFGS race in two threads, so the runs differ."""
+    pairs = linear_pairs()
+    costs = []
+    for f8, m8 in pairs:
+        row = []
+        for th in (1, 4, 8, 16):
+            R.set_threads(th)
+            row.append(R.linear(f8, (1, 1, 1), m8, (1, 1, 1))[0])
+        costs.append(row)
+    R.set_threads(1)
+    save("linear_runs", fixed=np.array([p[0] for p in pairs]), moving=np.array([p[1] for p in pairs]),
+         costs=np.array(costs, np.float32))
 
 
 def preprocess(R):

@@ -160,3 +160,28 @@ def test_poisson_arrivals_templates_and_storage_types():
         assert r["linear_cost"] == np.float32(cost) and np.array_equal(r["arg"].view(np.uint32), arg.view(np.uint32))
         assert r["cdm_ok"] == ok
         assert np.array_equal(f.view(np.uint32), field.view(np.uint32))
+
+
+def test_mm_reg_pipeline_job_equals_plain():
+    """subject_pre: the mm_reg pipeline (reg/mm_reg.hpp:14-36, 348-416) -- template through
+    template_image_pre (normalize_upper_lower2, 255.999), subject through subject_image_pre
+    (gaussian + Otsu-median normalisation), affine then CDM on uint8 -- equals the plain
+    calls on the same preprocessed volumes."""
+    rng = np.random.default_rng(ph.seed_for(5, 9))
+    t = ph.class_phantom((36, 40, 34), rng)
+    p = ph.random_affine(rng, rot_deg=6, trans_vox=2)
+    s = (34, 42, 32)
+    T = ph.affine_matrix_f32(p, s, (1, 1, 1), s, (1, 1, 1))
+    m = ph.rician(ph.apply_matrix(ph.class_phantom(s, rng), T, s), rng)
+    q_t, _ = tb.normalize_to_u8(t)
+    q_m = tb.subject_image_pre(m)
+    cost, arg, _ = tb.reg.linear(q_t, (1, 1, 1), q_m, (1, 1, 1))
+    Tf = tb.affine_to_matrix(arg, t.shape, (1, 1, 1), m.shape, (1, 1, 1))
+    want, ok = tb.reg.cdm(q_t, tb.resample(q_m, t.shape, Tf, allow_shift_copy=True))
+    field = np.zeros(t.shape + (3,), np.float32)
+    with tb.Engine() as eng:
+        tid = eng.add_template(t)
+        r = eng.wait(eng.submit(m, template=tid, cdm=True, field_out=field, subject_pre=True))
+    assert r["status"] == 0 and r["cdm_ok"] == ok
+    assert r["linear_cost"] == np.float32(cost) and np.array_equal(r["arg"].view(np.uint32), arg.view(np.uint32))
+    assert np.array_equal(field.view(np.uint32), want.view(np.uint32))

@@ -60,32 +60,17 @@ def test_reg_bound_mask_start_within_reference_runs(harness, golden, tmp_path):
     assert c1 <= worst * 1.01, (c1, g["lin_costs"])
 
 
-@pytest.mark.slow
-def test_reg_bound_against_reference_runs(harness, tmp_path):
-    """Six seeded phantom pairs (masked and noisy-background, MI): our final cost against
-    the better of two reference runs -- within 1 % on average and 5 % at worst (the
-    reference's own runs differ by up to 12 % on such pairs)."""
-    import oracle
-    from tipl_b200 import phantom as ph
-
-    try:
-        R = oracle.Reference()
-    except FileNotFoundError:
-        pytest.skip("reference build not present")
-    diffs = []
-    for seed in range(6):
-        rng = np.random.default_rng(3000 + seed)
-        shape = (30, 34, 28)
-        f8 = ph.normalize_to_u8(ph.class_phantom(shape, rng))
-        T = R.affine_to_matrix(ph.random_affine(rng, rot_deg=10, trans_vox=3), shape, (1, 1, 1), shape, (1, 1, 1))
-        m8 = R.resample(f8, shape, T)
-        if seed % 2:
-            m8 = ph.normalize_to_u8(ph.rician(m8.astype(np.float32), rng))
+def test_reg_bound_against_reference_runs(harness, golden, tmp_path):
+    """Six seeded phantom pairs (masked and noisy-background, MI) against four recorded
+    runs of the reference each (tests/golden/linear_runs.npz; the runs differ by up to
+    4 % on these pairs): our final cost within 1 % of the reference median on average
+    and no more than 2 % above the worst run on any pair."""
+    g = golden("linear_runs")
+    diffs, over_worst = [], []
+    for f8, m8, runs in zip(g["fixed"], g["moving"], g["costs"]):
         ours, _ = run(harness, tmp_path, f8, m8, 1, 0)
-        refs = []
-        for th in (1, 8):
-            R.set_threads(th)
-            refs.append(R.linear(f8, (1, 1, 1), m8, (1, 1, 1))[0])
-        diffs.append((float(ours) - min(refs)) / abs(min(refs)))
-    diffs = np.array(diffs)
-    assert diffs.mean() <= 0.01 and diffs.max() <= 0.05, diffs
+        med = float(np.median(runs))
+        diffs.append((float(ours) - med) / abs(med))
+        over_worst.append((float(ours) - float(runs.max())) / abs(float(runs.max())))
+    diffs, over_worst = np.array(diffs), np.array(over_worst)
+    assert diffs.mean() <= 0.01 and over_worst.max() <= 0.02, (diffs, over_worst)

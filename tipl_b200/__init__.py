@@ -398,7 +398,7 @@ class Engine:
 
     def submit(self, moving, moving_vs=(1.0, 1.0, 1.0), template=None, fixed=None, fixed_vs=(1.0, 1.0, 1.0),
                linear=True, linear_param: LinearParam | None = None, arg=None, cdm=False,
-               cdm_param: CdmParam | None = None, field_out=None) -> int:
+               cdm_param: CdmParam | None = None, field_out=None, subject_pre=False) -> int:
         L = _lib.lib()
         j = _lib.Job()
         L.regb_job_default(C.byref(j))
@@ -418,6 +418,7 @@ class Engine:
         if arg is not None:
             j.arg[:] = [float(v) for v in arg]
         j.run_cdm = int(bool(cdm))
+        j.subject_pre = int(bool(subject_pre))
         if cdm_param is not None:
             j.cdm = cdm_param
         if field_out is not None:

@@ -64,7 +64,7 @@ class Job(C.Structure):
     _fields_ = [("template_id", C.c_int), ("fixed", Volume), ("fixed_vs", C.c_float * 3), ("moving", Volume),
                 ("moving_vs", C.c_float * 3), ("run_linear", C.c_int), ("linear", LinearParam),
                 ("arg", C.c_float * 12), ("run_cdm", C.c_int), ("cdm", CdmParam), ("field_out", C.c_void_p),
-                ("field_location", C.c_int)]
+                ("field_location", C.c_int), ("subject_pre", C.c_int)]
 
 
 class Result(C.Structure):

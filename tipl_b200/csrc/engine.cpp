@@ -26,6 +26,7 @@
 #include "batcher.h"
 #include "host.h"
 #include "kernels.h"
+#include "preprocess.h"
 #include "stats.h"
 #include "scheduler.h"
 
@@ -217,9 +218,11 @@ private:
         if (j.template_id < 0)
             b += nf * ps;
         b += nm * (double)pix_size(j.moving.dtype);
-        const bool float_cdm = ftype != REGB_U8 || j.moving.dtype != REGB_U8;
-        if (j.moving.dtype != REGB_U8)
+        const bool float_cdm = !j.subject_pre && (ftype != REGB_U8 || j.moving.dtype != REGB_U8);
+        if (j.moving.dtype != REGB_U8 || j.subject_pre)
             b += nm;                          // uint8 copy for the affine stage
+        if (j.subject_pre)
+            b += 12.0 * nm;                   // widened copy, smoothed copy, values above the threshold
         if (j.template_id < 0 && ftype != REGB_U8)
             b += nf;
         if (j.run_cdm && float_cdm)
@@ -347,13 +350,30 @@ private:
             }
         }
         const uint8_t* moving_u8 = (const uint8_t*)d_moving;
-        if (s.moving.dtype != REGB_U8 && s.run_linear) {
+        if (s.subject_pre) {
+            // the mm_reg pipeline: the subject through subject_image_pre, the template
+            // through template_image_pre (its uint8 copy), both stages on uint8
+            DevBuf<float> wide;
+            const float* f = (const float*)d_moving;
+            if (s.moving.dtype != REGB_F32) {
+                to_f32(d_moving, s.moving.dtype, nm, wide, st.s);
+                f = wide.p;
+            }
+            moving_q.alloc(nm, st.s);
+            subject_image_pre(f, s.moving.dim, moving_q.p, st.s);
+            moving_u8 = moving_q.p;
+            if (!fixed_u8) {
+                to_u8(d_fixed, fdtype, nfx, fixed_q, st.s);
+                fixed_u8 = fixed_q.p;
+            }
+        } else if (s.moving.dtype != REGB_U8 && s.run_linear) {
             to_u8(d_moving, s.moving.dtype, nm, moving_q, st.s);
             moving_u8 = moving_q.p;
         }
-        // CDM runs on uint8 when both volumes are uint8 (the reference GPU path's type),
-        // otherwise in float on the volumes widened exactly from their storage type
-        const bool float_cdm = fdtype != REGB_U8 || s.moving.dtype != REGB_U8;
+        // CDM runs on uint8 when both volumes are uint8 or the subject was preprocessed
+        // (the reference GPU path's type), otherwise in float on the volumes widened
+        // exactly from their storage type
+        const bool float_cdm = !s.subject_pre && (fdtype != REGB_U8 || s.moving.dtype != REGB_U8);
         const float* moving_f32 = nullptr;
         if (s.run_cdm && float_cdm) {
             if (!fixed_f32 || s.template_id < 0) {
@@ -405,11 +425,12 @@ private:
             if (pix)
                 REGB_CK(launch_resample<float>(moving_f32, md, (float*)Is.p, fdd, T, sh, st.s));
             else
-                REGB_CK(launch_resample<uint8_t>((const uint8_t*)d_moving, md, Is.p, fdd, T, sh, st.s));
+                REGB_CK(launch_resample<uint8_t>(s.subject_pre ? moving_u8 : (const uint8_t*)d_moving, md, Is.p, fdd,
+                                                 T, sh, st.s));
             DevBuf<float> field(3 * nf, st.s);
             int iters = 0;
-            regb_status cs = cdm_register(pix ? (const void*)fixed_f32 : d_fixed, Is.p, fdim, pix, field.p, s.cdm,
-                                          &j->cancel, st.s, &iters, &sched_);
+            const void* It = pix ? (const void*)fixed_f32 : (s.subject_pre ? (const void*)fixed_u8 : d_fixed);
+            regb_status cs = cdm_register(It, Is.p, fdim, pix, field.p, s.cdm, &j->cancel, st.s, &iters, &sched_);
             r.cdm_ok = (cs == REGB_OK) ? 1 : 0;
             r.cdm_iterations = iters;
             if (cs == REGB_CANCELLED)
@@ -495,6 +516,7 @@ void regb_job_default(regb_job* j)
     regb_cdm_param_default(&j->cdm);
     j->arg[6] = j->arg[7] = j->arg[8] = 1.0f;
     j->field_location = REGB_HOST;
+    j->subject_pre = 0;
 }
 
 regb_status regb_engine_create(const regb_engine_config* cfg, regb_engine** out)
