@@ -335,6 +335,58 @@ def precision_report(args):
     return 0
 
 
+def pre_case(args):
+    """Subject preprocessing of a 182x218x182 float32 subject: the fused Gaussian round
+    (CUDA events over 20 launches, after warm-up) against the HBM copy peak, the whole
+    subject_image_pre on device buffers, and the reference's CPU subject_image_pre."""
+    import torch
+
+    import tipl_b200 as tb
+    from tipl_b200 import phantom as ph
+
+    rng = np.random.default_rng(ph.seed_for(4, 13))
+    t = ph.rician(ph.class_phantom(SHAPE, rng), rng)
+    d = torch.from_numpy(t).cuda()
+    g = torch.empty_like(d)
+    u = torch.empty(SHAPE, dtype=torch.uint8, device="cuda")
+    for _ in range(3):
+        tb.gaussian(d, out=g)
+        tb.subject_image_pre(d, out=u)
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    cur = torch.cuda.current_stream()
+    a.record()
+    for _ in range(20):
+        tb.gaussian(d, out=g, stream=cur)  # device views on the caller's stream: no sync per call
+    b.record()
+    torch.cuda.synchronize()
+    g_ms = a.elapsed_time(b) / 20
+    t0 = time.perf_counter()
+    for _ in range(5):
+        tb.subject_image_pre(d, out=u)
+    torch.cuda.synchronize()
+    pre_ms = (time.perf_counter() - t0) / 5 * 1000.0
+    hbm, kind = peaks()
+    nbytes = 2 * 4 * t.size
+    line = {"kernel_case": "pre", "gaussian_ms": g_ms, "gaussian_gbs": nbytes / (g_ms / 1000.0) / 1e9,
+            "gaussian_frac_of_hbm": nbytes / (g_ms / 1000.0) / 1e9 / hbm, "hbm_peak_gbs": hbm, "peak_kind": kind,
+            "subject_image_pre_ms": pre_ms}
+    try:
+        import oracle
+
+        R = oracle.Reference()
+        R.set_threads(os.cpu_count() or 1)
+        t0 = time.perf_counter()
+        ref = R.subject_image_pre(t)
+        line["reference_cpu_ms"] = (time.perf_counter() - t0) * 1000.0
+        line["bit_exact"] = bool(np.array_equal(ref, u.cpu().numpy()))
+    except (OSError, FileNotFoundError):
+        pass
+    print(json.dumps(line))
+    return 0
+
+
 def kernel_case(args):
     """Three launches of one cost kernel on the full-size pair, K candidates each."""
     import torch
@@ -481,7 +533,7 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=3,
                     help="served mode: plain single-job registrations timed afterwards for the served/plain ratio")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel-case", choices=["mi", "corr", "cdm"], default=None,
+    ap.add_argument("--kernel-case", choices=["mi", "corr", "cdm", "pre"], default=None,
                     help="run only K-candidate cost batches of the full-size pair (for profiler captures)")
     ap.add_argument("--k", type=int, default=12)
     ap.add_argument("--precision-report", action="store_true",
@@ -496,6 +548,8 @@ def main():
         return run_reference(args)
     if args.kernel_case == "cdm":
         return cdm_case(args)
+    if args.kernel_case == "pre":
+        return pre_case(args)
     if args.kernel_case:
         return kernel_case(args)
 

@@ -2,6 +2,7 @@
 // Every entry validates its views, stages host memory through device buffers when
 // a view lives on the host, and turns failures into regb_status codes.
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include "affine_eval.h"
@@ -229,8 +230,8 @@ regb_status regb_normalize_to_u8(const regb_volume* in, regb_volume* out, float 
         if (!pix_size(in->dtype) || out->dtype != REGB_U8 || !same_dims(in->dim, out->dim))
             throw Failure(REGB_ERR_ARG, "normalize: in U8/F32/U16/BF16, out U8 of the same shape");
         const bool dev = in->location == REGB_DEVICE && out->location == REGB_DEVICE;
-        Stream own;
-        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : own.s;
+        std::unique_ptr<Stream> own;  // only when the caller's stream is not used
+        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : (own = std::make_unique<Stream>())->s;
         const size_t n = nvox(in->dim);
         Staged a, b;
         a.in(in->ptr, n * pix_size(in->dtype), in->location, st, true);
@@ -255,8 +256,8 @@ regb_status regb_widen_to_f32(const regb_volume* in, regb_volume* out, void* str
             !same_dims(in->dim, out->dim))
             throw Failure(REGB_ERR_ARG, "widen: in U8/U16/BF16, out F32 of the same shape");
         const bool dev = in->location == REGB_DEVICE && out->location == REGB_DEVICE;
-        Stream own;
-        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : own.s;
+        std::unique_ptr<Stream> own;  // only when the caller's stream is not used
+        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : (own = std::make_unique<Stream>())->s;
         const size_t n = nvox(in->dim);
         Staged a, b;
         a.in(in->ptr, n * pix_size(in->dtype), in->location, st, true);
@@ -281,8 +282,8 @@ regb_status regb_gaussian(const regb_volume* in, regb_volume* out, int bandwidth
         if (in->ptr == out->ptr)
             throw Failure(REGB_ERR_ARG, "gaussian: in and out must be distinct");
         const bool dev = in->location == REGB_DEVICE && out->location == REGB_DEVICE;
-        Stream own;
-        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : own.s;
+        std::unique_ptr<Stream> own;  // only when the caller's stream is not used
+        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : (own = std::make_unique<Stream>())->s;
         const size_t n = nvox(in->dim);
         Staged a, b;
         a.in(in->ptr, n * 4, in->location, st, true);
@@ -303,8 +304,8 @@ regb_status regb_subject_image_pre(const regb_volume* in, regb_volume* out, void
         if (!pix_size(in->dtype) || out->dtype != REGB_U8 || !same_dims(in->dim, out->dim))
             throw Failure(REGB_ERR_ARG, "subject_image_pre: in U8/F32/U16/BF16, out U8 of the same shape");
         const bool dev = in->location == REGB_DEVICE && out->location == REGB_DEVICE;
-        Stream own;
-        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : own.s;
+        std::unique_ptr<Stream> own;  // only when the caller's stream is not used
+        cudaStream_t st = (dev && stream) ? (cudaStream_t)stream : (own = std::make_unique<Stream>())->s;
         const size_t n = nvox(in->dim);
         Staged a, b;
         a.in(in->ptr, n * pix_size(in->dtype), in->location, st, true);

@@ -55,12 +55,19 @@ __global__ void __launch_bounds__(kThreads) minmax_kernel(const void* __restrict
         lo = min(lo, k);
         hi = max(hi, k);
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    __shared__ unsigned slo[kThreads / 32], shi[kThreads / 32];
     if ((threadIdx.x & 31) == 0) {
+        slo[threadIdx.x >> 5] = lo;
+        shi[threadIdx.x >> 5] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < kThreads / 32; ++k) {
+            lo = min(lo, slo[k]);
+            hi = max(hi, shi[k]);
+        }
         atomicMin(&mm[0], lo);
         atomicMax(&mm[1], hi);
     }
@@ -110,12 +117,12 @@ cudaError_t launch_normalize_to_u8(const void* in, int dtype, long long n, float
         e = cudaMemsetAsync(mm + 1, 0, sizeof(unsigned), st);         // max key
     if (e != cudaSuccess)
         return e;
-    const int g = grid_for(n);
+    const int g = grid_for(n), gm = std::min(g, 148 * 4);
     switch (dtype) {
-    case 0: minmax_kernel<0><<<g, kThreads, 0, st>>>(in, n, mm); normalize_kernel<0><<<g, kThreads, 0, st>>>(in, n, mm, upper, out); break;
-    case 1: minmax_kernel<1><<<g, kThreads, 0, st>>>(in, n, mm); normalize_kernel<1><<<g, kThreads, 0, st>>>(in, n, mm, upper, out); break;
-    case 2: minmax_kernel<2><<<g, kThreads, 0, st>>>(in, n, mm); normalize_kernel<2><<<g, kThreads, 0, st>>>(in, n, mm, upper, out); break;
-    case 3: minmax_kernel<3><<<g, kThreads, 0, st>>>(in, n, mm); normalize_kernel<3><<<g, kThreads, 0, st>>>(in, n, mm, upper, out); break;
+    case 0: minmax_kernel<0><<<gm, kThreads, 0, st>>>(in, n, mm); normalize_kernel<0><<<g, kThreads, 0, st>>>(in, n, mm, upper, out); break;
+    case 1: minmax_kernel<1><<<gm, kThreads, 0, st>>>(in, n, mm); normalize_kernel<1><<<g, kThreads, 0, st>>>(in, n, mm, upper, out); break;
+    case 2: minmax_kernel<2><<<gm, kThreads, 0, st>>>(in, n, mm); normalize_kernel<2><<<g, kThreads, 0, st>>>(in, n, mm, upper, out); break;
+    case 3: minmax_kernel<3><<<gm, kThreads, 0, st>>>(in, n, mm); normalize_kernel<3><<<g, kThreads, 0, st>>>(in, n, mm, upper, out); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -128,7 +135,7 @@ cudaError_t launch_minmax(const void* in, int dtype, long long n, unsigned* mm, 
         e = cudaMemsetAsync(mm + 1, 0, sizeof(unsigned), st);
     if (e != cudaSuccess)
         return e;
-    const int g = grid_for(n);
+    const int g = std::min(grid_for(n), 148 * 4);  // one atomic pair per block
     switch (dtype) {
     case 0: minmax_kernel<0><<<g, kThreads, 0, st>>>(in, n, mm); break;
     case 1: minmax_kernel<1><<<g, kThreads, 0, st>>>(in, n, mm); break;

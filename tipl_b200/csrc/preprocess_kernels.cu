@@ -15,17 +15,18 @@ namespace {
 
 // ------------------------------------------------------------------ Gaussian
 // One round of the reference's x, y, z passes fused in one kernel.  A block owns a
-// 32 x 8 column of outputs over kGz planes; it walks z with a ring of y-passed planes,
-// staging each input plane with a one-voxel halo in shared memory.  Halo and edge
-// samples are loaded from clamped coordinates, which is exactly the reference's
-// "repeat the edge sample" rule for every pass (the x-pass of a clamped row is the
-// x-pass of the edge row).
-constexpr int kGx = 32, kGy = 8, kGz = 16, kGThreads = kGx * kGy;
+// 32 x 8 x 8 tile of outputs: it stages the tile and a one-voxel halo (34 x 10 x 10) in
+// shared memory, then runs the x pass over every staged row, the y pass over the rows
+// the z pass needs, and the z pass into the output -- three barriers a block, 13
+// independent loads in flight per thread.  Halo and edge samples come from clamped
+// coordinates, which is exactly the reference's "repeat the edge sample" rule for every
+// pass (the x pass of a clamped row is the x pass of the edge row).
+constexpr int kGx = 32, kGy = 8, kGz = 8, kGThreads = 256;
 
 struct GaussSmem {
-    float in[kGy + 2][kGx + 2];  // input plane with halo
-    float xp[kGy + 2][kGx];      // x-pass of the plane (incl. y halo rows)
-    float yp[3][kGy][kGx];       // ring of x+y-passed planes (z-1, z, z+1)
+    float in[kGz + 2][kGy + 2][kGx + 2];
+    float xp[kGz + 2][kGy + 2][kGx];
+    float yp[kGz + 2][kGy][kGx];
 };
 
 __device__ __forceinline__ float tap3(float l, float c, float r)
@@ -34,49 +35,70 @@ __device__ __forceinline__ float tap3(float l, float c, float r)
     return __fadd_rn(__fadd_rn(l, __fadd_rn(c, c)), r);
 }
 
-__device__ __forceinline__ void stage_plane(const float* __restrict__ in, int w, int h, int d, int x0, int y0, int z,
-                                            GaussSmem& s, float (*dst)[kGx])
-{
-    const int t = threadIdx.x;
-    const int zc = min(max(z, 0), d - 1);
-    const float* plane = in + (long long)zc * w * h;
-    for (int i = t; i < (kGy + 2) * (kGx + 2); i += kGThreads) {
-        const int ly = i / (kGx + 2), lx = i % (kGx + 2);
-        const int gx = min(max(x0 + lx - 1, 0), w - 1), gy = min(max(y0 + ly - 1, 0), h - 1);
-        s.in[ly][lx] = plane[(long long)gy * w + gx];
-    }
-    __syncthreads();
-    for (int i = t; i < (kGy + 2) * kGx; i += kGThreads) {
-        const int ly = i / kGx, lx = i % kGx;
-        s.xp[ly][lx] = tap3(s.in[ly][lx], s.in[ly][lx + 1], s.in[ly][lx + 2]);
-    }
-    __syncthreads();
-    {
-        const int ly = t / kGx, lx = t % kGx;
-        dst[ly][lx] = tap3(s.xp[ly][lx], s.xp[ly + 1][lx], s.xp[ly + 2][lx]);
-    }
-    __syncthreads();
-}
-
 __global__ void __launch_bounds__(kGThreads) gaussian_round_kernel(const float* __restrict__ in,
                                                                     float* __restrict__ out, int w, int h, int d,
                                                                     float scale, int apply_scale)
 {
-    __shared__ GaussSmem s;
+    extern __shared__ float4 gsm4[];
+    GaussSmem& s = *reinterpret_cast<GaussSmem*>(gsm4);
+    // thread (tx, ty) of a 32 x 8 block owns staged column tx + 1 of rows ty and ty + 8
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int x0 = blockIdx.x * kGx, y0 = blockIdx.y * kGy, z0 = blockIdx.z * kGz;
-    const int z1 = min(d, z0 + kGz);
-    const int ly = threadIdx.x / kGx, lx = threadIdx.x % kGx;
-    const int gx = x0 + lx, gy = y0 + ly;
-    // ring slots: plane z-1, z, z+1 live in yp[(z + 2) % 3], yp[z % 3]... indexed by (z + 3) % 3
-    stage_plane(in, w, h, d, x0, y0, z0 - 1, s, s.yp[(z0 + 2) % 3]);
-    stage_plane(in, w, h, d, x0, y0, z0, s, s.yp[z0 % 3]);
-    for (int z = z0; z < z1; ++z) {
-        stage_plane(in, w, h, d, x0, y0, z + 1, s, s.yp[(z + 1) % 3]);
-        if (gx < w && gy < h) {
-            float v = tap3(s.yp[(z + 2) % 3][ly][lx], s.yp[z % 3][ly][lx], s.yp[(z + 1) % 3][ly][lx]);
-            if (apply_scale)
-                v = __fmul_rn(v, scale);
-            out[((long long)z * h + gy) * w + gx] = v;
+    const int gxc = min(x0 + tx, w - 1);
+    // the two halo columns: lanes 0 and 1 also load x0 - 1 and x0 + 32 (clamped)
+    const int gxh = (tx == 0) ? max(x0 - 1, 0) : min(x0 + kGx, w - 1);
+    const bool row2 = ty < 2;  // rows 8 and 9 of the staged tile
+    const int gy0 = min(max(y0 + ty - 1, 0), h - 1), gy1 = min(max(y0 + ty + 7, 0), h - 1);
+    float c0[kGz + 2], c1[kGz + 2], h0[kGz + 2], h1[kGz + 2];
+#pragma unroll
+    for (int lz = 0; lz < kGz + 2; ++lz) {
+        const int gz = min(max(z0 + lz - 1, 0), d - 1);
+        const float* plane = in + (long long)gz * w * h;
+        c0[lz] = __ldg(plane + (long long)gy0 * w + gxc);
+        if (row2)
+            c1[lz] = __ldg(plane + (long long)gy1 * w + gxc);
+        if (tx < 2) {
+            h0[lz] = __ldg(plane + (long long)gy0 * w + gxh);
+            if (row2)
+                h1[lz] = __ldg(plane + (long long)gy1 * w + gxh);
+        }
+    }
+    const int hx = (tx == 0) ? 0 : kGx + 1;
+#pragma unroll
+    for (int lz = 0; lz < kGz + 2; ++lz) {
+        s.in[lz][ty][tx + 1] = c0[lz];
+        if (row2)
+            s.in[lz][ty + 8][tx + 1] = c1[lz];
+        if (tx < 2) {
+            s.in[lz][ty][hx] = h0[lz];
+            if (row2)
+                s.in[lz][ty + 8][hx] = h1[lz];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int lz = 0; lz < kGz + 2; ++lz) {
+        s.xp[lz][ty][tx] = tap3(s.in[lz][ty][tx], s.in[lz][ty][tx + 1], s.in[lz][ty][tx + 2]);
+        if (row2)
+            s.xp[lz][ty + 8][tx] = tap3(s.in[lz][ty + 8][tx], s.in[lz][ty + 8][tx + 1], s.in[lz][ty + 8][tx + 2]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int lz = 0; lz < kGz + 2; ++lz)
+        s.yp[lz][ty][tx] = tap3(s.xp[lz][ty][tx], s.xp[lz][ty + 1][tx], s.xp[lz][ty + 2][tx]);
+    __syncthreads();
+    const int gx = x0 + tx, gy = y0 + ty;
+    if (gx < w && gy < h) {
+        float* o = out + (long long)gy * w + gx;
+#pragma unroll
+        for (int lz = 0; lz < kGz; ++lz) {
+            const int gz = z0 + lz;
+            if (gz < d) {
+                float v = tap3(s.yp[lz][ty][tx], s.yp[lz + 1][ty][tx], s.yp[lz + 2][ty][tx]);
+                if (apply_scale)
+                    v = __fmul_rn(v, scale);
+                o[(long long)gz * w * h] = v;
+            }
         }
     }
 }
@@ -225,34 +247,56 @@ __global__ void __launch_bounds__(512) chunk_median_kernel(const float* __restri
                                                             float* __restrict__ med)
 {
     __shared__ unsigned hist[2048];
+    __shared__ unsigned part[512];
     __shared__ unsigned sel_bin, sel_rank;
     const long long cs = m / 256, rem = m % 256, c = blockIdx.x;
     const long long s0 = c * cs + (c < rem ? c : rem);
     const long long len = cs + (c < rem ? 1 : 0);
+    const int t = threadIdx.x;
     unsigned rank = (unsigned)(len / 2);  // 0-based rank sought
     unsigned prefix = 0u, pmask = 0u;
     const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
     for (int pass = 0; pass < 3; ++pass) {
         const int sh = shifts[pass], nb = 1 << widths[pass];
-        for (int i = threadIdx.x; i < nb; i += blockDim.x)
+        for (int i = t; i < 2048; i += blockDim.x)
             hist[i] = 0u;
         __syncthreads();
-        for (long long i = threadIdx.x; i < len; i += blockDim.x) {
-            const unsigned k = fkey(v[s0 + i]);
-            if ((k & pmask) == prefix)
-                atomicAdd(&hist[(k >> sh) & (nb - 1)], 1u);
+        // values of one chunk crowd into few bins: one atomic per distinct bin per warp
+        for (long long i0 = 0; i0 < len; i0 += blockDim.x) {
+            const long long i = i0 + t;
+            bool in = i < len;
+            unsigned k = in ? fkey(v[s0 + i]) : 0u;
+            in = in && (k & pmask) == prefix;
+            const unsigned bin = in ? (k >> sh) & (nb - 1) : 0xffffffffu;
+            const unsigned peers = __match_any_sync(0xffffffffu, bin);
+            if (in && (threadIdx.x & 31) == (__ffs(peers) - 1))
+                atomicAdd(&hist[bin], (unsigned)__popc(peers));
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned acc = 0u;
-            int b = 0;
-            for (; b < nb; ++b) {
-                if (acc + hist[b] > rank)
+        // block prefix over the bins: thread t owns bins 4t..4t+3
+        unsigned own = 0u;
+        for (int k = 0; k < 4; ++k)
+            own += (4 * t + k < nb) ? hist[4 * t + k] : 0u;
+        part[t] = own;
+        __syncthreads();
+        for (int o = 1; o < 512; o <<= 1) {
+            const unsigned add = t >= o ? part[t - o] : 0u;
+            __syncthreads();
+            part[t] += add;
+            __syncthreads();
+        }
+        const unsigned before = t ? part[t - 1] : 0u;
+        if (before <= rank && rank < part[t]) {
+            unsigned acc = before;
+            for (int k = 0; k < 4; ++k) {
+                const unsigned hk = hist[4 * t + k];
+                if (rank < acc + hk) {
+                    sel_bin = (unsigned)(4 * t + k);
+                    sel_rank = rank - acc;
                     break;
-                acc += hist[b];
+                }
+                acc += hk;
             }
-            sel_bin = (unsigned)b;
-            sel_rank = rank - acc;
         }
         __syncthreads();
         prefix |= sel_bin << sh;
@@ -260,7 +304,7 @@ __global__ void __launch_bounds__(512) chunk_median_kernel(const float* __restri
         rank = sel_rank;
         __syncthreads();
     }
-    if (threadIdx.x == 0)
+    if (t == 0)
         med[c] = __uint_as_float((prefix & 0x80000000u) ? (prefix & 0x7fffffffu) : ~prefix);
 }
 
@@ -302,8 +346,20 @@ int pgrid(long long n)
 cudaError_t launch_gaussian_round(const float* in, float* out, int w, int h, int d, float scale, int apply_scale,
                                   cudaStream_t st)
 {
+    static bool attr_done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return e;
+    if (dev < 64 && !attr_done[dev]) {
+        e = cudaFuncSetAttribute(gaussian_round_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(GaussSmem));
+        if (e != cudaSuccess)
+            return e;
+        attr_done[dev] = true;
+    }
     const dim3 grid((w + kGx - 1) / kGx, (h + kGy - 1) / kGy, (d + kGz - 1) / kGz);
-    gaussian_round_kernel<<<grid, kGThreads, 0, st>>>(in, out, w, h, d, scale, apply_scale);
+    gaussian_round_kernel<<<grid, kGThreads, sizeof(GaussSmem), st>>>(in, out, w, h, d, scale, apply_scale);
     return cudaGetLastError();
 }
 
