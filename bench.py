@@ -355,11 +355,13 @@ def pre_case(args):
     torch.cuda.synchronize()
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
-    cur = torch.cuda.current_stream()
-    a.record()
+    # a stream of our own (a NULL stream asks the library to use, and wait for, its own)
+    cur = torch.cuda.Stream()
+    cur.wait_stream(torch.cuda.current_stream())
+    a.record(cur)
     for _ in range(20):
         tb.gaussian(d, out=g, stream=cur)  # device views on the caller's stream: no sync per call
-    b.record()
+    b.record(cur)
     torch.cuda.synchronize()
     g_ms = a.elapsed_time(b) / 20
     t0 = time.perf_counter()

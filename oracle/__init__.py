@@ -65,6 +65,33 @@ class _Lib:
     def _fn(self, name):
         return getattr(self.lib, self._pfx + name)
 
+    # -- mapping steps of the mm_reg pipeline (reg/mm_reg.hpp:271-345)
+    def displacement_to_mapping(self, dis, T):
+        d = np.ascontiguousarray(dis, np.float32)
+        out = np.zeros_like(d)
+        self._fn("displacement_to_mapping" + ("" if self._pfx == "tiplref_" else "_f32"))(
+            _ptr(d), _ptr(_dims(d.shape)), _ptr(_f32(T)), _ptr(out))
+        return out
+
+    def inv_displacement_to_mapping(self, inv_dis, T, map_shape):
+        d = np.ascontiguousarray(inv_dis, np.float32)
+        out = np.zeros(tuple(map_shape) + (3,), np.float32)
+        self._fn("inv_displacement_to_mapping" + ("" if self._pfx == "tiplref_" else "_f32"))(
+            _ptr(d), _ptr(_dims(d.shape)), _ptr(_f32(T)), _ptr(_dims(map_shape)), _ptr(out))
+        return out
+
+    def compose_mapping(self, img, mapping):
+        m = np.ascontiguousarray(mapping, np.float32)
+        out = np.zeros(m.shape[:3], np.uint8)
+        self._fn("compose_mapping_u8")(_ptr(_u8(img)), _ptr(_dims(img.shape)), _ptr(m), _ptr(_dims(m.shape)),
+                                       _ptr(out))
+        return out
+
+    def correlation(self, x, y):
+        f = self._fn("correlation_u8")
+        f.restype = C.c_double
+        return f(_ptr(_u8(x)), _ptr(_u8(y)), C.c_longlong(x.size))
+
     # -- subject preprocessing of the mm_reg pipeline (reg/mm_reg.hpp:14-20)
     def gaussian(self, img, bandwidth=1):
         out = np.ascontiguousarray(img, np.float32).copy()

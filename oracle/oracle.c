@@ -273,6 +273,9 @@ ORC_NORMALIZE(orc_normalize_to_u8_f32, float)
 ORC_NORMALIZE(orc_normalize_to_u8_u16, uint16_t)
 #undef ORC_NORMALIZE
 
+/* ---- mapping steps of the mm_reg pipeline --------------------------------- */
+#include "oracle_map.h"
+
 /* ---- subject preprocessing of the mm_reg pipeline ------------------------- */
 #include "oracle_pre.h"
 

@@ -67,6 +67,11 @@ int orc_cdm_level_f64(const double* It, const double* Is, const int* dim, double
 
 int orc_normalize_to_u8_f32(const float* in, long long n, uint8_t* out, float upper);
 int orc_normalize_to_u8_u16(const uint16_t* in, long long n, uint8_t* out, float upper);
+void orc_displacement_to_mapping_f32(const float* dis, const int* dim, const float* T, float* mapping);
+void orc_inv_displacement_to_mapping_f32(const float* inv_dis, const int* dis_dim, const float* T,
+                                         const int* map_dim, float* inv_mapping);
+void orc_compose_mapping_u8(const uint8_t* from, const int* fdim, const float* mapping, const int* mdim, uint8_t* to);
+double orc_correlation_u8(const uint8_t* x, const uint8_t* y, long long n);
 void orc_gaussian_f32(float* img, const int* dim, int bandwidth);
 float orc_otsu_threshold_f32(const float* img, long long n);
 float orc_median_f32(const float* v, long long n);

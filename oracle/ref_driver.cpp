@@ -303,6 +303,39 @@ void tiplref_normalize_to_u8(const float* in, const int* dim, u8* out, float upp
         std::copy(o.begin(), o.end(), out);
 }
 
+// displacement_to_mapping(dis, mapping, T) (numerical/dif.hpp:42-51)
+void tiplref_displacement_to_mapping(const float* dis, const int* dim, const float* T, float* mapping)
+{
+    auto d = field_in(dis, dim);
+    tipl::image<3, vec3> m(shp(dim));
+    tipl::displacement_to_mapping(d, m, to_matrix(T));
+    field_out(m, mapping);
+}
+
+// inv_displacement_to_mapping(inv_dis, inv_mapping, T) (numerical/dif.hpp:53-66)
+void tiplref_inv_displacement_to_mapping(const float* inv_dis, const int* dis_dim, const float* T,
+                                         const int* map_dim, float* inv_mapping)
+{
+    auto d = field_in(inv_dis, dis_dim);
+    tipl::image<3, vec3> m(shp(map_dim));
+    tipl::inv_displacement_to_mapping(d, m, to_matrix(T));
+    field_out(m, inv_mapping);
+}
+
+// compose_mapping(from, mapping) for a uint8 image (numerical/dif.hpp:70-90)
+void tiplref_compose_mapping_u8(const u8* from, const int* fdim, const float* mapping, const int* mdim, u8* to)
+{
+    auto m = field_in(mapping, mdim);
+    auto o = tipl::compose_mapping(cview(from, fdim), m);
+    std::copy(o.begin(), o.end(), to);
+}
+
+// correlation(x, y) of two uint8 images (numerical/statistics.hpp:585-598)
+double tiplref_correlation_u8(const u8* x, const u8* y, long long n)
+{
+    return tipl::correlation(x, x + n, y);
+}
+
 // filter::gaussian(I, bandwidth) on a float image (filter/gaussian.hpp:84-96), in place
 void tiplref_gaussian(float* img, const int* dim, int bandwidth)
 {
