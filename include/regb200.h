@@ -200,6 +200,23 @@ regb_status regb_compose_displacement(const regb_volume* from, const regb_field*
 /* tipl::accumulate_displacement(dis, new_dis) (numerical/dif.hpp:166-186, 311-329):
  * new_dis <- dis composed with new_dis, in place. */
 regb_status regb_accumulate_displacement(const regb_field* dis, regb_field* new_dis, void* stream);
+/* displacement_to_mapping(dis, mapping, T) (numerical/dif.hpp:42-51): mapping(x) =
+ * T(x + dis(x)), the template-grid -> subject-voxel mapping of the mm_reg pipeline
+ * (reg/mm_reg.hpp:279-283).  dis and mapping share a shape. */
+regb_status regb_displacement_to_mapping(const regb_field* dis, const float T[12], regb_field* mapping, void* stream);
+/* inv_displacement_to_mapping(inv_dis, inv_mapping, T) (numerical/dif.hpp:53-66): over the
+ * inv_mapping grid, p = T^-1(x), inv_mapping(x) = p + trilinear(inv_dis, p) (zero off the
+ * field); the subject-grid -> template-voxel mapping (reg/mm_reg.hpp:274-278).
+ * REGB_FALSE when T is singular. */
+regb_status regb_inv_displacement_to_mapping(const regb_field* inv_dis, const float T[12], regb_field* inv_mapping,
+                                             void* stream);
+/* compose_mapping(from, mapping) (numerical/dif.hpp:70-90) of a uint8 volume: to(x) =
+ * trilinear(from, mapping(x)), 0 where the 2x2x2 cell leaves from; to has the mapping's shape. */
+regb_status regb_compose_mapping(const regb_volume* from, const regb_field* mapping, regb_volume* to, void* stream);
+/* correlation(x, y) (numerical/statistics.hpp:585-598) of two uint8 volumes of one shape:
+ * Pearson r from exact integer moments, 0 when either is constant; masked != 0 gives
+ * correlation_ygz (:600-619), over the voxels with y > 0 only (mm_reg's default r). */
+regb_status regb_correlation(const regb_volume* x, const regb_volume* y, int masked, double* r);
 /* downsample_with_padding (numerical/resampling.hpp:575-671); out dims (d+1)/2. */
 regb_status regb_downsample(const regb_volume* in, regb_volume* out, void* stream);
 /* best_d *= 2; upsample_with_padding(best_d, shape) (reg/cdm.hpp:402-403,

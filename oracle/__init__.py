@@ -87,8 +87,8 @@ class _Lib:
                                        _ptr(out))
         return out
 
-    def correlation(self, x, y):
-        f = self._fn("correlation_u8")
+    def correlation(self, x, y, masked=False):
+        f = self._fn("correlation_ygz_u8" if masked else "correlation_u8")
         f.restype = C.c_double
         return f(_ptr(_u8(x)), _ptr(_u8(y)), C.c_longlong(x.size))
 

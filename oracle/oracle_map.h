@@ -75,3 +75,23 @@ double orc_correlation_u8(const uint8_t* x, const uint8_t* y, long long n)
         return 0.0;
     return ((double)sxy / dn - mx * my) / sd1 / sd2;
 }
+
+/* correlation_ygz (numerical/statistics.hpp:600-619): correlation over the voxels with y > 0 */
+double orc_correlation_ygz_u8(const uint8_t* x, const uint8_t* y, long long n)
+{
+    if (n <= 0)
+        return 0.0;
+    uint8_t* nx = (uint8_t*)malloc((size_t)n);
+    uint8_t* ny = (uint8_t*)malloc((size_t)n);
+    long long m = 0;
+    for (long long i = 0; i < n; ++i)
+        if (y[i] > 0) {
+            nx[m] = x[i];
+            ny[m] = y[i];
+            ++m;
+        }
+    double r = m ? orc_correlation_u8(nx, ny, m) : 0.0;
+    free(nx);
+    free(ny);
+    return r;
+}

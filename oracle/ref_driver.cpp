@@ -336,6 +336,12 @@ double tiplref_correlation_u8(const u8* x, const u8* y, long long n)
     return tipl::correlation(x, x + n, y);
 }
 
+// correlation_ygz(x, y) of two uint8 images (numerical/statistics.hpp:600-619)
+double tiplref_correlation_ygz_u8(const u8* x, const u8* y, long long n)
+{
+    return tipl::correlation_ygz(x, x + n, y);
+}
+
 // filter::gaussian(I, bandwidth) on a float image (filter/gaussian.hpp:84-96), in place
 void tiplref_gaussian(float* img, const int* dim, int bandwidth)
 {

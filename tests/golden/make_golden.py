@@ -46,6 +46,29 @@ def main():
         preprocess(R)
     if args.only in (None, "linear_runs"):
         linear_runs(R)
+    if args.only in (None, "mapping"):
+        mapping(R)
+
+
+def mapping(R):
+    """displacement_to_mapping, inv_displacement_to_mapping, compose_mapping, correlation(_ygz)."""
+    rng = np.random.default_rng(ph.seed_for(5, 21))
+    out = {}
+    for k, (shp, mshp) in enumerate([((20, 24, 18), (22, 19, 25)), ((9, 7, 11), (9, 7, 11)), ((1, 12, 14), (3, 10, 15))]):
+        dis = rng.normal(0, 1.5, shp + (3,)).astype(np.float32)
+        dis.reshape(-1, 3)[::5] = 0
+        p = ph.random_affine(rng, rot_deg=8, trans_vox=2)
+        T = R.affine_to_matrix(p, shp, (1, 1, 1), mshp, (1, 1, 1))
+        img = (rng.random(mshp) * 255).astype(np.uint8)
+        m = R.displacement_to_mapping(dis, T)
+        x = (rng.random(shp) * 255).astype(np.uint8)
+        y = (rng.random(shp) * 255).astype(np.uint8)
+        y.flat[::3] = 0
+        out.update({f"c{k}_dis": dis, f"c{k}_T": T, f"c{k}_mshape": np.array(mshp), f"c{k}_img": img,
+                    f"c{k}_map": m, f"c{k}_inv": R.inv_displacement_to_mapping(dis, T, mshp),
+                    f"c{k}_composed": R.compose_mapping(img, m), f"c{k}_x": x, f"c{k}_y": y,
+                    f"c{k}_r": np.float64(R.correlation(x, y)), f"c{k}_r_ygz": np.float64(R.correlation(x, y, True))})
+    save("mapping", **out)
 
 
 def linear_pairs():

@@ -191,6 +191,38 @@ def widen_to_f32(img, out=None, stream=None):
     return out
 
 
+def displacement_to_mapping(dis, T, stream=None):
+    """displacement_to_mapping(dis, mapping, T): mapping(x) = T(x + dis(x))."""
+    out = _like(dis, dis.shape)
+    _lib.check(_lib.lib().regb_displacement_to_mapping(C.byref(_field(dis)), _fptr(np.ascontiguousarray(T, np.float32)),
+                                                       C.byref(_field(out)), _stream(stream)))
+    return out
+
+
+def inv_displacement_to_mapping(inv_dis, T, map_shape, stream=None):
+    """inv_displacement_to_mapping: over map_shape, p = T^-1(x), p + trilinear(inv_dis, p)."""
+    out = _like(inv_dis, tuple(map_shape) + (3,))
+    _lib.check(_lib.lib().regb_inv_displacement_to_mapping(C.byref(_field(inv_dis)),
+                                                           _fptr(np.ascontiguousarray(T, np.float32)),
+                                                           C.byref(_field(out)), _stream(stream)))
+    return out
+
+
+def compose_mapping(img, mapping, stream=None):
+    """compose_mapping(from, mapping) of a uint8 volume."""
+    out = _like(img, mapping.shape[:3])
+    _lib.check(_lib.lib().regb_compose_mapping(C.byref(_vol(img)), C.byref(_field(mapping)), C.byref(_vol(out)),
+                                               _stream(stream)))
+    return out
+
+
+def correlation(x, y, masked=False) -> float:
+    """Pearson r of two uint8 volumes (exact integer moments); masked: over y > 0 only."""
+    r = C.c_double(0.0)
+    _lib.check(_lib.lib().regb_correlation(C.byref(_vol(x)), C.byref(_vol(y)), int(bool(masked)), C.byref(r)))
+    return r.value
+
+
 def gaussian(img, bandwidth=1, out=None, stream=None):
     """filter::gaussian of a float32 volume (separable [1 2 1], bandwidth rounds)."""
     if out is None:

@@ -106,6 +106,10 @@ _SIGS = {
     "regb_normalize_to_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p]),
     "regb_widen_to_f32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "regb_gaussian": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "regb_displacement_to_mapping": (C.c_int, [C.c_void_p] * 4),
+    "regb_inv_displacement_to_mapping": (C.c_int, [C.c_void_p] * 4),
+    "regb_compose_mapping": (C.c_int, [C.c_void_p] * 4),
+    "regb_correlation": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     "regb_subject_image_pre": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "regb_estimate_affine_param": (C.c_int, [C.c_void_p] * 5),
     "regb_resample": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p]),

@@ -481,6 +481,95 @@ regb_status regb_compose_displacement(const regb_volume* from, const regb_field*
     });
 }
 
+regb_status regb_displacement_to_mapping(const regb_field* dis, const float T[12], regb_field* mapping, void* stream)
+{
+    return guarded([&] {
+        check_field(dis, "dis");
+        check_field(mapping, "mapping");
+        if (!T || !same_dims(dis->dim, mapping->dim))
+            throw Failure(REGB_ERR_ARG, "displacement_to_mapping: null T or shapes differ");
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t n = nvox(dis->dim);
+        Staged a, o;
+        a.in(dis->ptr, n * 12, dis->location, st, true);
+        o.in(mapping->ptr, n * 12, mapping->location, st, false);
+        REGB_CK(launch_displacement_to_mapping((const float*)a.d, Dim3{dis->dim[0], dis->dim[1], dis->dim[2]}, T,
+                                               (float*)o.d, st));
+        count_launch();
+        o.out(mapping->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_inv_displacement_to_mapping(const regb_field* inv_dis, const float T[12], regb_field* inv_mapping,
+                                             void* stream)
+{
+    return guarded([&] {
+        check_field(inv_dis, "inv_dis");
+        check_field(inv_mapping, "inv_mapping");
+        if (!T)
+            throw Failure(REGB_ERR_ARG, "inv_displacement_to_mapping: null T");
+        float iT[12];
+        std::memcpy(iT, T, sizeof(iT));
+        if (!matrix_inverse(iT))
+            return REGB_FALSE;
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t nd = nvox(inv_dis->dim), nm = nvox(inv_mapping->dim);
+        Staged a, o;
+        a.in(inv_dis->ptr, nd * 12, inv_dis->location, st, true);
+        o.in(inv_mapping->ptr, nm * 12, inv_mapping->location, st, false);
+        REGB_CK(launch_inv_displacement_to_mapping(
+            (const float*)a.d, Dim3{inv_dis->dim[0], inv_dis->dim[1], inv_dis->dim[2]}, iT,
+            Dim3{inv_mapping->dim[0], inv_mapping->dim[1], inv_mapping->dim[2]}, (float*)o.d, st));
+        count_launch();
+        o.out(inv_mapping->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_compose_mapping(const regb_volume* from, const regb_field* mapping, regb_volume* to, void* stream)
+{
+    return guarded([&] {
+        check_vol(from, "from");
+        check_field(mapping, "mapping");
+        check_vol(to, "to");
+        if (from->dtype != REGB_U8 || to->dtype != REGB_U8 || !same_dims(mapping->dim, to->dim))
+            throw Failure(REGB_ERR_ARG, "compose_mapping: uint8 from/to, to shaped like the mapping");
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t nf = nvox(from->dim), nm = nvox(mapping->dim);
+        Staged a, m, o;
+        a.in(from->ptr, nf, from->location, st, true);
+        m.in(mapping->ptr, nm * 12, mapping->location, st, true);
+        o.in(to->ptr, nm, to->location, st, false);
+        REGB_CK(launch_compose_mapping_u8((const uint8_t*)a.d, Dim3{from->dim[0], from->dim[1], from->dim[2]},
+                                          (const float*)m.d, Dim3{mapping->dim[0], mapping->dim[1], mapping->dim[2]},
+                                          (uint8_t*)o.d, st));
+        count_launch();
+        o.out(to->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_correlation(const regb_volume* x, const regb_volume* y, int masked, double* r)
+{
+    return guarded([&] {
+        check_vol(x, "x");
+        check_vol(y, "y");
+        if (!r || x->dtype != REGB_U8 || y->dtype != REGB_U8 || !same_dims(x->dim, y->dim))
+            throw Failure(REGB_ERR_ARG, "correlation: two uint8 volumes of one shape");
+        Stream s;
+        const size_t n = nvox(x->dim);
+        Staged a, b;
+        a.in(x->ptr, n, x->location, s.s, true);
+        b.in(y->ptr, n, y->location, s.s, true);
+        *r = correlation_u8((const uint8_t*)a.d, (const uint8_t*)b.d, (long long)n, masked != 0, s.s);
+        return REGB_OK;
+    });
+}
+
 regb_status regb_accumulate_displacement(const regb_field* dis, regb_field* new_dis, void* stream)
 {
     return guarded([&] {

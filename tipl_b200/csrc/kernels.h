@@ -139,6 +139,18 @@ cudaError_t launch_positive_count(const float* v, long long n, float s, unsigned
 cudaError_t launch_otsu_normalize(const float* v, long long n, float s, int shift, float c, float upper, uint8_t* out,
                                   cudaStream_t st);
 
+// Mapping steps of the mm_reg pipeline (mapping_kernels.cu).  Fields are AoS float xyz.
+// mapping = T(dis + index); out = iT(index) + trilinear(inv_dis, iT(index)) over MD;
+// to = uint8 trilinear(from, mapping) (0 off from); m[6] = exact sums x, y, x^2, y^2, xy and
+// the count, over all voxels or (masked) those with y > 0.
+cudaError_t launch_displacement_to_mapping(const float* dis, Dim3 D, const float* T, float* mapping, cudaStream_t st);
+cudaError_t launch_inv_displacement_to_mapping(const float* inv_dis, Dim3 DD, const float* iT, Dim3 MD, float* out,
+                                               cudaStream_t st);
+cudaError_t launch_compose_mapping_u8(const uint8_t* from, Dim3 FD, const float* mapping, Dim3 MD, uint8_t* to,
+                                      cudaStream_t st);
+cudaError_t launch_moments_u8(const uint8_t* x, const uint8_t* y, long long n, int masked, unsigned long long* m,
+                              cudaStream_t st);
+
 // Voxels > 0 per (x, y), (x, z), (y, z) line of a uint8 volume (zeroes the tables first).
 cudaError_t launch_mask_counts(const uint8_t* v, Dim3 dim, uint32_t* xy, uint32_t* xz, uint32_t* yz,
                                cudaStream_t st);

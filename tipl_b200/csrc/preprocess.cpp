@@ -137,6 +137,27 @@ float otsu_median(const float* d_img, long long n, cudaStream_t st)
     return middle(v);
 }
 
+// correlation(x, y) (numerical/statistics.hpp:569-598), or correlation_ygz (:600-619:
+// only the voxels with y > 0): means, deviations and covariance in double from the
+// exact integer sums (the reference widens its sums the same way).
+double correlation_u8(const uint8_t* d_x, const uint8_t* d_y, long long n, bool masked, cudaStream_t st)
+{
+    DevBuf<unsigned long long> m(6, st);
+    REGB_CK(launch_moments_u8(d_x, d_y, n, masked ? 1 : 0, m.p, st));
+    count_launch();
+    unsigned long long h[6];
+    REGB_CK(cudaMemcpyAsync(h, m.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    REGB_CK(cudaStreamSynchronize(st));
+    if (h[5] == 0)
+        return 0.0;
+    const double dn = (double)h[5], mx = (double)h[0] / dn, my = (double)h[1] / dn;
+    const double vx = (double)h[2] / dn - mx * mx, vy = (double)h[3] / dn - my * my;
+    const double sd1 = vx > 0.0 ? std::sqrt(vx) : 0.0, sd2 = vy > 0.0 ? std::sqrt(vy) : 0.0;
+    if (sd1 == 0 || sd2 == 0)
+        return 0.0;
+    return ((double)h[4] / dn - mx * my) / sd1 / sd2;
+}
+
 void subject_image_pre(const float* d_in, const int* dim, uint8_t* d_out, cudaStream_t st)
 {
     const long long n = (long long)dim[0] * dim[1] * dim[2];
