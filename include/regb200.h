@@ -213,6 +213,10 @@ regb_status regb_inv_displacement_to_mapping(const regb_field* inv_dis, const fl
 /* compose_mapping(from, mapping) (numerical/dif.hpp:70-90) of a uint8 volume: to(x) =
  * trilinear(from, mapping(x)), 0 where the 2x2x2 cell leaves from; to has the mapping's shape. */
 regb_status regb_compose_mapping(const regb_volume* from, const regb_field* mapping, regb_volume* to, void* stream);
+/* It_match_fov (reg/mm_reg.hpp:313-329): a copy of the uint8 template It with 0 wherever
+ * T (template voxel -> subject voxel) lands outside a subject volume of moving_dim. */
+regb_status regb_match_fov(const regb_volume* It, const float T[12], const int moving_dim[3], regb_volume* out,
+                           void* stream);
 /* correlation(x, y) (numerical/statistics.hpp:585-598) of two uint8 volumes of one shape:
  * Pearson r from exact integer moments, 0 when either is constant; masked != 0 gives
  * correlation_ygz (:600-619), over the voxels with y > 0 only (mm_reg's default r). */
@@ -313,6 +317,13 @@ typedef struct {
                                   255.999) unless already uint8; 1: subject_image_pre (gaussian +
                                   Otsu-median normalisation, reg/mm_reg.hpp:14-20) -- then the whole
                                   job runs on uint8 like the mm_reg pipeline */
+    int mm_reg;                /* 1: the rest of the mm_reg pipeline (reg/mm_reg.hpp:286-416) after a
+                                  uint8 CDM: the reverse CDM (subject on the template grid against the
+                                  template), the mappings, and the linear / nonlinear correlations
+                                  (correlation_ygz) in the result */
+    float* field_rev_out;      /* optional: the reverse displacement (template dims x 3 floats) */
+    float* mapping_out;        /* optional: template grid -> subject voxel mapping (template dims x 3) */
+    float* inv_mapping_out;    /* optional: subject grid -> template voxel mapping (moving dims x 3) */
 } regb_job;
 
 typedef struct {
@@ -324,6 +335,9 @@ typedef struct {
     int cdm_iterations;
     double queued_ms;          /* submit -> start */
     double run_ms;             /* start -> done */
+    int cdm_rev_ok;            /* mm_reg: 1 when the reverse CDM returned true */
+    double r_linear;           /* mm_reg: correlation_ygz(affine-resampled subject, template) */
+    double r_nonlinear;        /* mm_reg: correlation_ygz(subject through the mapping, template) */
 } regb_result;
 
 typedef struct {

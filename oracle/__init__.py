@@ -87,6 +87,12 @@ class _Lib:
                                        _ptr(out))
         return out
 
+    def match_fov(self, It, T, moving_shape):
+        out = np.zeros(It.shape, np.uint8)
+        self.lib.orc_match_fov_u8(_ptr(_u8(It)), _ptr(_dims(It.shape)), _ptr(_f32(T)), _ptr(_dims(moving_shape)),
+                                  _ptr(out))
+        return out
+
     def correlation(self, x, y, masked=False):
         f = self._fn("correlation_ygz_u8" if masked else "correlation_u8")
         f.restype = C.c_double

@@ -73,6 +73,7 @@ void orc_inv_displacement_to_mapping_f32(const float* inv_dis, const int* dis_di
 void orc_compose_mapping_u8(const uint8_t* from, const int* fdim, const float* mapping, const int* mdim, uint8_t* to);
 double orc_correlation_u8(const uint8_t* x, const uint8_t* y, long long n);
 double orc_correlation_ygz_u8(const uint8_t* x, const uint8_t* y, long long n);
+void orc_match_fov_u8(const uint8_t* It, const int* fdim, const float* T, const int* mdim, uint8_t* out);
 void orc_gaussian_f32(float* img, const int* dim, int bandwidth);
 float orc_otsu_threshold_f32(const float* img, long long n);
 float orc_median_f32(const float* v, long long n);

@@ -95,3 +95,21 @@ double orc_correlation_ygz_u8(const uint8_t* x, const uint8_t* y, long long n)
     free(ny);
     return r;
 }
+
+/* It_match_fov (reg/mm_reg.hpp:313-329): 0 where T(x) is outside a volume of mdim
+ * (shape::is_valid, utility/shape.hpp:116-122) */
+void orc_match_fov_u8(const uint8_t* It, const int* fdim, const float* T, const int* mdim, uint8_t* out)
+{
+    size_t i = 0;
+    for (int z = 0; z < fdim[2]; ++z)
+        for (int y = 0; y < fdim[1]; ++y)
+            for (int x = 0; x < fdim[0]; ++x, ++i) {
+                float p[3];
+                apply_T_u8(T, (float)x, (float)y, (float)z, p);
+                int ok = 1;
+                for (int a = 0; a < 3; ++a)
+                    if (p[a] < 0 || p[a] >= (float)(unsigned)mdim[a])
+                        ok = 0;
+                out[i] = ok ? It[i] : 0;
+            }
+}

@@ -185,3 +185,39 @@ def test_mm_reg_pipeline_job_equals_plain():
     assert r["status"] == 0 and r["cdm_ok"] == ok
     assert r["linear_cost"] == np.float32(cost) and np.array_equal(r["arg"].view(np.uint32), arg.view(np.uint32))
     assert np.array_equal(field.view(np.uint32), want.view(np.uint32))
+
+
+def test_mm_reg_job_outputs_equal_plain_calls(orc):
+    """mm_reg = 1: after the affine stage, linear r (correlation_ygz), It_match_fov, the
+    forward and reverse CDM run side by side, the two mappings and the nonlinear r
+    (reg/mm_reg.hpp:271-416) -- every output equals the plain calls bit for bit."""
+    rng = np.random.default_rng(ph.seed_for(5, 10))
+    t = ph.class_phantom((36, 40, 34), rng)
+    s = (32, 44, 30)
+    p = ph.random_affine(rng, rot_deg=6, trans_vox=2)
+    T0 = ph.affine_matrix_f32(p, s, (1, 1, 1), s, (1, 1, 1))
+    m = ph.rician(ph.apply_matrix(ph.class_phantom(s, rng), T0, s), rng)
+    q_t, _ = tb.normalize_to_u8(t)
+    q_m = tb.subject_image_pre(m)
+    cost, arg, _ = tb.reg.linear(q_t, (1, 1, 1), q_m, (1, 1, 1))
+    T = tb.affine_to_matrix(arg, t.shape, (1, 1, 1), m.shape, (1, 1, 1))
+    J = tb.resample(q_m, t.shape, T, allow_shift_copy=True)
+    r_lin = tb.correlation(J, q_t, masked=True)
+    It2 = tb.match_fov(q_t, T, m.shape)
+    assert np.array_equal(It2, orc.match_fov(q_t, T, m.shape))
+    t2f, ok = tb.reg.cdm(It2, J)
+    f2t, ok_rev = tb.reg.cdm(J, It2)
+    to2from = tb.displacement_to_mapping(t2f, T)
+    from2to = tb.inv_displacement_to_mapping(f2t, T, m.shape)
+    r_nl = tb.correlation(tb.compose_mapping(q_m, to2from), It2, masked=True)
+    out = {k: np.zeros(t.shape + (3,), np.float32) for k in ("f", "rev", "map")}
+    inv = np.zeros(m.shape + (3,), np.float32)
+    with tb.Engine() as eng:
+        tid = eng.add_template(t)
+        r = eng.wait(eng.submit(m, template=tid, cdm=True, subject_pre=True, mm_reg=True, field_out=out["f"],
+                                field_rev_out=out["rev"], mapping_out=out["map"], inv_mapping_out=inv))
+    assert r["status"] == 0 and r["cdm_ok"] == ok and r["cdm_rev_ok"] == ok_rev
+    assert r["linear_cost"] == np.float32(cost) and np.array_equal(r["arg"], arg)
+    assert r["r_linear"] == r_lin and r["r_nonlinear"] == r_nl and r_nl > r_lin
+    for got, want in ((out["f"], t2f), (out["rev"], f2t), (out["map"], to2from), (inv, from2to)):
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))

@@ -216,6 +216,15 @@ def compose_mapping(img, mapping, stream=None):
     return out
 
 
+def match_fov(It, T, moving_shape, stream=None):
+    """mm_reg's It_match_fov: It with 0 where T(x) falls outside a volume of moving_shape."""
+    out = _like(It, It.shape)
+    md = (C.c_int * 3)(*[int(v) for v in (moving_shape[2], moving_shape[1], moving_shape[0])])
+    _lib.check(_lib.lib().regb_match_fov(C.byref(_vol(It)), _fptr(np.ascontiguousarray(T, np.float32)), md,
+                                         C.byref(_vol(out)), _stream(stream)))
+    return out
+
+
 def correlation(x, y, masked=False) -> float:
     """Pearson r of two uint8 volumes (exact integer moments); masked: over y > 0 only."""
     r = C.c_double(0.0)
@@ -430,7 +439,8 @@ class Engine:
 
     def submit(self, moving, moving_vs=(1.0, 1.0, 1.0), template=None, fixed=None, fixed_vs=(1.0, 1.0, 1.0),
                linear=True, linear_param: LinearParam | None = None, arg=None, cdm=False,
-               cdm_param: CdmParam | None = None, field_out=None, subject_pre=False) -> int:
+               cdm_param: CdmParam | None = None, field_out=None, subject_pre=False, mm_reg=False,
+               field_rev_out=None, mapping_out=None, inv_mapping_out=None) -> int:
         L = _lib.lib()
         j = _lib.Job()
         L.regb_job_default(C.byref(j))
@@ -451,6 +461,7 @@ class Engine:
             j.arg[:] = [float(v) for v in arg]
         j.run_cdm = int(bool(cdm))
         j.subject_pre = int(bool(subject_pre))
+        j.mm_reg = int(bool(mm_reg))
         if cdm_param is not None:
             j.cdm = cdm_param
         if field_out is not None:
@@ -462,6 +473,14 @@ class Engine:
                 j.field_out = field_out.ctypes.data
                 j.field_location = _lib.HOST
             keep.append(field_out)
+        for name, buf in (("field_rev_out", field_rev_out), ("mapping_out", mapping_out),
+                          ("inv_mapping_out", inv_mapping_out)):
+            if buf is not None:
+                # same location as field_out (host numpy or device tensor)
+                setattr(j, name, buf.data_ptr() if _is_dev(buf) else buf.ctypes.data)
+                if field_out is None:
+                    j.field_location = _lib.DEVICE if _is_dev(buf) else _lib.HOST
+                keep.append(buf)
         jid = C.c_uint64(0)
         _lib.check(L.regb_engine_submit(self._h, C.byref(j), C.byref(jid)))
         self._keep[jid.value] = keep
@@ -471,7 +490,8 @@ class Engine:
     def _res(r):
         return {"status": r.status, "linear_cost": r.linear_cost, "arg": np.array(r.arg[:], np.float32),
                 "cost_evals": r.cost_evals, "cdm_ok": bool(r.cdm_ok), "cdm_iterations": r.cdm_iterations,
-                "queued_ms": r.queued_ms, "run_ms": r.run_ms}
+                "queued_ms": r.queued_ms, "run_ms": r.run_ms, "cdm_rev_ok": bool(r.cdm_rev_ok),
+                "r_linear": r.r_linear, "r_nonlinear": r.r_nonlinear}
 
     def poll(self, jid):
         r = _lib.Result()

@@ -64,13 +64,15 @@ class Job(C.Structure):
     _fields_ = [("template_id", C.c_int), ("fixed", Volume), ("fixed_vs", C.c_float * 3), ("moving", Volume),
                 ("moving_vs", C.c_float * 3), ("run_linear", C.c_int), ("linear", LinearParam),
                 ("arg", C.c_float * 12), ("run_cdm", C.c_int), ("cdm", CdmParam), ("field_out", C.c_void_p),
-                ("field_location", C.c_int), ("subject_pre", C.c_int)]
+                ("field_location", C.c_int), ("subject_pre", C.c_int), ("mm_reg", C.c_int),
+                ("field_rev_out", C.c_void_p), ("mapping_out", C.c_void_p), ("inv_mapping_out", C.c_void_p)]
 
 
 class Result(C.Structure):
     _fields_ = [("status", C.c_int), ("linear_cost", C.c_float), ("arg", C.c_float * 12),
                 ("cost_evals", C.c_longlong), ("cdm_ok", C.c_int), ("cdm_iterations", C.c_int),
-                ("queued_ms", C.c_double), ("run_ms", C.c_double)]
+                ("queued_ms", C.c_double), ("run_ms", C.c_double), ("cdm_rev_ok", C.c_int),
+                ("r_linear", C.c_double), ("r_nonlinear", C.c_double)]
 
 
 class EngineStats(C.Structure):
@@ -109,6 +111,7 @@ _SIGS = {
     "regb_displacement_to_mapping": (C.c_int, [C.c_void_p] * 4),
     "regb_inv_displacement_to_mapping": (C.c_int, [C.c_void_p] * 4),
     "regb_compose_mapping": (C.c_int, [C.c_void_p] * 4),
+    "regb_match_fov": (C.c_int, [C.c_void_p] * 5),
     "regb_correlation": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     "regb_subject_image_pre": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "regb_estimate_affine_param": (C.c_int, [C.c_void_p] * 5),

@@ -553,6 +553,29 @@ regb_status regb_compose_mapping(const regb_volume* from, const regb_field* mapp
     });
 }
 
+regb_status regb_match_fov(const regb_volume* It, const float T[12], const int moving_dim[3], regb_volume* out,
+                           void* stream)
+{
+    return guarded([&] {
+        check_vol(It, "It");
+        check_vol(out, "out");
+        if (!T || !moving_dim || It->dtype != REGB_U8 || out->dtype != REGB_U8 || !same_dims(It->dim, out->dim))
+            throw Failure(REGB_ERR_ARG, "match_fov: uint8 It and out of one shape, T, moving_dim");
+        check_dims(moving_dim, "moving_dim");
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t n = nvox(It->dim);
+        Staged a, o;
+        a.in(It->ptr, n, It->location, st, true);
+        o.in(out->ptr, n, out->location, st, false);
+        REGB_CK(launch_match_fov_u8((const uint8_t*)a.d, Dim3{It->dim[0], It->dim[1], It->dim[2]}, T,
+                                    Dim3{moving_dim[0], moving_dim[1], moving_dim[2]}, (uint8_t*)o.d, st));
+        count_launch();
+        o.out(out->ptr, st);
+        REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
 regb_status regb_correlation(const regb_volume* x, const regb_volume* y, int masked, double* r)
 {
     return guarded([&] {

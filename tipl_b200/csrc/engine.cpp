@@ -19,6 +19,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <exception>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -251,6 +252,8 @@ private:
                 if (k + 1 == lv.size() || lr[k] <= 1.0f)
                     worst = std::max(worst, lv[k]);
             b += worst * (60.0 + ps) + 0.3 * nf * ps;
+            if (j.mm_reg)  // the reverse CDM, the mappings, the composed subject
+                b += worst * (60.0 + ps) + 0.3 * nf * ps + 12.0 * nf + 12.0 * nf + 12.0 * nm + 2.0 * nf;
         }
         return (size_t)b + (16u << 20);
     }
@@ -430,16 +433,81 @@ private:
             DevBuf<float> field(3 * nf, st.s);
             int iters = 0;
             const void* It = pix ? (const void*)fixed_f32 : (s.subject_pre ? (const void*)fixed_u8 : d_fixed);
-            regb_status cs = cdm_register(It, Is.p, fdim, pix, field.p, s.cdm, &j->cancel, st.s, &iters, &sched_);
+            const uint8_t* I8 = s.subject_pre ? moving_u8 : (const uint8_t*)d_moving;  // uint8 subject (pix 0)
+            const bool mm = s.mm_reg && !pix;
+            // mm_reg: linear r (calculate_linear_r, reg/mm_reg.hpp:286-311, masked_r), and the
+            // reverse CDM -- cdm_common(J, It) beside cdm_common(It, J), reg/mm_reg.hpp:392-407
+            DevBuf<float> field_rev;
+            std::thread rev;
+            regb_status cs_rev = REGB_FALSE;
+            int iters_rev = 0;
+            std::exception_ptr rev_err;
+            DevBuf<uint8_t> It_fov;
+            if (mm) {
+                r.r_linear = correlation_u8(Is.p, (const uint8_t*)It, (long long)nf, true, st.s);
+                // It_match_fov (match_fov is on by default, reg/mm_reg.hpp:309-310): the
+                // template outside the subject's field of view is 0 for the nonlinear stage
+                It_fov.alloc(nf, st.s);
+                REGB_CK(launch_match_fov_u8((const uint8_t*)It, fdd, T, md, It_fov.p, st.s));
+                count_launch();
+                It = It_fov.p;
+                field_rev.alloc(3 * nf, st.s);
+                st.sync();  // Is and field_rev are ready before the reverse stream uses them
+                rev = std::thread([&] {
+                    try {
+                        Stream st2;
+                        cs_rev = cdm_register(Is.p, It, fdim, 0, field_rev.p, s.cdm, &j->cancel, st2.s, &iters_rev,
+                                              &sched_);
+                        st2.sync();
+                    } catch (...) {
+                        rev_err = std::current_exception();
+                    }
+                });
+            }
+            regb_status cs = REGB_FALSE;
+            std::exception_ptr fwd_err;
+            try {
+                cs = cdm_register(It, Is.p, fdim, pix, field.p, s.cdm, &j->cancel, st.s, &iters, &sched_);
+            } catch (...) {
+                fwd_err = std::current_exception();
+            }
+            if (rev.joinable())
+                rev.join();
+            if (fwd_err)
+                std::rethrow_exception(fwd_err);
+            if (rev_err)
+                std::rethrow_exception(rev_err);
             r.cdm_ok = (cs == REGB_OK) ? 1 : 0;
             r.cdm_iterations = iters;
-            if (cs == REGB_CANCELLED)
+            if (cs == REGB_CANCELLED || cs_rev == REGB_CANCELLED)
                 r.status = REGB_CANCELLED;
+            const cudaMemcpyKind kind =
+                s.field_location == REGB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
             if (s.field_out && cs != REGB_FALSE)
-                REGB_CK(cudaMemcpyAsync(s.field_out, field.p, sizeof(float) * 3 * nf,
-                                        s.field_location == REGB_DEVICE ? cudaMemcpyDeviceToDevice
-                                                                        : cudaMemcpyDeviceToHost,
-                                        st.s));
+                REGB_CK(cudaMemcpyAsync(s.field_out, field.p, sizeof(float) * 3 * nf, kind, st.s));
+            if (mm && r.status != REGB_CANCELLED) {
+                r.cdm_rev_ok = (cs_rev == REGB_OK) ? 1 : 0;
+                // compute_mapping_from_displacement (reg/mm_reg.hpp:271-284)
+                DevBuf<float> to2from(3 * nf, st.s), from2to(3 * nm, st.s);
+                REGB_CK(launch_displacement_to_mapping(field.p, fdd, T, to2from.p, st.s));
+                float iT[12];
+                std::memcpy(iT, T, sizeof(iT));
+                const bool inv_ok = matrix_inverse(iT);
+                if (inv_ok)
+                    REGB_CK(launch_inv_displacement_to_mapping(field_rev.p, fdd, iT, md, from2to.p, st.s));
+                count_launch(inv_ok ? 2 : 1);
+                // calculate_nonlinear_r (reg/mm_reg.hpp:330-345): the subject through the mapping
+                DevBuf<uint8_t> J2(nf, st.s);
+                REGB_CK(launch_compose_mapping_u8(I8, md, to2from.p, fdd, J2.p, st.s));
+                count_launch();
+                r.r_nonlinear = correlation_u8(J2.p, (const uint8_t*)It, (long long)nf, true, st.s);
+                if (s.field_rev_out && cs_rev != REGB_FALSE)
+                    REGB_CK(cudaMemcpyAsync(s.field_rev_out, field_rev.p, sizeof(float) * 3 * nf, kind, st.s));
+                if (s.mapping_out)
+                    REGB_CK(cudaMemcpyAsync(s.mapping_out, to2from.p, sizeof(float) * 3 * nf, kind, st.s));
+                if (s.inv_mapping_out && inv_ok)
+                    REGB_CK(cudaMemcpyAsync(s.inv_mapping_out, from2to.p, sizeof(float) * 3 * nm, kind, st.s));
+            }
             st.sync();
         }
         return r;
@@ -517,6 +585,7 @@ void regb_job_default(regb_job* j)
     j->arg[6] = j->arg[7] = j->arg[8] = 1.0f;
     j->field_location = REGB_HOST;
     j->subject_pre = 0;
+    j->mm_reg = 0;
 }
 
 regb_status regb_engine_create(const regb_engine_config* cfg, regb_engine** out)
@@ -561,6 +630,8 @@ regb_status regb_engine_submit(regb_engine* e, const regb_job* job, uint64_t* id
             throw Failure(REGB_ERR_ARG, "null argument");
         if (!vol_ok(job->moving) || (job->template_id < 0 && !vol_ok(job->fixed)))
             throw Failure(REGB_ERR_ARG, "bad fixed/moving volume");
+        if (job->mm_reg && !job->run_cdm)
+            throw Failure(REGB_ERR_ARG, "mm_reg needs run_cdm");
         *id = e->e->submit(*job);
         return REGB_OK;
     });

@@ -150,6 +150,8 @@ cudaError_t launch_compose_mapping_u8(const uint8_t* from, Dim3 FD, const float*
                                       cudaStream_t st);
 cudaError_t launch_moments_u8(const uint8_t* x, const uint8_t* y, long long n, int masked, unsigned long long* m,
                               cudaStream_t st);
+// out = It where T(x) lies inside a volume of shape MD, else 0 (mm_reg's It_match_fov)
+cudaError_t launch_match_fov_u8(const uint8_t* It, Dim3 FD, const float* T, Dim3 MD, uint8_t* out, cudaStream_t st);
 
 // Voxels > 0 per (x, y), (x, z), (y, z) line of a uint8 volume (zeroes the tables first).
 cudaError_t launch_mask_counts(const uint8_t* v, Dim3 dim, uint32_t* xy, uint32_t* xz, uint32_t* yz,

@@ -105,7 +105,33 @@ __global__ void __launch_bounds__(kMThreads) moments_u8_kernel(const uint8_t* __
     }
 }
 
+// It_match_fov (reg/mm_reg.hpp:313-329): template voxels whose transformed position is
+// outside the subject's volume (shape::is_valid, utility/shape.hpp:116-122) become 0
+__global__ void __launch_bounds__(kMThreads) match_fov_kernel(const uint8_t* __restrict__ It, Dim3 FD, Xform T,
+                                                               Dim3 MD, uint8_t* __restrict__ out)
+{
+    const long long n = FD.n();
+    for (long long i = (long long)blockIdx.x * kMThreads + threadIdx.x; i < n; i += (long long)gridDim.x * kMThreads) {
+        int x, y, z;
+        unflat((int)i, FD, x, y, z);
+        float p0, p1, p2;
+        apply_xform(T.m, (float)x, (float)y, (float)z, p0, p1, p2);
+        const bool ok = !(p0 < 0.0f || p0 >= (float)MD.w || p1 < 0.0f || p1 >= (float)MD.h || p2 < 0.0f ||
+                          p2 >= (float)MD.d);
+        out[i] = ok ? It[i] : (uint8_t)0;
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_match_fov_u8(const uint8_t* It, Dim3 FD, const float* T, Dim3 MD, uint8_t* out, cudaStream_t st)
+{
+    Xform X;
+    for (int k = 0; k < 12; ++k)
+        X.m[k] = T[k];
+    match_fov_kernel<<<mgrid(FD.n()), kMThreads, 0, st>>>(It, FD, X, MD, out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_displacement_to_mapping(const float* dis, Dim3 D, const float* T, float* mapping, cudaStream_t st)
 {
