@@ -45,6 +45,9 @@ FALLBACK_HBM_GBS = 6650.0
 # 12-candidate launch on the 182x218x182 pair (profiles/mi_kernel_affine_182x218x182.md:
 # 17.613568 MB / 86.65 M voxel evaluations); scaled to each bench launch by its voxels.
 MI_DRAM_BYTES_PER_VOXEL_EVAL = 17.613568e6 / (12 * 7221032)
+COST_NAME = {"mi": "MI", "mi32": "MI (32x32 bins)"}
+COST_DESC = {"mi": "MI 256x256 joint histogram (the reference's)",
+             "mi32": "MI 32x32 joint histogram (both volumes quantised to 0..31 by normalize_upper_lower2(31.99))"}
 
 
 def env_rank():
@@ -485,7 +488,8 @@ def kernel_case(args):
     rng = np.random.default_rng(1)
     Ts = np.array([tb.affine_to_matrix(ph.random_affine(rng, rot_deg=5, trans_vox=3), SHAPE, VS, SHAPE, VS)
                    for _ in range(args.k)], np.float32)
-    fn = tb.mi_cost if args.kernel_case == "mi" else tb.corr_cost
+    fn = {"mi": tb.mi_cost, "mi32": tb.mi32_cost, "corr": tb.corr_cost}[args.kernel_case]
+    is_mi = args.kernel_case != "corr"
     from tipl_b200 import _lib
 
     L = _lib.lib()
@@ -497,8 +501,8 @@ def kernel_case(args):
     st = _lib.Stats()
     L.regb_stats_get(st)
     torch.cuda.synchronize()
-    ms = (st.mi_ms / max(1, st.mi_launches)) if args.kernel_case == "mi" else (st.corr_ms / max(1, st.corr_launches))
-    vox = (st.mi_voxels / max(1, st.mi_launches)) if args.kernel_case == "mi" else (
+    ms = (st.mi_ms / max(1, st.mi_launches)) if is_mi else (st.corr_ms / max(1, st.corr_launches))
+    vox = (st.mi_voxels / max(1, st.mi_launches)) if is_mi else (
         st.corr_voxels / max(1, st.corr_launches))
     print(json.dumps({"kernel_case": args.kernel_case, "k": args.k, "cost0": float(c[0]), "ms_per_launch": ms,
                       "voxel_evals_per_s": vox / (ms / 1000.0)}))
@@ -543,15 +547,16 @@ def run_served(args, rank, world, dist):
     # the plain single-job path on the same subjects, one registration at a time
     fdev = torch.from_numpy(f8).cuda()
     t_plain = 0.0
+    lp = tb.reg.linear_param(cost_type=tb.reg.MI32 if args.cost == "mi32" else tb.reg.MI)
     if args.plain_steps:
-        tb.reg.linear(fdev, VS, dev_subj[0], VS)  # warm-up
+        tb.reg.linear(fdev, VS, dev_subj[0], VS, param=lp)  # warm-up
         for k in range(args.plain_steps):
             flush.fill_(1)
             torch.cuda.synchronize()
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record()
-            tb.reg.linear(fdev, VS, dev_subj[k % len(dev_subj)], VS)
+            tb.reg.linear(fdev, VS, dev_subj[k % len(dev_subj)], VS, param=lp)
             b.record()
             torch.cuda.synchronize()
             t_plain += a.elapsed_time(b) / 1000.0
@@ -561,7 +566,7 @@ def run_served(args, rank, world, dist):
     lat, costs, evals = [], [], 0
 
     def step(subj):
-        ids = [eng.submit(m, VS, template=tid) for m in subj]
+        ids = [eng.submit(m, VS, template=tid, linear_param=lp) for m in subj]
         return [eng.wait(i) for i in ids]
 
     for _ in range(args.warmup):
@@ -618,7 +623,9 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=3,
                     help="served mode: plain single-job registrations timed afterwards for the served/plain ratio")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel-case", choices=["mi", "corr", "cdm", "pre"], default=None,
+    ap.add_argument("--cost", choices=["mi", "mi32"], default="mi",
+                    help="served / plain affine cost: the reference's 256x256-bin MI, or the 32x32-bin variant")
+    ap.add_argument("--kernel-case", choices=["mi", "mi32", "corr", "cdm", "pre"], default=None,
                     help="run only K-candidate cost batches of the full-size pair (for profiler captures)")
     ap.add_argument("--k", type=int, default=12)
     ap.add_argument("--precision-report", action="store_true",
@@ -665,8 +672,10 @@ def main():
     md = torch.from_numpy(m8).cuda()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
+    lp = tb.reg.linear_param(cost_type=tb.reg.MI32 if args.cost == "mi32" else tb.reg.MI)
+
     def one(fx, mx):
-        return tb.reg.linear(fx, VS, mx, VS)
+        return tb.reg.linear(fx, VS, mx, VS, param=lp)
 
     for _ in range(args.warmup):
         one(fd, md)
@@ -722,12 +731,14 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "registrations/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-                "config": {"workload": "affine MI registration, 182x218x182 uint8 pair, 1 mm, one subject per step",
-                           "mode": args.mode, "cost": "MI 256x256 joint histogram",
+                "config": {"workload": f"affine {COST_NAME[args.cost]} registration, 182x218x182 uint8 pair, 1 mm, "
+                                       "one subject per step",
+                           "mode": args.mode, "cost": COST_DESC[args.cost],
                            "l2": "flushed between timed steps (256 MB write)",
                            "final_cost_mean": float(np.mean(costs)), "cost_evals_per_registration":
                                evals / max(1, args.steps), "parallelism": f"replicas x{world}"},
-                "roofline": {"bound": "hbm", "kernel": "mi_kernel", "achieved": achieved, "peak": hbm,
+                "roofline": {"bound": "hbm", "kernel": "mi32_kernel" if args.cost == "mi32" else "mi_kernel",
+                             "achieved": achieved, "peak": hbm,
                              "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
                              "traffic": MI_DRAM_BYTES_PER_VOXEL_EVAL * st.mi_voxels / max(1, st.mi_launches),
                              "traffic_note": "ncu DRAM bytes per voxel evaluation x this run's voxels per launch",
@@ -780,10 +791,10 @@ def served_line(args, rank, world, dist, torch):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
                 "data": "synthetic",
-                "config": {"workload": f"affine MI registration of {args.batch} subjects per step against one "
-                                       "resident 182x218x182 uint8 template, 1 mm, served+batched",
+                "config": {"workload": f"affine {COST_NAME[args.cost]} registration of {args.batch} subjects per "
+                                       "step against one resident 182x218x182 uint8 template, 1 mm, served+batched",
                            "mode": "served", "subjects_per_step": args.batch,
-                           "cost": "MI 256x256 joint histogram", "l2": "flushed between timed steps (256 MB write)",
+                           "cost": COST_DESC[args.cost], "l2": "flushed between timed steps (256 MB write)",
                            "final_cost_mean": float(np.mean(costs)) if costs else None,
                            "cost_evals_per_registration": evals / max(1, len(costs)),
                            "latency_ms": {"p50": pct(0.50), "p95": pct(0.95), "p99": pct(0.99)},
@@ -792,7 +803,8 @@ def served_line(args, rank, world, dist, torch):
                            "plain_single_job_registrations_per_s": plain,
                            "served_over_plain": (regs / t_dev / world) / plain if plain else None,
                            "parallelism": f"replicas x{world}"},
-                "roofline": {"bound": "hbm", "kernel": "mi_kernel", "achieved": achieved, "peak": hbm,
+                "roofline": {"bound": "hbm", "kernel": "mi32_kernel" if args.cost == "mi32" else "mi_kernel",
+                             "achieved": achieved, "peak": hbm,
                              "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
                              "traffic": MI_DRAM_BYTES_PER_VOXEL_EVAL * st.mi_voxels / max(1, st.mi_launches),
                              "traffic_note": "ncu DRAM bytes per voxel evaluation x this run's voxels per launch",

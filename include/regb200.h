@@ -59,7 +59,11 @@ typedef struct {
 typedef enum { REGB_REG_TRANSLOCATION = 1, REGB_REG_ROTATION = 2, REGB_REG_RIGID_BODY = 3,
                REGB_REG_SCALING = 4, REGB_REG_TRANSLOCATION_SCALING = 5, REGB_REG_RIGID_SCALING = 7,
                REGB_REG_TILT = 8, REGB_REG_AFFINE = 15 } regb_reg_type;
-typedef enum { REGB_COST_CORR = 0, REGB_COST_MI = 1 } regb_cost_type;
+/* REGB_COST_MI32: mutual information on a 32 x 32 joint histogram -- the reference's
+ * mutual_information with mi_band_width 5 (reg/linear.hpp:81-82, 174-203), both volumes
+ * quantised at every pyramid level by normalize_upper_lower2(v, 31.99) as it does for
+ * non-uint8 images.  The reference builds only the 256-bin form; this is a variant. */
+typedef enum { REGB_COST_CORR = 0, REGB_COST_MI = 1, REGB_COST_MI32 = 2 } regb_cost_type;
 typedef enum { REGB_BOUND_REG = 0, REGB_BOUND_NARROW = 1, REGB_BOUND_LARGE = 2 } regb_bound;
 
 /* linear_reg_param (reg/linear.hpp:268-288); bound selects reg_bound / narrow_bound /
@@ -174,6 +178,14 @@ regb_status regb_resample(const regb_volume* from, regb_volume* to, const float 
  * hist_out (optional, host, K*65536 int32) receives the joint histograms. */
 regb_status regb_mi_cost(const regb_volume* fixed, const regb_volume* moving, const float* T, int K,
                          double* cost, int32_t* hist_out, void* stream);
+/* No counterpart in the reference: the same MI on a 32x32 joint histogram
+ * (REGB_COST_MI32).  Both volumes are first quantised to 0..31 by
+ * normalize_upper_lower2(v, 31.99) (the reference's step for non-uint8 inputs,
+ * reg/linear.hpp:195-196); bin = (fixed << 5) + moving sample; the cost is
+ * -sum(mu log(mu / row / col)) / 1024 (reg/linear.hpp:87-104 with 32 bins).
+ * hist_out (optional, host, K*1024 int32) receives the joint histograms. */
+regb_status regb_mi32_cost(const regb_volume* fixed, const regb_volume* moving, const float* T, int K,
+                           double* cost, int32_t* hist_out, void* stream);
 /* No counterpart in the reference.  The MI cost of regb_mi_cost for callers that
  * cannot allocate device memory -- a processing callback inside a host application
  * that owns all device memory through its own pool, or a latency-critical loop that

@@ -166,6 +166,7 @@ class Oracle(_Lib):
         L = self.lib
         L.orc_mi_cost_from_hist.restype = C.c_double
         L.orc_mi_cost_u8.restype = C.c_double
+        L.orc_mi32_cost_u8.restype = C.c_double
         L.orc_corr_cost_u8.restype = C.c_double
         L.orc_mi_cost_u8_f64.restype = C.c_double
         L.orc_corr_cost_u8_f64.restype = C.c_double
@@ -239,6 +240,14 @@ class Oracle(_Lib):
     def mi_cost(self, fixed, moving, T) -> float:
         return self.lib.orc_mi_cost_u8(_ptr(_u8(fixed)), _ptr(_dims(fixed.shape)), _ptr(_u8(moving)),
                                        _ptr(_dims(moving.shape)), _ptr(_f32(T)))
+
+    def mi32_cost(self, fixed, moving, T, with_hist=False):
+        """MI on a 32x32 joint histogram of the volumes quantised to 0..31; with_hist
+        also returns the 1024 joint counts."""
+        h = np.zeros(1024, np.int32)
+        c = self.lib.orc_mi32_cost_u8(_ptr(_u8(fixed)), _ptr(_dims(fixed.shape)), _ptr(_u8(moving)),
+                                      _ptr(_dims(moving.shape)), _ptr(_f32(T)), _ptr(h))
+        return (c, h) if with_hist else c
 
     def mi_cost_f64(self, fixed, moving, T64) -> float:
         """MI cost with the transform and interpolation in double (error reporting)."""

@@ -271,6 +271,7 @@ int orc_is_integer_shift(const float* T, int* shift)
     }
 ORC_NORMALIZE(orc_normalize_to_u8_f32, float)
 ORC_NORMALIZE(orc_normalize_to_u8_u16, uint16_t)
+ORC_NORMALIZE(orc_normalize_to_u8_u8, uint8_t)
 #undef ORC_NORMALIZE
 
 /* ---- mapping steps of the mm_reg pipeline --------------------------------- */
@@ -346,6 +347,62 @@ double orc_mi_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, c
     double c = orc_mi_cost_from_hist(hist, fh);
     free(hist);
     return c;
+}
+
+/* MI on a 32x32 joint histogram.  No counterpart in the reference, whose
+ * mi_band_width is fixed at 8 (reg/linear.hpp:84-85); these are its
+ * mutual_information steps (reg/linear.hpp:173-203) with 5 bits:
+ *   - both volumes quantised by normalize_upper_lower2(v, 32 - 0.01f) (:195-196,
+ *     the reference's step for non-uint8 inputs); a constant volume becomes all 0;
+ *   - from_hist = histogram(from, 0, 31, 32) (:198, numerical/basic_op.hpp:1293-1311);
+ *   - H[(from[x] << 5) + to(T x)]++ with the uint8 trilinear sample (:138-146);
+ *   - -sum(n ln(n / row / col)) / 1024 (:87-104).
+ * hist (optional, 1024 entries) receives H. */
+double orc_mi32_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T,
+                        int32_t* hist)
+{
+    const long long nf = (long long)fdim[0] * fdim[1] * fdim[2], nt = (long long)tdim[0] * tdim[1] * tdim[2];
+    uint8_t* qf = (uint8_t*)calloc((size_t)(nf > 0 ? nf : 1), 1);
+    uint8_t* qt = (uint8_t*)calloc((size_t)(nt > 0 ? nt : 1), 1);
+    const float upper = 32.0f - 0.01f;
+    orc_normalize_to_u8_u8(from, nf, qf, upper);
+    orc_normalize_to_u8_u8(to, nt, qt, upper);
+    int32_t fh[32], H[1024];
+    const float range = 32.0f / 31.0f;
+    memset(fh, 0, sizeof(fh));
+    for (long long i = 0; i < nf; ++i) {
+        int b = (int)floorf((float)qf[i] * range);
+        if (b < 0) b = 0;
+        if (b > 31) b = 31;
+        ++fh[b];
+    }
+    memset(H, 0, sizeof(H));
+    size_t i = 0;
+    for (int z = 0; z < fdim[2]; ++z)
+        for (int y = 0; y < fdim[1]; ++y)
+            for (int x = 0; x < fdim[0]; ++x, ++i) {
+                float p[3];
+                apply_T_u8(T, (float)x, (float)y, (float)z, p);
+                uint8_t v = 0;
+                trilinear_u8(qt, tdim, p[0], p[1], p[2], &v);
+                ++H[((uint32_t)qf[i] << 5) + v];
+            }
+    uint32_t col[32];
+    memset(col, 0, sizeof(col));
+    for (int k = 0; k < 1024; ++k)
+        col[k & 31] += (uint32_t)H[k];
+    double sum = 0.0;
+    for (int k = 0; k < 1024; ++k) {
+        double mu = H[k];
+        if (mu == 0.0f)
+            continue;
+        sum += mu * log(mu / (double)fh[k >> 5] / (double)col[k & 31]);
+    }
+    if (hist)
+        memcpy(hist, H, sizeof(H));
+    free(qf);
+    free(qt);
+    return -(sum / (double)1024.0f);
 }
 
 /* ---- FP64 restatement of the affine costs (error reporting only) ----------

@@ -33,6 +33,9 @@ void orc_mi_hist_u8(const uint8_t* from, const int* fdim, const uint8_t* to, con
                     int32_t* hist);
 double orc_mi_cost_from_hist(const int32_t* hist, const int32_t* from_hist);
 double orc_mi_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T);
+/* MI on a 32x32 joint histogram of the volumes quantised to 0..31; hist: optional, 1024 */
+double orc_mi32_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T,
+                        int32_t* hist);
 double orc_corr_cost_u8(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const float* T);
 double orc_mi_cost_u8_f64(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const double* T);
 double orc_corr_cost_u8_f64(const uint8_t* from, const int* fdim, const uint8_t* to, const int* tdim, const double* T);
@@ -67,6 +70,7 @@ int orc_cdm_level_f64(const double* It, const double* Is, const int* dim, double
 
 int orc_normalize_to_u8_f32(const float* in, long long n, uint8_t* out, float upper);
 int orc_normalize_to_u8_u16(const uint16_t* in, long long n, uint8_t* out, float upper);
+int orc_normalize_to_u8_u8(const uint8_t* in, long long n, uint8_t* out, float upper);
 void orc_displacement_to_mapping_f32(const float* dis, const int* dim, const float* T, float* mapping);
 void orc_inv_displacement_to_mapping_f32(const float* inv_dis, const int* dis_dim, const float* T,
                                          const int* map_dim, float* inv_mapping);

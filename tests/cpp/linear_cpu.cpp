@@ -5,7 +5,7 @@
 // the optimiser's host logic can be checked against the reference's linear() without
 // a GPU.  The oracle is the checker here; nothing in the library calls it.
 //
-//   linear_cpu <w> <h> <d> <from.u8> <w> <h> <d> <to.u8> <cost: 1 MI | 2 corr>
+//   linear_cpu <w> <h> <d> <from.u8> <w> <h> <d> <to.u8> <cost: 0 corr | 1 MI | 2 MI32>
 //              <bound: 0 reg | 1 narrow | 2 large> <out.bin> [12 initial parameters]
 // out.bin: float cost, float arg[12], int64 evals.
 #include <cstdio>
@@ -150,8 +150,9 @@ int main(int argc, char** argv)
         for (int t = 0; t < nt; ++t)
             th.emplace_back([&, t] {
                 for (int k = t; k < n; k += nt)
-                    c[k] = cost_type == REGB_COST_MI ? orc_mi_cost_u8(L.from, L.fd, L.to, L.td, T + 12 * k)
-                                                     : orc_corr_cost_u8(L.from, L.fd, L.to, L.td, T + 12 * k);
+                    c[k] = cost_type == REGB_COST_MI     ? orc_mi_cost_u8(L.from, L.fd, L.to, L.td, T + 12 * k)
+                           : cost_type == REGB_COST_MI32 ? orc_mi32_cost_u8(L.from, L.fd, L.to, L.td, T + 12 * k, nullptr)
+                                                         : orc_corr_cost_u8(L.from, L.fd, L.to, L.td, T + 12 * k);
             });
         for (auto& t : th)
             t.join();

@@ -31,7 +31,7 @@ def save(name, **arrays):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=os.environ.get("TIPL_REF_ROOT", oracle.DEFAULT_REF_ROOT))
-    ap.add_argument("--only", default=None, help="make one fixture group: core | mask_init")
+    ap.add_argument("--only", default=None, help="make one fixture group: core | mask_init | precision | preprocess | linear_runs | mapping | mi32")
     args = ap.parse_args()
     oracle.build(args.ref_root, with_ref=True)
     R = oracle.Reference()
@@ -48,6 +48,39 @@ def main():
         linear_runs(R)
     if args.only in (None, "mapping"):
         mapping(R)
+    if args.only in (None, "mi32"):
+        mi32(R)
+
+
+def mi32(R):
+    """The 32x32-bin MI variant through the reference's own steps: normalize_upper_lower2
+    to 31.99 (the uint16 instantiation; uint8 values widen exactly), then the reference's
+    256x256 get_mutual_info / get_mutual_info_mean on the quantised volumes.  With values
+    0..31 every non-zero bin lies in the top-left 32x32 block, in the same order, so the
+    32x32 histogram is that block and the 32-bin cost is the 256-bin cost times 64 (the
+    mean is over 1024 instead of 65536 bins; both scalings are exact)."""
+    rng = np.random.default_rng(ph.seed_for(2, 32))
+    out = {}
+    for k, (fs, ms) in enumerate([((30, 34, 28), (32, 30, 29)), ((23, 19, 27), (23, 19, 27)),
+                                  ((1, 20, 24), (1, 22, 24))]):
+        if fs[0] > 1:
+            t = ph.class_phantom(fs, rng)
+            m = ph.rician(ph.class_phantom(ms, rng), rng)
+            f8, m8 = ph.normalize_to_u8(t), ph.normalize_to_u8(m)
+        else:
+            f8 = (rng.random(fs) * 256).astype(np.uint8)
+            m8 = (rng.random(ms) * 200 + 40).astype(np.uint8)
+        Ts = [np.array([1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0], np.float32)]
+        for _ in range(3):
+            p = ph.random_affine(rng, rot_deg=8, trans_vox=3)
+            Ts.append(R.affine_to_matrix(p, fs, (1, 1, 1), ms, (1, 1, 1)))
+        qf = R.normalize_u16_to_u8(f8.astype(np.uint16), 32.0 - 0.01)
+        qm = R.normalize_u16_to_u8(m8.astype(np.uint16), 32.0 - 0.01)
+        out[f"c{k}_fixed"], out[f"c{k}_moving"] = f8, m8
+        out[f"c{k}_T"] = np.array(Ts, np.float32)
+        out[f"c{k}_hist"] = np.array([R.mi_hist(qf, qm, T).reshape(256, 256)[:32, :32].ravel() for T in Ts], np.int32)
+        out[f"c{k}_cost"] = np.array([R.mi_cost(qf, qm, T) * 64.0 for T in Ts], np.float64)
+    save("mi32", **out)
 
 
 def mapping(R):
@@ -189,7 +222,7 @@ def mask_init(R):
     starts = np.array([[0, 0, 0, 0, 0, 0, 1, 1, 1, 0, 0, 0],
                        [1, 0.5, -0.5, 0.05, 0.02, -0.03, 1.02, 0.97, 1.0, 0.01, 0, -0.01]], np.float32)
     narrow = [R.linear_bound(f8, (1, 1, 1), m8, (1, 1, 1), arg=st, bound=1, cost_type=ct)
-              for st in starts for ct in (1, 2)]
+              for st in starts for ct in (1, 0)]
     R.set_threads(1)
     save("mask_init", vols=flat, shapes=shapes, has=has, pairs=np.array(pairs, np.int32),
          vs=np.array(vss, np.float32), est=np.array(est, np.float32), T=np.array(Ts, np.float32),

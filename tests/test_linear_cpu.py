@@ -44,7 +44,7 @@ def test_narrow_bound_bit_exact(harness, golden, tmp_path):
     g = golden("mask_init")
     k = 0
     for st in g["narrow_start"]:
-        for cost in (1, 2):
+        for cost in (1, 0):  # MI, correlation
             c, a = run(harness, tmp_path, g["lin_fixed"], g["lin_moving"], cost, 1, st)
             assert c.view(np.uint32) == g["narrow_cost"][k].view(np.uint32), (cost, c, g["narrow_cost"][k])
             assert np.array_equal(a.view(np.uint32), g["narrow_arg"][k].view(np.uint32))

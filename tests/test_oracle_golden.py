@@ -51,6 +51,19 @@ def test_affine_costs(orc, golden):
         assert orc.corr_cost(m, f, T) == cs  # roles swapped, transform inverted
 
 
+@pytest.mark.parametrize("ci", range(3))
+def test_mi32_variant(orc, golden, ci):
+    """32x32-bin MI: joint counts bit-exact and the cost equal to the reference's own
+    steps (quantisation to 31.99, its 256-bin MI on the quantised volumes, times 64)."""
+    g = golden("mi32")
+    f, m = g[f"c{ci}_fixed"], g[f"c{ci}_moving"]
+    for T, h, c in zip(g[f"c{ci}_T"], g[f"c{ci}_hist"], g[f"c{ci}_cost"]):
+        cost, hist = orc.mi32_cost(f, m, T, with_hist=True)
+        assert same(hist, h)
+        assert int(hist.sum()) == f.size
+        assert cost == c
+
+
 @pytest.mark.parametrize("ci", range(4))
 def test_cdm_passes(orc, golden, ci):
     g = golden("cdm_passes")

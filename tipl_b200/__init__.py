@@ -12,7 +12,8 @@ tipl::reg::cdm_common          ``reg.cdm(It, Is, param)``
 tipl::resample                 ``resample(src, out_shape, T)``
 tipl::compose_displacement     ``compose_displacement(src, dis)``
 tipl::accumulate_displacement  ``accumulate_displacement(dis, new_dis)``
-mutual_information / corr      ``mi_cost`` / ``corr_cost`` (K transforms at once)
+mutual_information / corr      ``mi_cost`` / ``corr_cost`` (K transforms at once); ``mi32_cost``
+                               the 32x32-bin MI variant
 transformation_matrix(...)     ``affine_to_matrix(param, ...)``
 =============================  ===================================================
 
@@ -30,7 +31,7 @@ import numpy as np
 from . import _lib
 from ._lib import CdmParam, Field, LinearParam, RegbError, Volume  # noqa: F401
 
-__all__ = ["affine_to_matrix", "affine_to_matrix_f64", "matrix_inverse", "resample", "mi_cost", "corr_cost",
+__all__ = ["affine_to_matrix", "affine_to_matrix_f64", "matrix_inverse", "resample", "mi_cost", "mi32_cost", "corr_cost",
            "compose_displacement", "accumulate_displacement", "downsample", "upsample_field_x2", "cdm_gradient",
            "cdm_poisson", "cdm_max_length", "cdm_smooth", "reg", "Engine", "RegbError", "version"]
 
@@ -290,6 +291,19 @@ def mi_cost(fixed, moving, Ts, return_hist=False, stream=None):
     return (cost, hist) if return_hist else cost
 
 
+def mi32_cost(fixed, moving, Ts, return_hist=False, stream=None):
+    """-MI of the 32x32 joint histogram for each of K transforms, both volumes first
+    quantised to 0..31 by normalize_upper_lower2(v, 31.99) (a variant of the reference
+    MI functor, whose histogram is fixed at 256x256)."""
+    Tm = np.ascontiguousarray(Ts, np.float32).reshape(-1, 12)
+    K = Tm.shape[0]
+    cost = np.zeros(K, np.float64)
+    hist = np.zeros((K, 1024), np.int32) if return_hist else None
+    _lib.check(_lib.lib().regb_mi32_cost(C.byref(_vol(fixed)), C.byref(_vol(moving)), _fptr(Tm), K, _fptr(cost),
+                                         _fptr(hist) if hist is not None else None, _stream(stream)))
+    return (cost, hist) if return_hist else cost
+
+
 def corr_cost(fixed, moving, Ts, stream=None):
     """1 - r^2 for each of K transforms (reference correlation functor)."""
     Tm = np.ascontiguousarray(Ts, np.float32).reshape(-1, 12)
@@ -371,7 +385,7 @@ class reg:
     """tipl::reg entry points."""
 
     AFFINE, RIGID_BODY, TRANSLOCATION = 15, 3, 1
-    CORR, MI = 0, 1
+    CORR, MI, MI32 = 0, 1, 2  # MI32: the 32x32-bin MI variant
 
     @staticmethod
     def linear_param(reg_type=15, cost_type=1, bound=0, search_count=16, absolute_bound=1) -> LinearParam:

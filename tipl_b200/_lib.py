@@ -118,6 +118,8 @@ _SIGS = {
     "regb_resample": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p]),
     "regb_mi_cost": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p,
                                C.c_void_p, C.c_void_p]),
+    "regb_mi32_cost": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]),
     "regb_mi_cost_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                        C.c_void_p, C.c_void_p]),
     "regb_corr_cost": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_void_p, C.c_int, C.c_void_p,

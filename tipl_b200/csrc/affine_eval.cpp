@@ -50,7 +50,9 @@ void set_task_chunks(AffineTask& t, int cost_type)
         rpc = (rows + 147) / 148;
         rpc = std::max<long long>(rpc, (32768 + w - 1) / w);
         rpc = std::min<long long>(rpc, hi);
-    } else
+    } else if (cost_type == REGB_COST_MI32)
+        rpc = std::max<long long>(1, (8192 + w - 1) / w);  // small blocks, many per SM
+    else
         rpc = std::max<long long>(1, (32768 + w - 1) / w);
     t.chunk = (int)rpc;
     t.nchunk = (int)std::max<long long>(1, (rows + rpc - 1) / rpc);
@@ -64,7 +66,7 @@ void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, dou
         t.ticket = s.ticket.p + k;
         t.cost = s.cost.p + k;
         t.moments = s.moments.p + 3 * k;
-        t.hist = (cost_type == REGB_COST_MI) ? s.hist.p + (size_t)k * 65536 : nullptr;
+        t.hist = (cost_type != REGB_COST_CORR) ? s.hist.p + (size_t)k * 65536 : nullptr;
         max_chunks = std::max(max_chunks, t.nchunk);
     }
     REGB_CK(cudaMemcpyAsync(s.tasks.p, s.h_tasks.p, sizeof(AffineTask) * K, cudaMemcpyHostToDevice, st));
@@ -73,13 +75,16 @@ void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, dou
         const AffineTask& t = s.h_tasks.p[k];
         vox += (double)t.fd.n();
         // algorithmic bytes of one evaluation: the fixed grid and the sampled volume
-        // once each, plus the 256x256 int32 histogram written and read (MI)
-        bytes += (double)t.fd.n() + (double)t.md.n() + (cost_type == REGB_COST_MI ? 524288.0 : 0.0);
+        // once each, plus the int32 joint histogram written and read (MI: 256x256, MI32: 32x32)
+        bytes += (double)t.fd.n() + (double)t.md.n() +
+                 (cost_type == REGB_COST_MI ? 524288.0 : (cost_type == REGB_COST_MI32 ? 8192.0 : 0.0));
     }
     KernelTimer tm;
-    tm.begin(st, cost_type == REGB_COST_MI ? 0 : 1);
+    tm.begin(st, cost_type == REGB_COST_CORR ? 1 : 0);  // both MI forms count as MI
     if (cost_type == REGB_COST_MI)
         REGB_CK(launch_mi(s.tasks.p, K, max_chunks, st));
+    else if (cost_type == REGB_COST_MI32)
+        REGB_CK(launch_mi32(s.tasks.p, K, max_chunks, st));
     else
         REGB_CK(launch_corr(s.tasks.p, K, max_chunks, st));
     tm.end(st, K, vox, bytes);
@@ -97,6 +102,19 @@ AffineEvaluator::AffineEvaluator(const std::vector<Pair>& levels, int cost_type,
     for (size_t i = 0; i < levels.size(); ++i) {
         Lvl& L = lv_[i];
         L.p = levels[i];
+        if (cost_type == REGB_COST_MI32) {
+            // per level, normalize_upper_lower2(v, 31.99): values 0..31 (a constant volume stays 0)
+            DevBuf<unsigned> mm(2, st);
+            L.qf.alloc((size_t)L.p.fd.n(), st);
+            L.qt.alloc((size_t)L.p.td.n(), st);
+            L.qf.zero();
+            L.qt.zero();
+            REGB_CK(launch_normalize_to_u8(L.p.from, REGB_U8, L.p.fd.n(), kMi32Upper, L.qf.p, mm.p, st));
+            REGB_CK(launch_normalize_to_u8(L.p.to, REGB_U8, L.p.td.n(), kMi32Upper, L.qt.p, mm.p, st));
+            count_launch(4);
+            L.p.from = L.qf.p;
+            L.p.to = L.qt.p;
+        }
         const uint8_t* grid = L.p.from;
         long long n = L.p.fd.n();
         if (cost_type == REGB_COST_CORR && L.p.fd.n() > L.p.td.n()) {  // reg/linear.hpp:28-33
@@ -154,7 +172,7 @@ std::vector<double> AffineEvaluator::eval(int level, const float* T, int K)
         batcher_->eval(t.data(), K, cost_type_, out.data());
         return out;
     }
-    s_.ensure(K, cost_type_ == REGB_COST_MI, st_);
+    s_.ensure(K, cost_type_ != REGB_COST_CORR, st_);
     for (int k = 0; k < K; ++k)
         make_task(level, T + 12 * k, s_.h_tasks.p[k]);
     run_affine_tasks(s_, K, cost_type_, st_, out.data());

@@ -24,6 +24,9 @@ struct TaskScratch {
 
 class AffineBatcher;
 
+// normalize_upper_lower2 bound of the 32-bin MI: float(32) - 0.01f (reg/linear.hpp:195-196)
+constexpr float kMi32Upper = 32.0f - 0.01f;
+
 // Fills the scratch pointers of h_tasks[0..K), launches the MI or correlation
 // kernel for all of them, and copies the costs back (synchronises st).
 void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, double* out);
@@ -52,6 +55,7 @@ private:
     struct Lvl {
         Pair p;
         bool swap = false;  // correlation: the to-volume is the smaller one and becomes the grid
+        DevBuf<uint8_t> qf, qt;  // 32-bin MI: the level's volumes quantised to 0..31
         DevBuf<int32_t> row_hist;
         DevBuf<unsigned long long> sums;
         long long sx = 0, sxx = 0;

@@ -244,6 +244,109 @@ cudaError_t launch_mi(const AffineTask* d_tasks, int ntask, int max_chunks, cuda
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- MI, 32 x 32 bins
+// The same joint histogram with 5-bit bins (mi_band_width 5 of reg/linear.hpp:81-82):
+// both volumes hold values 0..31 (quantised per pyramid level by
+// normalize_upper_lower2(v, 31.99), as the reference's mutual_information does for
+// non-uint8 images, reg/linear.hpp:186-199), bin = (template << 5) + sample.  The
+// 1024-bin per-block histogram is 4 KB of shared memory, so blocks are small and many;
+// bin 0 is again recovered as the remainder.  Cost = -sum n ln(n / (row col)) / 1024.
+constexpr int kMi32Threads = 256;
+
+__global__ void __launch_bounds__(kMi32Threads) mi32_kernel(const AffineTask* __restrict__ tasks)
+{
+    __shared__ uint32_t sh[1024];
+    __shared__ uint32_t col[32];
+    __shared__ double red[32];
+    __shared__ unsigned long long tot;
+    __shared__ unsigned int last;
+    const AffineTask& tk = tasks[blockIdx.y];
+    const int chunk = blockIdx.x;
+    if (chunk >= tk.nchunk)
+        return;
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x)
+        sh[i] = 0u;
+    __syncthreads();
+    const Dim3 fd = tk.fd;
+    const SampleGeo g = sample_geo(tk.md);
+    const int rows = fd.h * fd.d;
+    const int r0 = chunk * tk.chunk, r1 = min(rows, r0 + tk.chunk);
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const float* __restrict__ T = tk.T;
+    ColXform cx;
+    cx.set(T);
+    for (int r = r0 + (threadIdx.x >> 5); r < r1; r += nw) {
+        RowXform xr;
+        xr.set(T, r % fd.h, r / fd.h);
+        const uint8_t* __restrict__ fr = tk.fixed + (long long)r * fd.w;
+        for (int x = lane; x < fd.w; x += 32) {
+            float px, py, pz;
+            xr.at(cx, (float)x, px, py, pz);
+            const uint32_t b = ((uint32_t)__ldg(fr + x) << 5) | sample_u8(tk.moving, g, px, py, pz);
+            if (b)
+                atomicAdd(sh + b, 1u);
+        }
+    }
+    __syncthreads();
+    uint32_t* __restrict__ gh = tk.hist;
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x)
+        if (sh[i])
+            atomicAdd(gh + i, sh[i]);
+    if (tk.keep)
+        return;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        last = (atomicAdd(tk.ticket, 1u) == (unsigned)tk.nchunk - 1u);
+    __syncthreads();
+    if (!last)
+        return;
+    __threadfence();
+    // reduction (reg/linear.hpp:87-104 with 32 x 32 bins); the block is the last one
+    const int t = threadIdx.x;
+    if (t < 32)
+        col[t] = 0u;
+    if (t == 0)
+        tot = 0ull;
+    __syncthreads();
+    for (int b = t; b < 1024; b += blockDim.x) {
+        const uint32_t v = __ldcg(gh + b);
+        sh[b] = v;
+        if (v) {
+            atomicAdd(col + (b & 31), v);
+            atomicAdd(&tot, (unsigned long long)v);
+        }
+    }
+    __syncthreads();
+    const uint32_t n00 = (uint32_t)(fd.n() - (long long)tot);
+    if (t == 0) {
+        sh[0] = n00;
+        col[0] += n00;
+    }
+    __syncthreads();
+    double acc = 0.0;
+    for (int b = t; b < 1024; b += blockDim.x) {
+        const uint32_t nb = sh[b];
+        if (nb) {
+            const double mu = (double)nb;
+            acc += mu * log(mu / (double)tk.row_hist[b >> 5] / (double)col[b & 31]);
+        }
+    }
+    acc = block_sum(acc, red);
+    if (t == 0) {
+        *tk.cost = -(acc / 1024.0);
+        *tk.ticket = 0u;
+    }
+    for (int b = t; b < 1024; b += blockDim.x)
+        gh[b] = 0u;
+}
+
+cudaError_t launch_mi32(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
+{
+    mi32_kernel<<<dim3(max_chunks, ntask), kMi32Threads, 0, st>>>(d_tasks);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- correlation
 // Exact integer moments of the resampled moving volume y against the fixed grid
 // x: sum y, sum y^2, sum x*y (the template's sum x and sum x^2 are per job).  A

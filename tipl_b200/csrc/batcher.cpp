@@ -24,8 +24,8 @@ AffineBatcher::~AffineBatcher()
     cv_req_.notify_all();
     if (th_.joinable())
         th_.join();
-    scratch_[0].release();
-    scratch_[1].release();
+    for (TaskScratch& s : scratch_)
+        s.release();
     if (st_) {
         cudaStreamSynchronize(st_);
         cudaStreamDestroy(st_);
@@ -51,6 +51,8 @@ void AffineBatcher::eval(const AffineTask* tasks, int n, int cost_type, double* 
 {
     if (n == 0)
         return;
+    if (cost_type < 0 || cost_type >= kCostTypes)
+        throw Failure(REGB_ERR_ARG, "unknown cost type");
     Req r{tasks, n, cost_type, out};
     std::unique_lock<std::mutex> lk(m_);
     pending_.push_back(&r);
@@ -73,7 +75,7 @@ void AffineBatcher::loop()
         std::vector<Req*> batch(pending_.begin(), pending_.end());
         pending_.clear();
         lk.unlock();
-        for (int ct = 0; ct < 2; ++ct) {
+        for (int ct = 0; ct < kCostTypes; ++ct) {
             int total = 0;
             for (Req* r : batch)
                 if (r->cost_type == ct)
@@ -82,7 +84,7 @@ void AffineBatcher::loop()
                 continue;
             try {
                 TaskScratch& s = scratch_[ct];
-                s.ensure(total, ct == REGB_COST_MI, st_);
+                s.ensure(total, ct != REGB_COST_CORR, st_);
                 int k = 0;
                 for (Req* r : batch)
                     if (r->cost_type == ct) {

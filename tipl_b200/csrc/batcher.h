@@ -10,6 +10,8 @@
 
 namespace regb {
 
+constexpr int kCostTypes = 3;  // REGB_COST_CORR, REGB_COST_MI, REGB_COST_MI32
+
 // Collects cost-evaluation requests from many jobs and evaluates all pending ones
 // of a cost type in one launch.  A request's tasks carry their own volumes, so
 // requests of different jobs, shapes and pyramid levels mix freely; every task's
@@ -48,7 +50,7 @@ private:
     bool stop_ = false;
     int gather_us_;
     long long launches_ = 0, tasks_ = 0;
-    TaskScratch scratch_[2];
+    TaskScratch scratch_[kCostTypes];  // one per cost type (REGB_COST_CORR, _MI, _MI32)
     cudaStream_t st_ = nullptr;
     std::thread th_;
 };

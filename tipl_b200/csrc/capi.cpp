@@ -410,9 +410,10 @@ static regb_status affine_cost(const regb_volume* fixed, const regb_volume* movi
         AffineEvaluator::Pair pr{(const uint8_t*)a.d, Dim3{fixed->dim[0], fixed->dim[1], fixed->dim[2]},
                                  (const uint8_t*)b.d, Dim3{moving->dim[0], moving->dim[1], moving->dim[2]}};
         AffineEvaluator ev({pr}, cost_type, st);
-        if (hist_out && cost_type == REGB_COST_MI) {
+        if (hist_out && cost_type != REGB_COST_CORR) {
             // histograms requested: evaluate one task at a time and read its counts
             // before the kernel's last block clears them.
+            const int nb = cost_type == REGB_COST_MI ? 65536 : 1024;
             TaskScratch s;
             s.ensure(1, true, st);
             PinBuf<uint32_t> h(65536);
@@ -425,16 +426,19 @@ static regb_status affine_cost(const regb_volume* fixed, const regb_volume* movi
                 t.hist = s.hist.p;
                 t.keep = 1;  // leave the counts in place for the read-back
                 REGB_CK(cudaMemcpyAsync(s.tasks.p, s.h_tasks.p, sizeof(AffineTask), cudaMemcpyHostToDevice, st));
-                REGB_CK(launch_mi(s.tasks.p, 1, t.nchunk, st));
-                REGB_CK(cudaMemcpyAsync(h.p, s.hist.p, 65536 * 4, cudaMemcpyDeviceToHost, st));
+                if (cost_type == REGB_COST_MI)
+                    REGB_CK(launch_mi(s.tasks.p, 1, t.nchunk, st));
+                else
+                    REGB_CK(launch_mi32(s.tasks.p, 1, t.nchunk, st));
+                REGB_CK(cudaMemcpyAsync(h.p, s.hist.p, (size_t)nb * 4, cudaMemcpyDeviceToHost, st));
                 REGB_CK(cudaStreamSynchronize(st));
                 // bin 0 is not counted on the device; it is the remainder
                 long long tot = 0;
-                for (int i = 1; i < 65536; ++i)
+                for (int i = 1; i < nb; ++i)
                     tot += h.p[i];
                 h.p[0] = (uint32_t)((long long)nvox(fixed->dim) - tot);
-                std::memcpy(hist_out + (size_t)k * 65536, h.p, 65536 * 4);
-                REGB_CK(cudaMemsetAsync(s.hist.p, 0, 65536 * 4, st));
+                std::memcpy(hist_out + (size_t)k * nb, h.p, (size_t)nb * 4);
+                REGB_CK(cudaMemsetAsync(s.hist.p, 0, (size_t)nb * 4, st));
             }
         }
         std::vector<double> c = ev.eval(0, T, K);
@@ -447,6 +451,12 @@ regb_status regb_mi_cost(const regb_volume* fixed, const regb_volume* moving, co
                          int32_t* hist_out, void* stream)
 {
     return affine_cost(fixed, moving, T, K, cost, hist_out, REGB_COST_MI, stream);
+}
+
+regb_status regb_mi32_cost(const regb_volume* fixed, const regb_volume* moving, const float* T, int K, double* cost,
+                           int32_t* hist_out, void* stream)
+{
+    return affine_cost(fixed, moving, T, K, cost, hist_out, REGB_COST_MI32, stream);
 }
 
 regb_status regb_corr_cost(const regb_volume* fixed, const regb_volume* moving, const float* T, int K, double* cost,
@@ -805,8 +815,8 @@ regb_status regb_linear(const regb_volume* from, const float from_vs[3], const r
         regb_linear_param_default(&p);
         if (param)
             p = *param;
-        if (p.cost_type != REGB_COST_MI && p.cost_type != REGB_COST_CORR)
-            throw Failure(REGB_ERR_ARG, "cost_type must be MI or CORR");
+        if (p.cost_type != REGB_COST_MI && p.cost_type != REGB_COST_CORR && p.cost_type != REGB_COST_MI32)
+            throw Failure(REGB_ERR_ARG, "cost_type must be MI, MI32 or CORR");
         Stream s;
         Staged a, b;
         a.in(from->ptr, nvox(from->dim), from->location, s.s, true);
@@ -849,8 +859,8 @@ regb_status regb_linear_run(const regb_volume* from, const float from_vs[3], con
             throw Failure(REGB_ERR_ARG, "linear takes uint8 volumes (reg/linear.hpp:622-629)");
         if (!from_vs || !to_vs || !arg || !state)
             throw Failure(REGB_ERR_ARG, "null voxel size / arg / state");
-        if (state->cost_type != REGB_COST_MI && state->cost_type != REGB_COST_CORR)
-            throw Failure(REGB_ERR_ARG, "cost_type must be MI or CORR");
+        if (state->cost_type != REGB_COST_MI && state->cost_type != REGB_COST_CORR && state->cost_type != REGB_COST_MI32)
+            throw Failure(REGB_ERR_ARG, "cost_type must be MI, MI32 or CORR");
         Stream s;
         Staged a, b;
         a.in(from->ptr, nvox(from->dim), from->location, s.s, true);

@@ -632,6 +632,9 @@ regb_status regb_engine_submit(regb_engine* e, const regb_job* job, uint64_t* id
             throw Failure(REGB_ERR_ARG, "bad fixed/moving volume");
         if (job->mm_reg && !job->run_cdm)
             throw Failure(REGB_ERR_ARG, "mm_reg needs run_cdm");
+        const int ct = job->linear.cost_type;
+        if (job->run_linear && ct != REGB_COST_CORR && ct != REGB_COST_MI && ct != REGB_COST_MI32)
+            throw Failure(REGB_ERR_ARG, "cost_type must be MI, MI32 or CORR");
         *id = e->e->submit(*job);
         return REGB_OK;
     });

@@ -85,6 +85,8 @@ cudaError_t launch_resample(const T* from, Dim3 fd, T* to, Dim3 td, const float*
                             cudaStream_t st);
 cudaError_t launch_mi(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
 cudaError_t launch_corr(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
+// 32 x 32-bin MI (volumes quantised to 0..31); hist: 1024 counters per task, zero on entry
+cudaError_t launch_mi32(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
 cudaError_t launch_fixed_stats(const uint8_t* f, long long n, int32_t* hist, unsigned long long* sums,
                                cudaStream_t st);
 
