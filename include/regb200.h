@@ -92,7 +92,7 @@ void regb_cdm_param_default(regb_cdm_param* p);
 const char* regb_version(void);
 const char* regb_last_error(void);   /* thread-local text of the last failure */
 regb_status regb_device_info(int* device, int* sm_count, size_t* free_bytes, size_t* total_bytes);
-/* Release every cached device buffer of this thread's context. */
+/* Release every cached device buffer of this thread's context and every cached page-locked host block. */
 regb_status regb_release(void);
 
 /* Launch accounting (no reference counterpart: instrumentation of this library).

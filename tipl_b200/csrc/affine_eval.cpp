@@ -2,6 +2,7 @@
 #include "batcher.h"
 #include "stats.h"
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 namespace regb {
@@ -38,6 +39,51 @@ void TaskScratch::release()
     cap = 0;
 }
 
+static bool tex_enabled()
+{
+    static const bool on = [] {
+        const char* e = std::getenv("REGB_MI_TEXTURE");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+void TexVol::reset()
+{
+    if (t)
+        cudaDestroyTextureObject(t);
+    t = 0;
+    mem.reset();
+}
+
+void TexVol::build(const uint8_t* v, Dim3 d, cudaStream_t st)
+{
+    reset();
+    // pitch-linear 2-D texture limits of sm_100 (131072 x 65000 texels), pitch in
+    // multiples of 32 bytes
+    const long long rows = (long long)d.h * d.d;
+    if (!tex_enabled() || d.w < 2 || rows < 2 || d.w > 131072 || rows > 65000)
+        return;
+    const size_t pitch = (((size_t)d.w * 2 + 31) / 32) * 32 / 2;  // in halves
+    mem.alloc(pitch * (size_t)rows, st);
+    REGB_CK(launch_u8_to_half_pitched(v, d.w, rows, mem.p, pitch, st));
+    cudaResourceDesc rd;
+    std::memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypePitch2D;
+    rd.res.pitch2D.devPtr = mem.p;
+    rd.res.pitch2D.desc = cudaCreateChannelDesc(16, 0, 0, 0, cudaChannelFormatKindFloat);
+    rd.res.pitch2D.width = (size_t)d.w;
+    rd.res.pitch2D.height = (size_t)rows;
+    rd.res.pitch2D.pitchInBytes = pitch * 2;
+    cudaTextureDesc td;
+    std::memset(&td, 0, sizeof(td));
+    td.addressMode[0] = td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    REGB_CK(cudaCreateTextureObject(&t, &rd, &td, nullptr));
+}
+
 void set_task_chunks(AffineTask& t, int cost_type)
 {
     // a chunk is a run of whole rows of the fixed grid
@@ -60,15 +106,21 @@ void set_task_chunks(AffineTask& t, int cost_type)
 
 void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, double* out)
 {
-    int max_chunks = 1;
+    int max_chunks = 1, max_chunks_tex = 1, ntex = 0;
     for (int k = 0; k < K; ++k) {
         AffineTask& t = s.h_tasks.p[k];
         t.ticket = s.ticket.p + k;
         t.cost = s.cost.p + k;
         t.moments = s.moments.p + 3 * k;
         t.hist = (cost_type != REGB_COST_CORR) ? s.hist.p + (size_t)k * 65536 : nullptr;
-        max_chunks = std::max(max_chunks, t.nchunk);
+        if (cost_type == REGB_COST_MI && t.tex) {
+            ++ntex;
+            max_chunks_tex = std::max(max_chunks_tex, t.nchunk);
+        } else
+            max_chunks = std::max(max_chunks, t.nchunk);
     }
+    if (ntex && ntex < K)  // texture tasks first (each task's outputs stay at its own index)
+        std::stable_partition(s.h_tasks.p, s.h_tasks.p + K, [](const AffineTask& t) { return t.tex != 0; });
     REGB_CK(cudaMemcpyAsync(s.tasks.p, s.h_tasks.p, sizeof(AffineTask) * K, cudaMemcpyHostToDevice, st));
     double vox = 0.0, bytes = 0.0;
     for (int k = 0; k < K; ++k) {
@@ -81,14 +133,17 @@ void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, dou
     }
     KernelTimer tm;
     tm.begin(st, cost_type == REGB_COST_CORR ? 1 : 0);  // both MI forms count as MI
-    if (cost_type == REGB_COST_MI)
-        REGB_CK(launch_mi(s.tasks.p, K, max_chunks, st));
-    else if (cost_type == REGB_COST_MI32)
+    if (cost_type == REGB_COST_MI) {
+        if (ntex)
+            REGB_CK(launch_mi_tex(s.tasks.p, ntex, max_chunks_tex, st));
+        if (ntex < K)
+            REGB_CK(launch_mi(s.tasks.p + ntex, K - ntex, max_chunks, st));
+    } else if (cost_type == REGB_COST_MI32)
         REGB_CK(launch_mi32(s.tasks.p, K, max_chunks, st));
     else
         REGB_CK(launch_corr(s.tasks.p, K, max_chunks, st));
     tm.end(st, K, vox, bytes);
-    count_launch();
+    count_launch(cost_type == REGB_COST_MI && ntex && ntex < K ? 2 : 1);
     REGB_CK(cudaMemcpyAsync(s.h_cost.p, s.cost.p, sizeof(double) * K, cudaMemcpyDeviceToHost, st));
     REGB_CK(cudaStreamSynchronize(st));
     std::memcpy(out, s.h_cost.p, sizeof(double) * K);
@@ -122,6 +177,8 @@ AffineEvaluator::AffineEvaluator(const std::vector<Pair>& levels, int cost_type,
             grid = L.p.to;
             n = L.p.td.n();
         }
+        if (cost_type == REGB_COST_MI)
+            L.tex.build(L.p.to, L.p.td, st);
         L.row_hist.alloc(256, st);
         L.sums.alloc(2, st);
         REGB_CK(launch_fixed_stats(grid, n, L.row_hist.p, L.sums.p, st));
@@ -154,6 +211,7 @@ void AffineEvaluator::make_task(int level, const float* T, AffineTask& t) const
     t.mode = 0;
     if (cost_type_ == REGB_COST_CORR && integer_shift(M, t.shift))
         t.mode = 1;  // the CPU resample's integer-shift copy
+    t.tex = (cost_type_ == REGB_COST_MI && !L.swap) ? (unsigned long long)L.tex.t : 0ull;
     t.row_hist = L.row_hist.p;
     t.sx = L.sx;
     t.sxx = L.sxx;

@@ -24,6 +24,31 @@ struct TaskScratch {
 
 class AffineBatcher;
 
+// A uint8 volume held as a (w, h*d) 2-D texture of halves for the MI kernel's
+// gathers (empty when the volume exceeds the pitch-linear texture limits).
+struct TexVol {
+    cudaTextureObject_t t = 0;
+    DevBuf<uint16_t> mem;
+    TexVol() = default;
+    TexVol(const TexVol&) = delete;
+    TexVol& operator=(const TexVol&) = delete;
+    TexVol(TexVol&& o) noexcept : t(o.t), mem(std::move(o.mem)) { o.t = 0; }
+    TexVol& operator=(TexVol&& o) noexcept
+    {
+        if (this != &o) {
+            reset();
+            t = o.t;
+            mem = std::move(o.mem);
+            o.t = 0;
+        }
+        return *this;
+    }
+    ~TexVol() { reset(); }
+    void reset();
+    // Builds the texture of v (device, dims d); leaves t = 0 when d does not fit.
+    void build(const uint8_t* v, Dim3 d, cudaStream_t st);
+};
+
 // normalize_upper_lower2 bound of the 32-bin MI: float(32) - 0.01f (reg/linear.hpp:195-196)
 constexpr float kMi32Upper = 32.0f - 0.01f;
 
@@ -56,6 +81,7 @@ private:
         Pair p;
         bool swap = false;  // correlation: the to-volume is the smaller one and becomes the grid
         DevBuf<uint8_t> qf, qt;  // 32-bin MI: the level's volumes quantised to 0..31
+        TexVol tex;              // MI: the moving volume as a texture (t = 0: byte loads)
         DevBuf<int32_t> row_hist;
         DevBuf<unsigned long long> sums;
         long long sx = 0, sxx = 0;

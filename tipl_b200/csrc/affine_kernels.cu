@@ -12,6 +12,7 @@
 // The last block of a task (ticket counter) reduces that task's counts to its
 // cost and clears the task's scratch, so the next launch finds it zeroed.
 #include <atomic>
+#include <cuda_fp16.h>
 #include "common.cuh"
 #include "stats.h"
 #include "kernels.h"
@@ -144,6 +145,7 @@ __device__ void mi_reduce_and_clear(uint32_t* __restrict__ hist, const int32_t* 
         hist[b] = 0u;
 }
 
+template <bool TEX>
 __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __restrict__ tasks)
 {
     extern __shared__ uint32_t sh[];
@@ -162,6 +164,7 @@ __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __r
     const int r0 = chunk * tk.chunk, r1 = min(rows, r0 + tk.chunk);
     const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const uint8_t* __restrict__ moving = tk.moving;
+    const float hf = (float)tk.md.h;
     const float* __restrict__ T = tk.T;
     ColXform cx;
     cx.set(T);
@@ -191,7 +194,10 @@ __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __r
             const uint32_t fva = __ldg(fa + x);
             const uint32_t fvb = two ? (uint32_t)__ldg(fb + x) : 0u;
             uint32_t ta, tb;
-            sample_u8_pair(moving, g, px, py, pz, true, two, ta, tb);
+            if constexpr (TEX)
+                sample_tex_pair((cudaTextureObject_t)tk.tex, g, hf, px, py, pz, true, two, ta, tb);
+            else
+                sample_u8_pair(moving, g, px, py, pz, true, two, ta, tb);
             mi_count(sh, (fva << 8) | ta);
             if (two)
                 mi_count(sh, (fvb << 8) | tb);
@@ -225,7 +231,8 @@ __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __r
         *tk.ticket = 0u;
 }
 
-cudaError_t launch_mi(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
+template <bool TEX>
+static cudaError_t launch_mi_impl(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
 {
     static std::atomic<unsigned long long> attr_set{0};  // one bit per device
     int dev = 0;
@@ -234,21 +241,53 @@ cudaError_t launch_mi(const AffineTask* d_tasks, int ntask, int max_chunks, cuda
         return e;
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(attr_set.load() & bit)) {
-        e = cudaFuncSetAttribute(mi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMiSmemWords * 4);
+        e = cudaFuncSetAttribute(mi_kernel<TEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMiSmemWords * 4);
         if (e != cudaSuccess)
             return e;
         attr_set.fetch_or(bit);
     }
     dim3 grid(max_chunks, ntask);
-    mi_kernel<<<grid, kMiThreads, kMiSmemWords * 4, st>>>(d_tasks);
+    mi_kernel<TEX><<<grid, kMiThreads, kMiSmemWords * 4, st>>>(d_tasks);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mi(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
+{
+    return launch_mi_impl<false>(d_tasks, ntask, max_chunks, st);
+}
+
+cudaError_t launch_mi_tex(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
+{
+    return launch_mi_impl<true>(d_tasks, ntask, max_chunks, st);
+}
+
+__global__ void __launch_bounds__(256) u8_to_half_kernel(const uint8_t* __restrict__ in, int w, long long rows,
+                                                         __half* __restrict__ out, size_t pitch)
+{
+    const long long n = (long long)w * rows;
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+        const long long r = i / w;
+        out[r * (long long)pitch + (i - r * w)] = __uint2half_rn((unsigned)in[i]);  // exact below 2048
+    }
+}
+
+cudaError_t launch_u8_to_half_pitched(const uint8_t* in, int w, long long rows, void* out, size_t pitch,
+                                      cudaStream_t st)
+{
+    const long long n = (long long)w * rows;
+    if (n == 0)
+        return cudaSuccess;
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    u8_to_half_kernel<<<blocks, 256, 0, st>>>(in, w, rows, (__half*)out, pitch);
+    count_launch();
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- MI, 32 x 32 bins
-// The same joint histogram with 5-bit bins (mi_band_width 5 of reg/linear.hpp:81-82):
-// both volumes hold values 0..31 (quantised per pyramid level by
-// normalize_upper_lower2(v, 31.99), as the reference's mutual_information does for
-// non-uint8 images, reg/linear.hpp:186-199), bin = (template << 5) + sample.  The
+// The same joint histogram with 5-bit bins (the reference fixes mi_band_width at 8,
+// reg/linear.hpp:84-85): both volumes hold values 0..31 (quantised per pyramid level
+// by normalize_upper_lower2(v, 31.99), the reference mutual_information's step for
+// non-uint8 images, reg/linear.hpp:190-197), bin = (template << 5) + sample.  The
 // 1024-bin per-block histogram is 4 KB of shared memory, so blocks are small and many;
 // bin 0 is again recovered as the remainder.  Cost = -sum n ln(n / (row col)) / 1024.
 constexpr int kMi32Threads = 256;

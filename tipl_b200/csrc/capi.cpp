@@ -182,6 +182,7 @@ regb_status regb_release(void)
         REGB_CK(cudaDeviceGetDefaultMemPool(&pool, dev));
         REGB_CK(cudaDeviceSynchronize());
         REGB_CK(cudaMemPoolTrimTo(pool, 0));
+        pinned_trim();
         return REGB_OK;
     });
 }

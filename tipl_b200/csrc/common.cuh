@@ -313,6 +313,55 @@ __device__ __forceinline__ void sample_u8_pair(const uint8_t* __restrict__ I, co
     oB = (okB && acc.y > 0.0f) ? (uint32_t)(__float_as_int(tr.y) - 0x4B000000) : 0u;
 }
 
+// sample_u8_pair with the cell's corners read by 2-D texture gathers instead of
+// eight byte loads.  The volume is held as a (w, h*d) texture of halves (exact for
+// 0..255, returned as float by the texture unit): slice z, row y is texture row
+// z*h + y.  With unnormalised coordinates, a gather at (ix + 1, r + 1) returns the
+// 2x2 block with lower corner (ix, r) as x = (ix, r+1), y = (ix+1, r+1),
+// z = (ix+1, r), w = (ix, r); a second gather h rows further down gives slice z+1.
+// Both coordinates are exact integers below 2^24.  Lanes whose cell test fails
+// gather at (1, 1) and return 0.
+__device__ __forceinline__ void sample_tex_pair(cudaTextureObject_t tex, const SampleGeo& g, float hf, float2 px,
+                                                float2 py, float2 pz, bool enA, bool enB, uint32_t& oA, uint32_t& oB)
+{
+    const bool okA = enA && !(px.x < 0.0f || py.x < 0.0f || pz.x < 0.0f) && (px.x < g.wl) && (py.x < g.hl) &&
+                     (pz.x < g.dl);
+    const bool okB = enB && !(px.y < 0.0f || py.y < 0.0f || pz.y < 0.0f) && (px.y < g.wl) && (py.y < g.hl) &&
+                     (pz.y < g.dl);
+    const float2 t23 = bc2(kTwo23);
+    const float2 rx = make_float2(__fadd_rz(px.x, kTwo23), __fadd_rz(px.y, kTwo23));
+    const float2 ry = make_float2(__fadd_rz(py.x, kTwo23), __fadd_rz(py.y, kTwo23));
+    const float2 rz = make_float2(__fadd_rz(pz.x, kTwo23), __fadd_rz(pz.y, kTwo23));
+    const float2 fx = sub2(rx, t23), fy = sub2(ry, t23), fz = sub2(rz, t23);
+    const float2 p0 = sub2(px, fx), p1 = sub2(py, fy), p2 = sub2(pz, fz);
+    const float2 one = bc2(1.0f);
+    const float2 n0 = sub2(one, p0), n1 = sub2(one, p1), n2 = sub2(one, p2);
+    const float2 n0n1 = mul2(n0, n1), p0n1 = mul2(p0, n1), n0p1 = mul2(n0, p1), p0p1 = mul2(p0, p1);
+    // texture coordinates (exact integers): u = ix + 1, v = iz*h + iy + 1
+    const float2 zh = make_float2(__fmul_rn(fz.x, hf), __fmul_rn(fz.y, hf));
+    const float2 u = add2(fx, one), v = add2(add2(zh, fy), one);
+    const float uA = okA ? u.x : 1.0f, vA = okA ? v.x : 1.0f;
+    const float uB = okB ? u.y : 1.0f, vB = okB ? v.y : 1.0f;
+    const float4 a0 = tex2Dgather<float4>(tex, uA, vA, 0);
+    const float4 b0 = tex2Dgather<float4>(tex, uB, vB, 0);
+    const float4 a1 = tex2Dgather<float4>(tex, uA, vA + hf, 0);
+    const float4 b1 = tex2Dgather<float4>(tex, uB, vB + hf, 0);
+    const float2 c[8] = {make_float2(a0.w, b0.w), make_float2(a0.z, b0.z), make_float2(a0.x, b0.x),
+                         make_float2(a0.y, b0.y), make_float2(a1.w, b1.w), make_float2(a1.z, b1.z),
+                         make_float2(a1.x, b1.x), make_float2(a1.y, b1.y)};
+    const float2 wt[8] = {mul2(n0n1, n2), mul2(p0n1, n2), mul2(n0p1, n2), mul2(p0p1, n2),
+                          mul2(n0n1, p2), mul2(p0n1, p2), mul2(n0p1, p2), mul2(p0p1, p2)};
+    float2 acc;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float2 m = make_float2(__fmul_rn(c[k].x, wt[k].x), __fmul_rn(c[k].y, wt[k].y));  // feeds a sum: scalar
+        acc = (k == 0) ? m : add2(acc, m);
+    }
+    const float2 tr = make_float2(__fadd_rz(acc.x, kTwo23), __fadd_rz(acc.y, kTwo23));
+    oA = (okA && acc.x > 0.0f) ? (uint32_t)(__float_as_int(tr.x) - 0x4B000000) : 0u;
+    oB = (okB && acc.y > 0.0f) ? (uint32_t)(__float_as_int(tr.y) - 0x4B000000) : 0u;
+}
+
 // Per-row part of the transform: for a fixed row (y, z), y*T[3a+1] and z*T[3a+2]
 // of each axis a; the per-voxel remainder ((x*T0 + yT1) + zT2) + s keeps the
 // reference's summation order.  The x column and the shift are held once (ColXform)

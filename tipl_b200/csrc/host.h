@@ -29,6 +29,14 @@ void set_last_error(const std::string& s);
 
 void ensure_device();  // pool release threshold etc., once per device
 
+// Page-locked host blocks from a process-wide cache: cudaMallocHost / cudaFreeHost
+// are slow and the free synchronises the device, so jobs that come and go reuse
+// blocks instead.  pinned_get rounds `bytes` up to its size class (written back);
+// pinned_put returns a block of that size.  pinned_trim frees every cached block.
+void* pinned_get(size_t& bytes);
+void pinned_put(void* p, size_t bytes);
+void pinned_trim();
+
 // A device buffer from the stream-ordered pool (cudaMallocAsync); freed on the
 // same stream, so reuse is ordered without device-wide synchronisation.
 template <typename T>
@@ -94,16 +102,23 @@ struct PinBuf {
         if (c <= n)
             return;
         reset();
-        REGB_CK(cudaMallocHost((void**)&p, c * sizeof(T)));
-        n = c;
+        bytes_ = c * sizeof(T);
+        p = (T*)pinned_get(bytes_);  // bytes_ becomes the block's size class
+        n = c;                       // the capacity callers see stays what they asked for
     }
     void reset()
     {
         if (p)
-            cudaFreeHost(p);
+            pinned_put(p, bytes_);
         p = nullptr;
         n = 0;
+        bytes_ = 0;
     }
+
+private:
+    size_t bytes_ = 0;
+
+public:
     ~PinBuf() { reset(); }
 };
 

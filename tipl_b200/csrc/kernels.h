@@ -28,6 +28,8 @@ struct AffineTask {
     Dim3 md;                // moving extent
     float T[12];            // fixed voxel -> moving voxel (sr row-major, shift)
     int mode;               // 0 trilinear, 1 integer-shift copy (correlation only)
+    unsigned long long tex; // 0, or the moving volume as a (w, h*d) texture of halves
+                            // (cudaTextureObject_t) read by the MI kernel's gathers
     int keep;               // MI: 1 = leave the counts in hist (no reduction, no clearing)
     int shift[3];
     int nchunk;             // chunks of this task
@@ -84,6 +86,12 @@ template <typename T>
 cudaError_t launch_resample(const T* from, Dim3 fd, T* to, Dim3 td, const float* Tm, const int* shift,
                             cudaStream_t st);
 cudaError_t launch_mi(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
+// The same with every task's moving volume read through its texture (tex != 0).
+cudaError_t launch_mi_tex(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
+// Writes a uint8 volume of n voxels as halves (a texture's backing store, rows of w
+// voxels at a pitch of `pitch` halves).
+cudaError_t launch_u8_to_half_pitched(const uint8_t* in, int w, long long rows, void* out, size_t pitch,
+                                      cudaStream_t st);
 cudaError_t launch_corr(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
 // 32 x 32-bin MI (volumes quantised to 0..31); hist: 1024 counters per task, zero on entry
 cudaError_t launch_mi32(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);

@@ -53,7 +53,7 @@ void CdmScheduler::loop()
         bool failed = false;
         try {
             const int n = (int)cur.size();
-            if ((int)h_segs_.n < n) {
+            if ((int)h_segs_.n < n || (int)segs_.n < n || (int)h_status_.n < n || (int)status_.n < n) {
                 const int cap = std::max(n, 2 * (int)h_segs_.n);
                 h_segs_.alloc(cap);
                 h_status_.alloc(cap);

@@ -2,6 +2,7 @@
 // transforms handed to the kernels are bit-identical to the ones the reference
 // would build from the same parameters.  Compiled without FMA contraction.
 #include <cmath>
+#include <map>
 #include <mutex>
 #include <string>
 #include "host.h"
@@ -17,6 +18,65 @@ void throw_cuda(cudaError_t e, const char* what)
 {
     (void)cudaGetLastError();
     throw Failure(REGB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Size classes are powers of two from 256 bytes; at most kPinnedCacheBytes stay cached.
+namespace {
+constexpr size_t kPinnedCacheBytes = size_t(256) << 20;
+std::mutex g_pin_m;
+std::map<size_t, std::vector<void*>> g_pin_free;
+size_t g_pin_cached = 0;
+size_t pin_class(size_t b)
+{
+    size_t c = 256;
+    while (c < b)
+        c <<= 1;
+    return c;
+}
+}  // namespace
+
+void* pinned_get(size_t& bytes)
+{
+    bytes = pin_class(bytes);
+    {
+        std::lock_guard<std::mutex> g(g_pin_m);
+        auto it = g_pin_free.find(bytes);
+        if (it != g_pin_free.end() && !it->second.empty()) {
+            void* p = it->second.back();
+            it->second.pop_back();
+            g_pin_cached -= bytes;
+            return p;
+        }
+    }
+    void* p = nullptr;
+    REGB_CK(cudaMallocHost(&p, bytes));
+    return p;
+}
+
+void pinned_put(void* p, size_t bytes)
+{
+    {
+        std::lock_guard<std::mutex> g(g_pin_m);
+        if (g_pin_cached + bytes <= kPinnedCacheBytes) {
+            g_pin_free[bytes].push_back(p);
+            g_pin_cached += bytes;
+            return;
+        }
+    }
+    cudaFreeHost(p);
+}
+
+void pinned_trim()
+{
+    std::map<size_t, std::vector<void*>> all;
+    {
+        std::lock_guard<std::mutex> g(g_pin_m);
+        all.swap(g_pin_free);
+        g_pin_cached = 0;
+    }
+    for (auto& kv : all)
+        for (void* p : kv.second)
+            cudaFreeHost(p);
 }
 
 size_t pix_size(int dtype)
