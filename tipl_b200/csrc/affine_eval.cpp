@@ -15,6 +15,9 @@ void TaskScratch::ensure(int k, bool need_hist, cudaStream_t st)
     if (need_hist) {
         hist.alloc((size_t)c * 65536, st);
         hist.zero();
+        col.alloc((size_t)c * 256, st);
+        col.zero();
+        part.alloc((size_t)c * kMiReduceBlocks, st);
     }
     moments.alloc((size_t)c * 3, st);
     moments.zero();
@@ -30,6 +33,8 @@ void TaskScratch::ensure(int k, bool need_hist, cudaStream_t st)
 void TaskScratch::release()
 {
     hist.reset();
+    col.reset();
+    part.reset();
     moments.reset();
     ticket.reset();
     cost.reset();
@@ -113,6 +118,8 @@ void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, dou
         t.cost = s.cost.p + k;
         t.moments = s.moments.p + 3 * k;
         t.hist = (cost_type != REGB_COST_CORR) ? s.hist.p + (size_t)k * 65536 : nullptr;
+        t.col = (cost_type != REGB_COST_CORR) ? s.col.p + (size_t)k * 256 : nullptr;
+        t.part = (cost_type != REGB_COST_CORR) ? s.part.p + (size_t)k * kMiReduceBlocks : nullptr;
         if (cost_type == REGB_COST_MI && t.tex) {
             ++ntex;
             max_chunks_tex = std::max(max_chunks_tex, t.nchunk);
@@ -143,7 +150,8 @@ void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, dou
     else
         REGB_CK(launch_corr(s.tasks.p, K, max_chunks, st));
     tm.end(st, K, vox, bytes);
-    count_launch(cost_type == REGB_COST_MI && ntex && ntex < K ? 2 : 1);
+    // the 256-bin MI is a histogram launch plus a reduction launch per kernel variant
+    count_launch(cost_type == REGB_COST_MI ? 2 * ((ntex ? 1 : 0) + (ntex < K ? 1 : 0)) : 1);
     REGB_CK(cudaMemcpyAsync(s.h_cost.p, s.cost.p, sizeof(double) * K, cudaMemcpyDeviceToHost, st));
     REGB_CK(cudaStreamSynchronize(st));
     std::memcpy(out, s.h_cost.p, sizeof(double) * K);

@@ -12,6 +12,8 @@ namespace regb {
 struct TaskScratch {
     int cap = 0;
     DevBuf<uint32_t> hist;
+    DevBuf<uint32_t> col;    // 256-bin MI: 256 column sums per task
+    DevBuf<double> part;     // 256-bin MI: kMiReduceBlocks partial sums per task
     DevBuf<unsigned long long> moments;
     DevBuf<unsigned int> ticket;
     DevBuf<double> cost;

@@ -90,6 +90,7 @@ template cudaError_t launch_resample<float>(const float*, Dim3, float*, Dim3, co
 // voxel total minus every other bin, recovered in the reduction.
 constexpr int kMiThreads = 768;  // 80 registers a thread at one block per SM
 constexpr int kMiSmemWords = 32768;
+static_assert(kMiThreads % 128 == 0 && kMiThreads >= 256, "the flush maps threads to 128 word columns");
 
 __device__ __forceinline__ void mi_count(uint32_t* sh, uint32_t bin)
 {
@@ -97,52 +98,70 @@ __device__ __forceinline__ void mi_count(uint32_t* sh, uint32_t bin)
         atomicAdd(sh + (bin >> 1), 1u << ((bin & 1u) << 4));
 }
 
-// Reduction of a complete 256x256 histogram to the reference's MI cost
-// (reg/linear.hpp:87-104): column sums, then sum over non-zero bins of
-// n*ln(n/row/col) in double, divided by 65536 and negated.
-__device__ void mi_reduce_and_clear(uint32_t* __restrict__ hist, const int32_t* __restrict__ row_hist,
-                                    long long nvox, double* __restrict__ cost, uint32_t* smem)
+// Reduction of the complete 256x256 histograms to the reference's MI cost
+// (reg/linear.hpp:87-104): with the column sums already formed by the histogram
+// blocks, each of kMiReduceBlocks blocks per task sums n*ln(n/row/col) in double
+// over 2048 bins (8 rows; thread t takes column t) and clears them; the last block
+// of the task adds the partial sums in block order, writes -sum/65536, and clears
+// the column sums and the ticket.  The order of every sum is fixed, so a task's cost
+// does not depend on what it is batched with.
+constexpr int kMiReduceThreads = 256;
+constexpr int kMiReduceRows = 256 / kMiReduceBlocks;
+
+__global__ void __launch_bounds__(kMiReduceThreads) mi_reduce_kernel(const AffineTask* __restrict__ tasks)
 {
-    uint32_t* col = smem;                 // 256
-    unsigned long long* tot = (unsigned long long*)(smem + 256);  // 1
-    double* red = (double*)(smem + 512);  // 32
+    const AffineTask& tk = tasks[blockIdx.y];
+    if (tk.keep)
+        return;
+    __shared__ uint32_t col[256];
+    __shared__ unsigned long long red64[32];
+    __shared__ double red[32];
+    __shared__ unsigned int last;
     const int t = threadIdx.x;
-    if (t < 256)
-        col[t] = 0u;
-    if (t == 0)
-        *tot = 0ull;
-    __syncthreads();
-    // column partial sums: thread t covers column (t & 255), every (blockDim/256)-th row
-    {
-        const int j = t & 255, rstep = blockDim.x >> 8;
-        uint32_t s = 0;
-        for (int r = t >> 8; r < 256; r += rstep)
-            s += __ldcg(hist + r * 256 + j);
-        atomicAdd(col + j, s);
-        unsigned long long ss = s;
-        ss = warp_sum(ss);
-        if ((t & 31) == 0)
-            atomicAdd(tot, ss);
+    const uint32_t c = __ldcg(tk.col + t);
+    col[t] = c;
+    // every voxel is in one bin: the uncounted background bin is the remainder
+    const unsigned long long tot = block_sum((unsigned long long)c, red64);
+    __shared__ uint32_t n00_s;
+    if (t == 0) {
+        n00_s = (uint32_t)(tk.fd.n() - (long long)tot);
+        col[0] += n00_s;
     }
     __syncthreads();
-    const uint32_t n00 = (uint32_t)(nvox - (long long)*tot);  // the uncounted background bin
-    __syncthreads();
-    if (t == 0)
-        col[0] += n00;
-    __syncthreads();
+    const uint32_t n00 = n00_s;
+    uint32_t* __restrict__ hist = tk.hist;
+    const double cd = (double)col[t];
     double acc = 0.0;
-    for (int b = t; b < 65536; b += blockDim.x) {
-        uint32_t n = (b == 0) ? n00 : __ldcg(hist + b);
+#pragma unroll
+    for (int k = 0; k < kMiReduceRows; ++k) {
+        const int row = blockIdx.x * kMiReduceRows + k;
+        const int b = row * 256 + t;
+        const uint32_t n = (b == 0) ? n00 : __ldcg(hist + b);
         if (n) {
-            double mu = (double)n;
-            acc += mu * log(mu / (double)row_hist[b >> 8] / (double)col[b & 255]);
+            const double mu = (double)n;
+            acc += mu * log(mu / (double)tk.row_hist[row] / cd);
+            hist[b] = 0u;
         }
     }
     acc = block_sum(acc, red);
     if (t == 0)
-        *cost = -(acc / 65536.0);
-    for (int b = t; b < 65536; b += blockDim.x)
-        hist[b] = 0u;
+        tk.part[blockIdx.x] = acc;
+    __threadfence();
+    __syncthreads();
+    if (t == 0)
+        last = (atomicAdd(tk.ticket, 1u) == (unsigned)kMiReduceBlocks - 1u);
+    __syncthreads();
+    if (!last)
+        return;
+    __threadfence();
+    if (t == 0) {
+        double sum = 0.0;
+        for (int i = 0; i < kMiReduceBlocks; ++i)
+            sum += __ldcg(tk.part + i);
+        *tk.cost = -(sum / 65536.0);
+        *tk.ticket = 0u;
+    }
+    tk.col[t] = 0u;  // every block of the task has read the column sums
 }
 
 template <bool TEX>
@@ -158,7 +177,6 @@ __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __r
     __syncthreads();
     const Dim3 fd = tk.fd;
     const SampleGeo g = sample_geo(tk.md);
-    const long long n = fd.n();
     // a chunk is a run of whole rows (y, z); warps take rows, lanes take x
     const int rows = fd.h * fd.d;
     const int r0 = chunk * tk.chunk, r1 = min(rows, r0 + tk.chunk);
@@ -204,31 +222,37 @@ __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __r
         }
     }
     __syncthreads();
-    // flush non-zero counters to the task's global histogram
+    // flush the non-zero counters to the task's global histogram.  Thread t walks
+    // word column c = t % 128 (bins 2c, 2c+1 of every row) over rows t / 128 + 6k,
+    // summing the two columns as it goes; the six partial column sums meet in
+    // shared memory and go to the task's column sums.
     uint32_t* __restrict__ gh = tk.hist;
-    for (int wi = threadIdx.x; wi < kMiSmemWords; wi += blockDim.x) {
-        uint32_t w = sh[wi];
+    const int wc = threadIdx.x & 127;
+    uint32_t clo = 0u, chi = 0u;
+    for (int r = threadIdx.x >> 7; r < 256; r += kMiThreads / 128) {
+        const int wi = r * 128 + wc;
+        const uint32_t w = sh[wi];
         if (w) {
-            if (w & 0xffffu)
-                atomicAdd(gh + 2 * wi, w & 0xffffu);
-            if (w >> 16)
-                atomicAdd(gh + 2 * wi + 1, w >> 16);
+            const uint32_t lo = w & 0xffffu, hi = w >> 16;
+            clo += lo;
+            chi += hi;
+            if (lo)
+                atomicAdd(gh + 2 * wi, lo);
+            if (hi)
+                atomicAdd(gh + 2 * wi + 1, hi);
         }
     }
-    if (tk.keep)
-        return;
-    __threadfence();
+    __shared__ uint32_t colp[256];
+    if (threadIdx.x < 256)
+        colp[threadIdx.x] = 0u;
     __syncthreads();
-    __shared__ unsigned int last;
-    if (threadIdx.x == 0)
-        last = (atomicAdd(tk.ticket, 1u) == (unsigned)tk.nchunk - 1u);
+    if (clo)
+        atomicAdd(colp + 2 * wc, clo);
+    if (chi)
+        atomicAdd(colp + 2 * wc + 1, chi);
     __syncthreads();
-    if (!last)
-        return;
-    __threadfence();
-    mi_reduce_and_clear(gh, tk.row_hist, n, tk.cost, sh);
-    if (threadIdx.x == 0)
-        *tk.ticket = 0u;
+    if (threadIdx.x < 256 && colp[threadIdx.x])
+        atomicAdd(tk.col + threadIdx.x, colp[threadIdx.x]);
 }
 
 template <bool TEX>
@@ -248,6 +272,10 @@ static cudaError_t launch_mi_impl(const AffineTask* d_tasks, int ntask, int max_
     }
     dim3 grid(max_chunks, ntask);
     mi_kernel<TEX><<<grid, kMiThreads, kMiSmemWords * 4, st>>>(d_tasks);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return e;
+    mi_reduce_kernel<<<dim3(kMiReduceBlocks, ntask), kMiReduceThreads, 0, st>>>(d_tasks);
     return cudaGetLastError();
 }
 

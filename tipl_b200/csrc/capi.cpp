@@ -425,12 +425,15 @@ static regb_status affine_cost(const regb_volume* fixed, const regb_volume* movi
                 t.cost = s.cost.p;
                 t.moments = s.moments.p;
                 t.hist = s.hist.p;
+                t.col = s.col.p;
+                t.part = s.part.p;
                 t.keep = 1;  // leave the counts in place for the read-back
                 REGB_CK(cudaMemcpyAsync(s.tasks.p, s.h_tasks.p, sizeof(AffineTask), cudaMemcpyHostToDevice, st));
                 if (cost_type == REGB_COST_MI)
                     REGB_CK(launch_mi(s.tasks.p, 1, t.nchunk, st));
                 else
                     REGB_CK(launch_mi32(s.tasks.p, 1, t.nchunk, st));
+                count_launch(cost_type == REGB_COST_MI ? 2 : 1);
                 REGB_CK(cudaMemcpyAsync(h.p, s.hist.p, (size_t)nb * 4, cudaMemcpyDeviceToHost, st));
                 REGB_CK(cudaStreamSynchronize(st));
                 // bin 0 is not counted on the device; it is the remainder
@@ -440,6 +443,7 @@ static regb_status affine_cost(const regb_volume* fixed, const regb_volume* movi
                 h.p[0] = (uint32_t)((long long)nvox(fixed->dim) - tot);
                 std::memcpy(hist_out + (size_t)k * nb, h.p, (size_t)nb * 4);
                 REGB_CK(cudaMemsetAsync(s.hist.p, 0, (size_t)nb * 4, st));
+                REGB_CK(cudaMemsetAsync(s.col.p, 0, 256 * 4, st));
             }
         }
         std::vector<double> c = ev.eval(0, T, K);

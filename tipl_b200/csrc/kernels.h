@@ -35,6 +35,8 @@ struct AffineTask {
     int nchunk;             // chunks of this task
     int chunk;              // rows (y, z) of the fixed grid per chunk
     uint32_t* hist;                // MI: 65536 counters
+    uint32_t* col;                 // MI (256 bins): the 256 column sums of hist
+    double* part;                  // MI (256 bins): kMiReduceBlocks partial sums
     const int32_t* row_hist;       // MI: template value histogram (256)
     unsigned long long* moments;   // correlation: sum y, sum y^2, sum x*y
     long long sx, sxx;             // correlation: template sum x, sum x^2
@@ -85,6 +87,11 @@ struct CdmSeg {
 template <typename T>
 cudaError_t launch_resample(const T* from, Dim3 fd, T* to, Dim3 td, const float* Tm, const int* shift,
                             cudaStream_t st);
+// Blocks per task of the 256x256 MI reduction (each reduces 65536 / 32 bins).
+constexpr int kMiReduceBlocks = 32;
+// The 256-bin MI: the histogram launch, then the reduction launch (which leaves
+// hist, col and ticket zeroed again).  A task with keep = 1 keeps its counts and
+// column sums and gets no cost.
 cudaError_t launch_mi(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
 // The same with every task's moving volume read through its texture (tex != 0).
 cudaError_t launch_mi_tex(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);

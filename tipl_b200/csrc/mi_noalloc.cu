@@ -33,6 +33,8 @@ constexpr int kNoAllocMaxK = 16;
 
 struct NoAllocScratch {
     uint32_t hist[kNoAllocMaxK][65536];   // joint histograms, one per transform
+    uint32_t col[kNoAllocMaxK][256];      // their column sums
+    double part[kNoAllocMaxK][kMiReduceBlocks];  // partial sums of the MI reduction
     unsigned int ticket[kNoAllocMaxK];    // completed blocks per transform
     unsigned long long moments[kNoAllocMaxK * 3];
     int32_t row_hist[256];                // the fixed volume's value histogram
@@ -91,6 +93,7 @@ extern "C" regb_status regb_mi_cost_noalloc(const uint8_t* fixed, const int fixe
         NoAllocScratch* s = scratch_on_current_device();
         // counters the kernels expect at zero; the array keeps whatever the last call left
         REGB_CK(cudaMemsetAsync(s->hist, 0, sizeof(uint32_t) * 65536 * K, st));
+        REGB_CK(cudaMemsetAsync(s->col, 0, sizeof(uint32_t) * 256 * K, st));
         REGB_CK(cudaMemsetAsync(s->ticket, 0, sizeof(unsigned int) * K, st));
         REGB_CK(launch_fixed_stats(fixed, nf, s->row_hist, s->sums, st));
         AffineTask h[kNoAllocMaxK];
@@ -106,6 +109,8 @@ extern "C" regb_status regb_mi_cost_noalloc(const uint8_t* fixed, const int fixe
             std::memcpy(t.T, T + 12 * k, sizeof(t.T));
             t.row_hist = s->row_hist;
             t.hist = s->hist[k];
+            t.col = s->col[k];
+            t.part = s->part[k];
             t.ticket = s->ticket + k;
             t.moments = s->moments + 3 * k;
             t.cost = cost + k;
@@ -114,7 +119,7 @@ extern "C" regb_status regb_mi_cost_noalloc(const uint8_t* fixed, const int fixe
         }
         REGB_CK(cudaMemcpyAsync(s->tasks, h, sizeof(AffineTask) * K, cudaMemcpyHostToDevice, st));
         REGB_CK(launch_mi(s->tasks, K, max_chunks, st));
-        count_launch();
+        count_launch(3);  // the fixed-volume statistics, the histogram and the reduction
         // h is a stack array: the copy must have read it before returning
         REGB_CK(cudaStreamSynchronize(st));
         return REGB_OK;
