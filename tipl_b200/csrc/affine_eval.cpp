@@ -95,11 +95,12 @@ void set_task_chunks(AffineTask& t, int cost_type)
     const long long w = t.fd.w, rows = (long long)t.fd.h * t.fd.d;
     long long rpc;
     if (cost_type == REGB_COST_MI) {
-        // 16-bit per-block counters: at most 65535 voxels per block; about one block
-        // per SM for a large grid, at least 32K voxels per block for a small one.
+        // 16-bit per-block counters: at most 65535 voxels per block.  Blocks are made
+        // nearly that large (at least 60,000 voxels) because each one ends with a flush
+        // of its whole shared histogram: fewer, fuller blocks flush less often.
         const long long hi = std::max<long long>(1, 65535 / w);
         rpc = (rows + 147) / 148;
-        rpc = std::max<long long>(rpc, (32768 + w - 1) / w);
+        rpc = std::max<long long>(rpc, (60000 + w - 1) / w);
         rpc = std::min<long long>(rpc, hi);
     } else if (cost_type == REGB_COST_MI32)
         rpc = std::max<long long>(1, (8192 + w - 1) / w);  // small blocks, many per SM

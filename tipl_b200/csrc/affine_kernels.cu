@@ -236,10 +236,10 @@ __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __r
             const uint32_t lo = w & 0xffffu, hi = w >> 16;
             clo += lo;
             chi += hi;
-            if (lo)
-                atomicAdd(gh + 2 * wi, lo);
-            if (hi)
-                atomicAdd(gh + 2 * wi + 1, hi);
+            // bins 2wi and 2wi+1 are adjacent 32-bit counters: one 64-bit add updates both
+            // (a bin never exceeds the voxel count < 2^32, so no carry crosses between them)
+            atomicAdd(reinterpret_cast<unsigned long long*>(gh + 2 * wi),
+                      ((unsigned long long)hi << 32) | (unsigned long long)lo);
         }
     }
     __shared__ uint32_t colp[256];
