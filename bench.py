@@ -43,8 +43,8 @@ METRIC = "registrations/s (affine 12-DOF MI, 182x218x182 uint8, 1 mm)"
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per voxel evaluation of mi_kernel, from one ncu capture of a
 # 12-candidate launch on the 182x218x182 pair (profiles/mi_kernel_affine_182x218x182.md:
-# 17.613568 MB / 86.65 M voxel evaluations); scaled to each bench launch by its voxels.
-MI_DRAM_BYTES_PER_VOXEL_EVAL = 17.613568e6 / (12 * 7221032)
+# 24.44544 MB / 86.65 M voxel evaluations); scaled to each bench launch by its voxels.
+MI_DRAM_BYTES_PER_VOXEL_EVAL = 24.44544e6 / (12 * 7221032)
 COST_NAME = {"mi": "MI", "mi32": "MI (32x32 bins)"}
 COST_DESC = {"mi": "MI 256x256 joint histogram (the reference's)",
              "mi32": "MI 32x32 joint histogram (both volumes quantised to 0..31 by normalize_upper_lower2(31.99))"}
