@@ -47,7 +47,7 @@ void TaskScratch::release()
 static bool tex_enabled()
 {
     static const bool on = [] {
-        const char* e = std::getenv("REGB_MI_TEXTURE");
+        const char* e = std::getenv("REGB_TEXTURE");
         return !(e && e[0] == '0');
     }();
     return on;
@@ -103,7 +103,9 @@ void set_task_chunks(AffineTask& t, int cost_type)
         rpc = std::max<long long>(rpc, (60000 + w - 1) / w);
         rpc = std::min<long long>(rpc, hi);
     } else if (cost_type == REGB_COST_MI32)
-        rpc = std::max<long long>(1, (8192 + w - 1) / w);  // small blocks, many per SM
+        // 32-bit counters (no per-block voxel bound); about one block per SM for a large
+        // grid, at least 60,000 voxels per block for a small one
+        rpc = std::max<long long>((rows + 147) / 148, (60000 + w - 1) / w);
     else
         rpc = std::max<long long>(1, (32768 + w - 1) / w);
     t.chunk = (int)rpc;
@@ -121,7 +123,7 @@ void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, dou
         t.hist = (cost_type != REGB_COST_CORR) ? s.hist.p + (size_t)k * 65536 : nullptr;
         t.col = (cost_type != REGB_COST_CORR) ? s.col.p + (size_t)k * 256 : nullptr;
         t.part = (cost_type != REGB_COST_CORR) ? s.part.p + (size_t)k * kMiReduceBlocks : nullptr;
-        if (cost_type == REGB_COST_MI && t.tex) {
+        if (t.tex) {
             ++ntex;
             max_chunks_tex = std::max(max_chunks_tex, t.nchunk);
         } else
@@ -141,18 +143,26 @@ void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, dou
     }
     KernelTimer tm;
     tm.begin(st, cost_type == REGB_COST_CORR ? 1 : 0);  // both MI forms count as MI
+    // texture tasks (the first ntex) and byte-load tasks run as separate launches
     if (cost_type == REGB_COST_MI) {
         if (ntex)
             REGB_CK(launch_mi_tex(s.tasks.p, ntex, max_chunks_tex, st));
         if (ntex < K)
             REGB_CK(launch_mi(s.tasks.p + ntex, K - ntex, max_chunks, st));
-    } else if (cost_type == REGB_COST_MI32)
-        REGB_CK(launch_mi32(s.tasks.p, K, max_chunks, st));
-    else
-        REGB_CK(launch_corr(s.tasks.p, K, max_chunks, st));
+    } else if (cost_type == REGB_COST_MI32) {
+        if (ntex)
+            REGB_CK(launch_mi32_tex(s.tasks.p, ntex, max_chunks_tex, st));
+        if (ntex < K)
+            REGB_CK(launch_mi32(s.tasks.p + ntex, K - ntex, max_chunks, st));
+    } else {
+        if (ntex)
+            REGB_CK(launch_corr_tex(s.tasks.p, ntex, max_chunks_tex, st));
+        if (ntex < K)
+            REGB_CK(launch_corr(s.tasks.p + ntex, K - ntex, max_chunks, st));
+    }
     tm.end(st, K, vox, bytes);
     // the 256-bin MI is a histogram launch plus a reduction launch per kernel variant
-    count_launch(cost_type == REGB_COST_MI ? 2 * ((ntex ? 1 : 0) + (ntex < K ? 1 : 0)) : 1);
+    count_launch((cost_type == REGB_COST_MI ? 2 : 1) * ((ntex ? 1 : 0) + (ntex < K ? 1 : 0)));
     REGB_CK(cudaMemcpyAsync(s.h_cost.p, s.cost.p, sizeof(double) * K, cudaMemcpyDeviceToHost, st));
     REGB_CK(cudaStreamSynchronize(st));
     std::memcpy(out, s.h_cost.p, sizeof(double) * K);
@@ -186,7 +196,11 @@ AffineEvaluator::AffineEvaluator(const std::vector<Pair>& levels, int cost_type,
             grid = L.p.to;
             n = L.p.td.n();
         }
-        if (cost_type == REGB_COST_MI)
+        // the sampled volume as a texture (the to-volume, or the from-volume when the
+        // correlation swaps the roles)
+        if (L.swap)
+            L.tex.build(L.p.from, L.p.fd, st);
+        else
             L.tex.build(L.p.to, L.p.td, st);
         L.row_hist.alloc(256, st);
         L.sums.alloc(2, st);
@@ -220,7 +234,7 @@ void AffineEvaluator::make_task(int level, const float* T, AffineTask& t) const
     t.mode = 0;
     if (cost_type_ == REGB_COST_CORR && integer_shift(M, t.shift))
         t.mode = 1;  // the CPU resample's integer-shift copy
-    t.tex = (cost_type_ == REGB_COST_MI && !L.swap) ? (unsigned long long)L.tex.t : 0ull;
+    t.tex = (unsigned long long)L.tex.t;  // the texture of the volume this task samples
     t.row_hist = L.row_hist.p;
     t.sx = L.sx;
     t.sxx = L.sxx;

@@ -83,7 +83,7 @@ private:
         Pair p;
         bool swap = false;  // correlation: the to-volume is the smaller one and becomes the grid
         DevBuf<uint8_t> qf, qt;  // 32-bin MI: the level's volumes quantised to 0..31
-        TexVol tex;              // MI: the moving volume as a texture (t = 0: byte loads)
+        TexVol tex;              // the sampled volume as a texture (t = 0: byte loads)
         DevBuf<int32_t> row_hist;
         DevBuf<unsigned long long> sums;
         long long sx = 0, sxx = 0;

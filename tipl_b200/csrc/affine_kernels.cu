@@ -318,11 +318,13 @@ cudaError_t launch_u8_to_half_pitched(const uint8_t* in, int w, long long rows, 
 // non-uint8 images, reg/linear.hpp:190-197), bin = (template << 5) + sample.  The
 // 1024-bin per-block histogram is 4 KB of shared memory, so blocks are small and many;
 // bin 0 is again recovered as the remainder.  Cost = -sum n ln(n / (row col)) / 1024.
-constexpr int kMi32Threads = 256;
+constexpr int kMi32Threads = 768;
+constexpr int kMi32Copies = 8;  // shared histogram copies; warp w counts into copy w % 8
 
-__global__ void __launch_bounds__(kMi32Threads) mi32_kernel(const AffineTask* __restrict__ tasks)
+template <bool TEX>
+__global__ void __launch_bounds__(kMi32Threads, 1) mi32_kernel(const AffineTask* __restrict__ tasks)
 {
-    __shared__ uint32_t sh[1024];
+    extern __shared__ uint32_t sh[];  // kMi32Copies x 1024 counters
     __shared__ uint32_t col[32];
     __shared__ double red[32];
     __shared__ unsigned long long tot;
@@ -331,7 +333,7 @@ __global__ void __launch_bounds__(kMi32Threads) mi32_kernel(const AffineTask* __
     const int chunk = blockIdx.x;
     if (chunk >= tk.nchunk)
         return;
-    for (int i = threadIdx.x; i < 1024; i += blockDim.x)
+    for (int i = threadIdx.x; i < kMi32Copies * 1024; i += blockDim.x)
         sh[i] = 0u;
     __syncthreads();
     const Dim3 fd = tk.fd;
@@ -339,26 +341,65 @@ __global__ void __launch_bounds__(kMi32Threads) mi32_kernel(const AffineTask* __
     const int rows = fd.h * fd.d;
     const int r0 = chunk * tk.chunk, r1 = min(rows, r0 + tk.chunk);
     const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    uint32_t* __restrict__ mine = sh + ((threadIdx.x >> 5) % kMi32Copies) * 1024;
+    const uint8_t* __restrict__ moving = tk.moving;
+    const float hf = (float)tk.md.h;
     const float* __restrict__ T = tk.T;
     ColXform cx;
     cx.set(T);
-    for (int r = r0 + (threadIdx.x >> 5); r < r1; r += nw) {
-        RowXform xr;
-        xr.set(T, r % fd.h, r / fd.h);
-        const uint8_t* __restrict__ fr = tk.fixed + (long long)r * fd.w;
-        for (int x = lane; x < fd.w; x += 32) {
-            float px, py, pz;
-            xr.at(cx, (float)x, px, py, pz);
-            const uint32_t b = ((uint32_t)__ldg(fr + x) << 5) | sample_u8(tk.moving, g, px, py, pz);
-            if (b)
-                atomicAdd(sh + b, 1u);
+    // lanes with the same bin add once (few distinct bins per warp at 32 levels)
+    auto count = [&](uint32_t bin, bool on) {
+        const unsigned act = __ballot_sync(0xffffffffu, on && bin != 0u);
+        if (on && bin != 0u) {
+            const unsigned peers = __match_any_sync(act, bin);
+            if ((int)(__ffs(peers) - 1) == lane)
+                atomicAdd(mine + bin, (uint32_t)__popc(peers));
+        }
+    };
+    // the sampling loop of mi_kernel: two adjacent rows per warp, packed pair arithmetic
+    for (int r = r0 + 2 * (threadIdx.x >> 5); r < r1; r += 2 * nw) {
+        const int rb = r + 1;
+        const bool two = rb < r1;
+        RowXform xa, xb;
+        xa.set(T, r % fd.h, r / fd.h);
+        xb.set(T, (two ? rb : r) % fd.h, (two ? rb : r) / fd.h);
+        const uint8_t* __restrict__ fa = tk.fixed + (long long)r * fd.w;
+        const uint8_t* __restrict__ fb = tk.fixed + (long long)(two ? rb : r) * fd.w;
+        const float2 yt0 = make_float2(xa.yt[0], xb.yt[0]), yt1 = make_float2(xa.yt[1], xb.yt[1]),
+                     yt2 = make_float2(xa.yt[2], xb.yt[2]);
+        const float2 zt0 = make_float2(xa.zt[0], xb.zt[0]), zt1 = make_float2(xa.zt[1], xb.zt[1]),
+                     zt2 = make_float2(xa.zt[2], xb.zt[2]);
+        const float2 s0 = bc2(cx.s[0]), s1 = bc2(cx.s[1]), s2 = bc2(cx.s[2]);
+        // every lane of the warp runs the same number of iterations (the counting is
+        // warp-collective); lanes past the row's end sample nothing and count nothing
+        for (int x0 = 0; x0 < fd.w; x0 += 32) {
+            const int x = x0 + lane;
+            const bool in = x < fd.w;
+            const float fx = (float)x;
+            const float2 px = add2(add2(add2(bc2(__fmul_rn(fx, cx.t0[0])), yt0), zt0), s0);
+            const float2 py = add2(add2(add2(bc2(__fmul_rn(fx, cx.t0[1])), yt1), zt1), s1);
+            const float2 pz = add2(add2(add2(bc2(__fmul_rn(fx, cx.t0[2])), yt2), zt2), s2);
+            const uint32_t fva = in ? (uint32_t)__ldg(fa + x) : 0u;
+            const uint32_t fvb = (in && two) ? (uint32_t)__ldg(fb + x) : 0u;
+            uint32_t ta, tb;
+            if constexpr (TEX)
+                sample_tex_pair((cudaTextureObject_t)tk.tex, g, hf, px, py, pz, in, in && two, ta, tb);
+            else
+                sample_u8_pair(moving, g, px, py, pz, in, in && two, ta, tb);
+            count((fva << 5) | ta, in);
+            count((fvb << 5) | tb, in && two);
         }
     }
     __syncthreads();
     uint32_t* __restrict__ gh = tk.hist;
-    for (int i = threadIdx.x; i < 1024; i += blockDim.x)
-        if (sh[i])
-            atomicAdd(gh + i, sh[i]);
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x) {
+        uint32_t v = 0u;
+#pragma unroll
+        for (int c = 0; c < kMi32Copies; ++c)
+            v += sh[c * 1024 + i];
+        if (v)
+            atomicAdd(gh + i, v);
+    }
     if (tk.keep)
         return;
     __threadfence();
@@ -408,10 +449,34 @@ __global__ void __launch_bounds__(kMi32Threads) mi32_kernel(const AffineTask* __
         gh[b] = 0u;
 }
 
+template <bool TEX>
+static cudaError_t launch_mi32_impl(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
+{
+    constexpr int smem = kMi32Copies * 1024 * 4;
+    static std::atomic<unsigned long long> attr_set{0};  // one bit per device
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr_set.load() & bit)) {
+        e = cudaFuncSetAttribute(mi32_kernel<TEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess)
+            return e;
+        attr_set.fetch_or(bit);
+    }
+    mi32_kernel<TEX><<<dim3(max_chunks, ntask), kMi32Threads, smem, st>>>(d_tasks);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_mi32(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
 {
-    mi32_kernel<<<dim3(max_chunks, ntask), kMi32Threads, 0, st>>>(d_tasks);
-    return cudaGetLastError();
+    return launch_mi32_impl<false>(d_tasks, ntask, max_chunks, st);
+}
+
+cudaError_t launch_mi32_tex(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
+{
+    return launch_mi32_impl<true>(d_tasks, ntask, max_chunks, st);
 }
 
 // ---------------------------------------------------------------- correlation
@@ -420,6 +485,7 @@ cudaError_t launch_mi32(const AffineTask* d_tasks, int ntask, int max_chunks, cu
 // thread sums at most kCorrPerThread voxels in 32 bits (255^2 * 64 < 2^32).
 constexpr int kCorrThreads = 256;
 
+template <bool TEX>
 __global__ void __launch_bounds__(kCorrThreads) corr_kernel(const AffineTask* __restrict__ tasks)
 {
     const AffineTask& tk = tasks[blockIdx.y];
@@ -478,7 +544,10 @@ __global__ void __launch_bounds__(kCorrThreads) corr_kernel(const AffineTask* __
                 const float2 py = add2(add2(add2(bc2(__fmul_rn(fx, cx.t0[1])), yt1), zt1), s1);
                 const float2 pz = add2(add2(add2(bc2(__fmul_rn(fx, cx.t0[2])), yt2), zt2), s2);
                 uint32_t va, vb;
-                sample_u8_pair(moving, g, px, py, pz, true, two, va, vb);
+                if constexpr (TEX)
+                    sample_tex_pair((cudaTextureObject_t)tk.tex, g, (float)md.h, px, py, pz, true, two, va, vb);
+                else
+                    sample_u8_pair(moving, g, px, py, pz, true, two, va, vb);
                 acc(__ldg(fa + x), va);
                 if (two)
                     acc(__ldg(fb + x), vb);
@@ -522,7 +591,14 @@ __global__ void __launch_bounds__(kCorrThreads) corr_kernel(const AffineTask* __
 cudaError_t launch_corr(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
 {
     dim3 grid(max_chunks, ntask);
-    corr_kernel<<<grid, kCorrThreads, 0, st>>>(d_tasks);
+    corr_kernel<false><<<grid, kCorrThreads, 0, st>>>(d_tasks);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_corr_tex(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
+{
+    dim3 grid(max_chunks, ntask);
+    corr_kernel<true><<<grid, kCorrThreads, 0, st>>>(d_tasks);
     return cudaGetLastError();
 }
 

@@ -29,7 +29,7 @@ struct AffineTask {
     float T[12];            // fixed voxel -> moving voxel (sr row-major, shift)
     int mode;               // 0 trilinear, 1 integer-shift copy (correlation only)
     unsigned long long tex; // 0, or the moving volume as a (w, h*d) texture of halves
-                            // (cudaTextureObject_t) read by the MI kernel's gathers
+                            // (cudaTextureObject_t) read by the cost kernels' gathers
     int keep;               // MI: 1 = leave the counts in hist (no reduction, no clearing)
     int shift[3];
     int nchunk;             // chunks of this task
@@ -102,6 +102,10 @@ cudaError_t launch_u8_to_half_pitched(const uint8_t* in, int w, long long rows, 
 cudaError_t launch_corr(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
 // 32 x 32-bin MI (volumes quantised to 0..31); hist: 1024 counters per task, zero on entry
 cudaError_t launch_mi32(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
+// The MI32 and correlation kernels with every task's moving volume read through its
+// texture (tex != 0; correlation tasks in integer-shift mode still read bytes).
+cudaError_t launch_mi32_tex(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
+cudaError_t launch_corr_tex(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
 cudaError_t launch_fixed_stats(const uint8_t* f, long long n, int32_t* hist, unsigned long long* sums,
                                cudaStream_t st);
 
