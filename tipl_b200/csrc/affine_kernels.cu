@@ -347,14 +347,9 @@ __global__ void __launch_bounds__(kMi32Threads, 1) mi32_kernel(const AffineTask*
     const float* __restrict__ T = tk.T;
     ColXform cx;
     cx.set(T);
-    // lanes with the same bin add once (few distinct bins per warp at 32 levels)
     auto count = [&](uint32_t bin, bool on) {
-        const unsigned act = __ballot_sync(0xffffffffu, on && bin != 0u);
-        if (on && bin != 0u) {
-            const unsigned peers = __match_any_sync(act, bin);
-            if ((int)(__ffs(peers) - 1) == lane)
-                atomicAdd(mine + bin, (uint32_t)__popc(peers));
-        }
+        if (on && bin != 0u)
+            atomicAdd(mine + bin, 1u);
     };
     // the sampling loop of mi_kernel: two adjacent rows per warp, packed pair arithmetic
     for (int r = r0 + 2 * (threadIdx.x >> 5); r < r1; r += 2 * nw) {
@@ -370,8 +365,7 @@ __global__ void __launch_bounds__(kMi32Threads, 1) mi32_kernel(const AffineTask*
         const float2 zt0 = make_float2(xa.zt[0], xb.zt[0]), zt1 = make_float2(xa.zt[1], xb.zt[1]),
                      zt2 = make_float2(xa.zt[2], xb.zt[2]);
         const float2 s0 = bc2(cx.s[0]), s1 = bc2(cx.s[1]), s2 = bc2(cx.s[2]);
-        // every lane of the warp runs the same number of iterations (the counting is
-        // warp-collective); lanes past the row's end sample nothing and count nothing
+        // lanes past the row's end sample nothing and count nothing
         for (int x0 = 0; x0 < fd.w; x0 += 32) {
             const int x = x0 + lane;
             const bool in = x < fd.w;
