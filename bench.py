@@ -338,6 +338,62 @@ def precision_report(args):
     return 0
 
 
+def nifti_case(args):
+    """NIfTI reads of a 182x218x182 int16 volume in RAS orientation with scl_slope /
+    scl_inter (the reader flips x and y): the library's read to a device float32 LPS
+    volume against the reference's own reader (gz_nifti >> I, oracle/_ref) on the
+    host, for an uncompressed .nii and a gzip .nii.gz.  Wall time per read, median of 5
+    after a warm-up read; the device volumes are compared bit for bit."""
+    import gzip
+    import tempfile
+
+    import torch
+
+    import tipl_b200 as tb
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import nifti_bytes
+
+    rng = np.random.default_rng(7)
+    v = rng.integers(-2000, 30000, SHAPE).astype(np.int16)
+    ras = [1.0, 0, 0, -90.0, 0, 1.0, 0, -126.0, 0, 0, 1.0, -72.0]
+    data, _ = nifti_bytes(v, 4, 16, srow=ras, slope=0.75, inter=10.0)
+    tmp = tempfile.mkdtemp()
+    paths = {"nii": os.path.join(tmp, "v.nii"), "nii.gz": os.path.join(tmp, "v.nii.gz")}
+    open(paths["nii"], "wb").write(data)
+    with gzip.GzipFile(paths["nii.gz"], "wb", mtime=0) as f:
+        f.write(data)
+    ref = None
+    try:
+        import oracle
+
+        if os.path.exists(oracle.REF_SO):
+            ref = oracle.Reference()
+    except Exception:
+        ref = None
+    line = {"kernel_case": "nifti", "volume": "182x218x182 int16, RAS, scaled", "voxels": int(v.size)}
+    for kind, path in paths.items():
+        ts = []
+        for k in range(6):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            I, info = tb.nifti_load(path, device="cuda")
+            torch.cuda.synchronize()
+            if k:
+                ts.append(time.perf_counter() - t0)
+        entry = {"ours_ms": 1000.0 * float(np.median(ts)), "file_bytes": os.path.getsize(path)}
+        if ref is not None:
+            rs = []
+            for k in range(3):
+                t0 = time.perf_counter()
+                r = ref.nifti_load(path, cap=v.size)
+                rs.append(time.perf_counter() - t0)
+            entry["reference_cpu_ms"] = 1000.0 * float(np.median(rs))
+            entry["bit_exact"] = bool(np.array_equal(I.cpu().numpy().view(np.uint32), r[0].view(np.uint32)))
+        line[kind] = entry
+    print(json.dumps(line))
+    return 0
+
+
 def pre_case(args):
     """Subject preprocessing of a 182x218x182 float32 subject: the fused Gaussian round
     (CUDA events over 20 launches, after warm-up) against the HBM copy peak, the whole
@@ -627,7 +683,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cost", choices=["mi", "mi32"], default="mi",
                     help="served / plain affine cost: the reference's 256x256-bin MI, or the 32x32-bin variant")
-    ap.add_argument("--kernel-case", choices=["mi", "mi32", "corr", "cdm", "pre"], default=None,
+    ap.add_argument("--kernel-case", choices=["mi", "mi32", "corr", "cdm", "pre", "nifti"], default=None,
                     help="run only K-candidate cost batches of the full-size pair (for profiler captures)")
     ap.add_argument("--k", type=int, default=12)
     ap.add_argument("--precision-report", action="store_true",
@@ -646,6 +702,8 @@ def main():
         return run_reference(args)
     if args.kernel_case == "cdm":
         return cdm_case(args)
+    if args.kernel_case == "nifti":
+        return nifti_case(args)
     if args.kernel_case == "pre":
         return pre_case(args)
     if args.kernel_case:

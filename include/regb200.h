@@ -233,6 +233,44 @@ regb_status regb_match_fov(const regb_volume* It, const float T[12], const int m
  * Pearson r from exact integer moments, 0 when either is constant; masked != 0 gives
  * correlation_ygz (:600-619), over the voxels with y > 0 only (mm_reg's default r). */
 regb_status regb_correlation(const regb_volume* x, const regb_volume* y, int masked, double* r);
+/* ---- NIfTI volumes (io/nifti.hpp) ------------------------------------------------- */
+/* Geometry of a NIfTI file as tipl::io::gz_nifti reports it after its LPS
+ * reorientation (toLPS, io/nifti.hpp:129-160, 1293-1298; handle_qform :1223-1260). */
+typedef struct {
+    int dim[3];            /* LPS dims (width, height, depth) */
+    float vs[3];           /* voxel size, reordered with the axes (nii >> vs) */
+    float srow[12];        /* voxel -> space rows srow_x, srow_y, srow_z (nii >> T) */
+    int file_dim[8];       /* dim[] as stored */
+    int datatype;          /* NIfTI datatype code, bitpix */
+    int bitpix;
+    int nvolumes;          /* volumes in the file (product of dim[4..dim[0]]) */
+    float scl_slope, scl_inter;
+    int sform_code;        /* after handle_qform */
+    int is_mni;            /* gz_nifti::is_mni (io/nifti.hpp:856-864) */
+    int big_endian;
+    int nifti2;            /* 1: a NIfTI-2 (540-byte) header */
+    int n_steps;           /* the reorientation: steps[0..n_steps) of 0..2 flip x/y/z, */
+    int steps[8];          /* 3 swap xy, 4 swap yz, 5 swap xz, in the order applied */
+    char descrip[81];
+} regb_nifti_info;
+/* Reads the header of a .nii, .nii.gz or .hdr/.img file (the gz_nifti open path,
+ * io/nifti.hpp:624-754, with gz_stream's gzip handling); no device work. */
+regb_status regb_nifti_info_read(const char* path, regb_nifti_info* info);
+/* nii >> image<3,float> (io/nifti.hpp:1134-1172, 1193-1205) for volume `volume`:
+ * the stored bytes go to the device as they are, and one kernel converts them
+ * (byte order, datatype, scl_slope/scl_inter) into out in LPS orientation.  out:
+ * REGB_F32, dims info->dim, host or device.  info (optional) receives the geometry.
+ * Datatypes 2, 4, 8, 16, 64, 256, 512, 768, 1024, 1280 (RGB and complex are not
+ * read). */
+regb_status regb_nifti_load(const char* path, int volume, regb_volume* out, regb_nifti_info* info, void* stream);
+/* nii << vs << T << is_mni << image (io/nifti.hpp:969-1030): writes vol (U8, U16 or F32,
+ * host or device) as a NIfTI-1 file with its voxels as they are, pixdim vs, srow rows
+ * and sform code 4 (is_mni) or 1.  Like the reference's writer, the file is always
+ * gzip-compressed (io/gz_stream.hpp:535-580), whatever the extension, and a U16 volume
+ * carries the int16 datatype code (its type table, io/nifti.hpp:286-290). */
+regb_status regb_nifti_save(const char* path, const regb_volume* vol, const float vs[3], const float srow[12],
+                            int is_mni, const char* descrip);
+
 /* downsample_with_padding (numerical/resampling.hpp:575-671); out dims (d+1)/2. */
 regb_status regb_downsample(const regb_volume* in, regb_volume* out, void* stream);
 /* best_d *= 2; upsample_with_padding(best_d, shape) (reg/cdm.hpp:402-403,

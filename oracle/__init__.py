@@ -473,6 +473,28 @@ class Reference(_Lib):
                                           _ptr(a), int(reg_type), int(cost_type), int(bound))
         return float(c), a
 
+    def nifti_load(self, path, cap=1 << 28):
+        """gz_nifti(path) >> I >> vs >> T >> is_mni: (I float32 (z, y, x), vs, srow[12], is_mni),
+        or None when the reference fails to read the file."""
+        dim = np.zeros(3, np.int32)
+        vs = np.zeros(3, np.float32)
+        srow = np.zeros(12, np.float32)
+        mni = C.c_int(0)
+        buf = np.zeros(int(cap), np.float32)
+        ok = self.lib.tiplref_nifti_load(str(path).encode(), _ptr(dim), _ptr(vs), _ptr(srow), _ptr(buf),
+                                         C.c_longlong(int(cap)), C.byref(mni))
+        if not ok:
+            return None
+        x, y, z = (int(v) for v in dim)
+        return buf[:x * y * z].reshape(z, y, x).copy(), vs, srow, bool(mni.value)
+
+    def nifti_save(self, path, vol, vs, srow, is_mni=False):
+        """gz_nifti(path, out) << vs << T << is_mni << I for a float32 or uint8 volume."""
+        v = np.ascontiguousarray(vol)
+        assert v.dtype in (np.float32, np.uint8)
+        return bool(self.lib.tiplref_nifti_save(str(path).encode(), _ptr(v), int(v.dtype == np.uint8),
+                                                _ptr(_dims(v.shape)), _ptr(_f32(vs)), _ptr(_f32(srow)), int(is_mni)))
+
     def normalize_u16_to_u8(self, img, upper=255.999):
         out = np.zeros(img.shape, np.uint8)
         self.lib.tiplref_normalize_u16_to_u8(_ptr(np.ascontiguousarray(img, np.uint16)), _ptr(_dims(img.shape)),

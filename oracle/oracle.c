@@ -283,6 +283,9 @@ ORC_NORMALIZE(orc_normalize_to_u8_u8, uint8_t)
 /* ---- mask-moment initialisation of linear() ------------------------------- */
 #include "oracle_mask.h"
 
+/* ---- NIfTI volumes read as float ------------------------------------------ */
+#include "oracle_nifti.h"
+
 /* ---- affine costs ---------------------------------------------------------- */
 
 /* histogram(img, hist, 0, 255, 256) (numerical/basic_op.hpp:1293-1311): bin =

@@ -91,6 +91,11 @@ void orc_estimate_affine_param_u8(const uint8_t* src, const int* sdim, const flo
 void orc_matrix_to_affine_param(const float* T, const int* from_dim, const float* from_vs, const int* to_dim,
                                 const float* to_vs, float* arg);
 
+/* NIfTI volume `vol` of path as float in LPS orientation (the reference's gz_nifti >> I);
+ * 1 on success */
+int orc_nifti_load(const char* path, int vol, float* out, long long cap, int* dim, float* vs, float* srow,
+                   int* steps, int* nsteps);
+
 #ifdef __cplusplus
 }
 #endif

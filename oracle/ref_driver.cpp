@@ -7,10 +7,14 @@
 //
 // Every entry point forwards to exactly one reference routine; the routine and its
 // file:line are named beside each function.
+#include <zlib.h>  // before the reference's headers: io/gz_stream.hpp is built only with zlib
+#include <map>  // io/gz_stream.hpp uses std::map without including it
 #include <algorithm>
 #include <vector>
 #include <cstring>
 #include <cstdint>
+#include "io/gz_stream.hpp"
+#include "io/nifti.hpp"
 #include "reg/linear.hpp"
 #include "reg/cdm.hpp"
 #include "reg/mm_reg.hpp"
@@ -376,4 +380,53 @@ void tiplref_normalize_u16_to_u8(const unsigned short* in, const int* dim, u8* o
         std::copy(o.begin(), o.end(), out);
 }
 
+
+// tipl::io::gz_nifti in(path, std::ios::in); in >> I >> vs >> T (io/nifti.hpp:617-754,
+// 1134-1205): I is the first volume as float, reoriented to LPS.  dim_out receives the
+// LPS dims, data_out (capacity cap floats) the voxels.  Returns 1 on success.
+int tiplref_nifti_load(const char* path, int* dim_out, float* vs_out, float* srow_out, float* data_out,
+                       long long cap, int* is_mni)
+{
+    tipl::io::gz_nifti in(path, std::ios::in);
+    if (!in)
+        return 0;
+    tipl::image<3, float> I;
+    tipl::vector<3> vs;
+    tipl::matrix<4, 4> T;
+    bool mni = false;
+    if (!(in >> I >> vs >> T >> mni))
+        return 0;
+    for (int i = 0; i < 3; ++i) {
+        dim_out[i] = int(I.shape()[i]);
+        vs_out[i] = vs[i];
+    }
+    std::copy_n(T.begin(), 12, srow_out);
+    *is_mni = mni ? 1 : 0;
+    if ((long long)I.size() > cap)
+        return 0;
+    std::copy(I.begin(), I.end(), data_out);
+    return 1;
+}
+
+// tipl::io::gz_nifti out(path, std::ios::out); out << vs << T << mni << I
+// (io/nifti.hpp:617-635, 969-1030) for a float or uint8 volume.
+int tiplref_nifti_save(const char* path, const void* data, int is_u8, const int* dim, const float* vs,
+                       const float* srow, int is_mni)
+{
+    tipl::io::gz_nifti out(path, std::ios::out);
+    if (!out)
+        return 0;
+    tipl::matrix<4, 4> T;
+    T.identity();
+    std::copy_n(srow, 12, T.begin());
+    tipl::vector<3> v(vs[0], vs[1], vs[2]);
+    if (is_u8) {
+        tipl::image<3, u8> I(shp(dim));
+        std::memcpy(I.data(), data, I.size());
+        return (out << v << T << bool(is_mni) << I) ? 1 : 0;
+    }
+    tipl::image<3, float> I(shp(dim));
+    std::memcpy(I.data(), data, I.size() * sizeof(float));
+    return (out << v << T << bool(is_mni) << I) ? 1 : 0;
+}
 }  // extern "C"

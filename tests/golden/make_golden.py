@@ -31,7 +31,7 @@ def save(name, **arrays):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=os.environ.get("TIPL_REF_ROOT", oracle.DEFAULT_REF_ROOT))
-    ap.add_argument("--only", default=None, help="make one fixture group: core | mask_init | precision | preprocess | linear_runs | mapping | mi32")
+    ap.add_argument("--only", default=None, help="make one fixture group: core | mask_init | precision | preprocess | linear_runs | mapping | mi32 | nifti")
     args = ap.parse_args()
     oracle.build(args.ref_root, with_ref=True)
     R = oracle.Reference()
@@ -50,6 +50,138 @@ def main():
         mapping(R)
     if args.only in (None, "mi32"):
         mi32(R)
+    if args.only in (None, "nifti"):
+        nifti(R)
+
+
+NIFTI_DIR = os.path.join(HERE, "nifti")
+
+
+def nifti_bytes(data, datatype, bitpix, srow=None, pixdim=(1.0, 1.0, 1.0), qform=None, big=False, version=1,
+                slope=1.0, inter=0.0, magic=None, extra_dims=(), sform_code=1):
+    """A NIfTI-1 (348-byte) or NIfTI-2 (540-byte) header followed by the voxels, built
+    field by field from the published layouts (header only when magic is 'ni1')."""
+    import struct
+
+    e = ">" if big else "<"
+    z, y, x = data.shape
+    dims = [3 + len(extra_dims), x, y, z] + list(extra_dims)
+    dims += [1] * (8 - len(dims))
+    pix = [1.0, *pixdim, 1.0, 1.0, 1.0, 1.0]
+    sform, qform_code = (sform_code, 0) if qform is None else (0, 1)
+    if qform is not None:
+        pix[0] = qform.get("qfac", 1.0)
+    q = qform or {}
+    srow = srow if srow is not None else [pixdim[0], 0, 0, 0, 0, pixdim[1], 0, 0, 0, 0, pixdim[2], 0]
+    vals = data.astype(data.dtype.newbyteorder(e), copy=False).tobytes()
+    if version == 1:
+        h = bytearray(352)
+        struct.pack_into(e + "i", h, 0, 348)
+        struct.pack_into(e + "8h", h, 40, *dims)
+        struct.pack_into(e + "hh", h, 70, datatype, bitpix)
+        struct.pack_into(e + "8f", h, 76, *pix)
+        struct.pack_into(e + "fff", h, 108, 352.0, slope, inter)
+        struct.pack_into(e + "hh", h, 252, qform_code, sform)
+        struct.pack_into(e + "6f", h, 256, q.get("b", 0.0), q.get("c", 0.0), q.get("d", 0.0), q.get("x", 0.0),
+                         q.get("y", 0.0), q.get("z", 0.0))
+        struct.pack_into(e + "12f", h, 280, *srow)
+        h[344:348] = (magic or b"n+1\0")
+        if magic == b"ni1\0":
+            return bytes(h[:348]), vals
+        return bytes(h) + vals, None
+    h = bytearray(544)
+    struct.pack_into(e + "i", h, 0, 540)
+    h[4:12] = b"n+2\0\r\n\x1a\n"
+    struct.pack_into(e + "hh", h, 12, datatype, bitpix)
+    struct.pack_into(e + "8q", h, 16, *dims)
+    struct.pack_into(e + "8d", h, 104, *pix)
+    struct.pack_into(e + "q", h, 168, 544)
+    struct.pack_into(e + "dd", h, 176, slope, inter)
+    struct.pack_into(e + "ii", h, 344, qform_code, sform)
+    struct.pack_into(e + "6d", h, 352, q.get("b", 0.0), q.get("c", 0.0), q.get("d", 0.0), q.get("x", 0.0),
+                     q.get("y", 0.0), q.get("z", 0.0))
+    struct.pack_into(e + "12d", h, 400, *srow)
+    return bytes(h) + vals, None
+
+
+def nifti_cases():
+    """(name, array (z, y, x), datatype, bitpix, keyword arguments of nifti_bytes)."""
+    rng = np.random.default_rng(ph.seed_for(6, 1))
+    sh = (5, 9, 7)
+    lps = [-1.5, 0, 0, 40.0, 0, -1.25, 0, 30.0, 0, 0, 2.0, -20.0]  # already LPS: no steps
+    ras = [1.5, 0, 0, -40.0, 0, 1.25, 0, -30.0, 0, 0, 2.0, -20.0]   # flips x and y
+    swap_xy = [0, 1.25, 0, -10.0, 1.5, 0, 0, -20.0, 0, 0, 2.0, 5.0]
+    swap_xz = [0, 0, -2.0, 3.0, 0, -1.25, 0, 7.0, 1.5, 0, 0, -9.0]
+    swap_yz = [-1.5, 0, 0, 1.0, 0, 0, 2.0, 2.0, 0, -1.25, 0, 3.0]
+    oblique = [1.4, 0.3, 0.05, -12.0, -0.2, 1.2, 0.4, 8.0, 0.1, -0.35, 1.9, 2.0]
+    return [
+        ("u8_lps", (rng.random(sh) * 255).astype(np.uint8), 2, 8, dict(srow=lps, pixdim=(1.5, 1.25, 2.0))),
+        ("i16_ras_scaled", rng.integers(-3000, 3000, sh).astype(np.int16), 4, 16,
+         dict(srow=ras, pixdim=(1.5, 1.25, 2.0), slope=2.5, inter=-3.0)),
+        ("f32_be_swapxy", rng.normal(0, 100, sh).astype(np.float32), 16, 32,
+         dict(srow=swap_xy, pixdim=(1.25, 1.5, 2.0), big=True)),
+        ("f64_nifti2_swapxz", rng.normal(0, 1e3, sh).astype(np.float64), 64, 64,
+         dict(srow=swap_xz, pixdim=(2.0, 1.25, 1.5), version=2)),
+        ("i32_qform", rng.integers(-2 ** 30, 2 ** 30, sh).astype(np.int32), 8, 32,
+         dict(pixdim=(1.1, 1.2, 1.3), qform={"b": 0.0, "c": 0.0, "d": 0.70710677, "x": 5.0, "y": -6.0, "z": 7.0,
+                                            "qfac": -1.0})),
+        ("u16_pair_swapyz", rng.integers(0, 65535, sh).astype(np.uint16), 512, 16,
+         dict(srow=swap_yz, pixdim=(1.5, 2.0, 1.25), magic=b"ni1\0")),
+        ("i8_oblique", rng.integers(-128, 127, sh).astype(np.int8), 256, 8, dict(srow=oblique)),
+        ("u32_be", rng.integers(0, 2 ** 32 - 1, sh, dtype=np.uint64).astype(np.uint32), 768, 32,
+         dict(srow=ras, big=True)),
+        ("i64_nifti2_be", rng.integers(-2 ** 60, 2 ** 60, sh, dtype=np.int64), 1024, 64,
+         dict(srow=lps, version=2, big=True, slope=0.5)),
+        ("u64", rng.integers(0, 2 ** 63, sh, dtype=np.uint64) * np.uint64(2), 1280, 64, dict(srow=ras, inter=1.0)),
+        ("i16_4d", rng.integers(-500, 500, (2,) + sh).astype(np.int16).reshape(2 * sh[0], sh[1], sh[2]), 4, 16,
+         dict(srow=ras, extra_dims=(2,))),
+        ("f32_mni", rng.random(sh).astype(np.float32), 16, 32,
+         dict(srow=[-1.0, 0, 0, 90.0, 0, -1.0, 0, 126.0, 0, 0, 1.0, -72.0], sform_code=4)),
+    ]
+
+
+def write_nifti_case(name, arr, dt, bp, kw, gz):
+    os.makedirs(NIFTI_DIR, exist_ok=True)
+    import gzip
+
+    head, img = nifti_bytes(arr, dt, bp, **kw)
+    if kw.get("extra_dims"):
+        # a NIfTI-1 4-D file: arr stacks the volumes along z; dim[3] is one volume's depth
+        import struct
+
+        e = ">" if kw.get("big") else "<"
+        hb = bytearray(head)
+        struct.pack_into(e + "h", hb, 46, arr.shape[0] // kw["extra_dims"][0])
+        head = bytes(hb)
+    if img is not None:
+        path = os.path.join(NIFTI_DIR, name + ".hdr")
+        open(path, "wb").write(head)
+        open(os.path.join(NIFTI_DIR, name + ".img"), "wb").write(img)
+        return path
+    path = os.path.join(NIFTI_DIR, name + (".nii.gz" if gz else ".nii"))
+    if gz:
+        with gzip.GzipFile(path, "wb", mtime=0) as f:
+            f.write(head)
+    else:
+        open(path, "wb").write(head)
+    return path
+
+
+def nifti(R):
+    """NIfTI files of every datatype, byte order and header form, read by the reference's
+    gz_nifti (>> I >> vs >> T >> is_mni); the files sit in tests/golden/nifti/."""
+    out = {}
+    for k, (name, arr, dt, bp, kw) in enumerate(nifti_cases()):
+        path = write_nifti_case(name, arr, dt, bp, kw, gz=(k % 2 == 1))
+        r = R.nifti_load(path)
+        assert r is not None, name
+        I, vs, srow, mni = r
+        out[name + "_path"] = np.array(os.path.relpath(path, HERE))
+        out[name + "_I"] = I
+        out[name + "_vs"] = vs
+        out[name + "_srow"] = srow
+        out[name + "_mni"] = np.array(mni)
+    save("nifti", **out)
 
 
 def mi32(R):

@@ -15,6 +15,7 @@ tipl::accumulate_displacement  ``accumulate_displacement(dis, new_dis)``
 mutual_information / corr      ``mi_cost`` / ``corr_cost`` (K transforms at once); ``mi32_cost``
                                the 32x32-bin MI variant
 transformation_matrix(...)     ``affine_to_matrix(param, ...)``
+gz_nifti >> I >> vs >> T       ``nifti_load(path)`` / ``nifti_info`` / ``nifti_save``
 =============================  ===================================================
 
 Arrays are numpy arrays shaped (z, y, x) (x-fastest memory, the reference's
@@ -32,7 +33,8 @@ from . import _lib
 from ._lib import CdmParam, Field, LinearParam, RegbError, Volume  # noqa: F401
 
 __all__ = ["affine_to_matrix", "affine_to_matrix_f64", "matrix_inverse", "resample", "mi_cost", "mi32_cost", "corr_cost",
-           "compose_displacement", "accumulate_displacement", "downsample", "upsample_field_x2", "cdm_gradient",
+           "nifti_info", "nifti_load", "nifti_save", "compose_displacement", "accumulate_displacement", "downsample",
+           "upsample_field_x2", "cdm_gradient",
            "cdm_poisson", "cdm_max_length", "cdm_smooth", "reg", "Engine", "RegbError", "version"]
 
 
@@ -312,6 +314,53 @@ def corr_cost(fixed, moving, Ts, stream=None):
     _lib.check(_lib.lib().regb_corr_cost(C.byref(_vol(fixed)), C.byref(_vol(moving)), _fptr(Tm), K, _fptr(cost),
                                          _stream(stream)))
     return cost
+
+
+# ---------------------------------------------------------------- NIfTI volumes (io/nifti.hpp)
+def nifti_info(path) -> dict:
+    """The geometry tipl::io::gz_nifti reports for a .nii / .nii.gz / .hdr file after its
+    LPS reorientation: dims (x, y, z), voxel size, srow rows, and the reorientation steps."""
+    info = _lib.NiftiInfo()
+    _lib.check(_lib.lib().regb_nifti_info_read(str(path).encode(), C.byref(info)))
+    return _info_dict(info)
+
+
+def _info_dict(info) -> dict:
+    return {"dim": tuple(info.dim), "vs": np.array(info.vs, np.float32), "srow": np.array(info.srow, np.float32),
+            "file_dim": tuple(info.file_dim), "datatype": info.datatype, "bitpix": info.bitpix,
+            "nvolumes": info.nvolumes, "scl_slope": info.scl_slope, "scl_inter": info.scl_inter,
+            "sform_code": info.sform_code, "is_mni": bool(info.is_mni), "big_endian": bool(info.big_endian),
+            "nifti2": bool(info.nifti2), "steps": list(info.steps[:info.n_steps]),
+            "descrip": info.descrip.decode(errors="replace")}
+
+
+def nifti_load(path, volume=0, device=None, stream=None):
+    """nii >> I >> vs >> T: volume `volume` as a float32 (z, y, x) array in LPS
+    orientation -- a CUDA torch tensor when device is given, else a numpy array -- and
+    the info dict (vs, srow, ...).  The conversion and reorientation run on the GPU."""
+    info = nifti_info(path)
+    x, y, z = info["dim"]
+    if device is not None:
+        import torch
+
+        out = torch.zeros((z, y, x), dtype=torch.float32, device=device)
+    else:
+        out = np.zeros((z, y, x), np.float32)
+    _lib.check(_lib.lib().regb_nifti_load(str(path).encode(), int(volume), C.byref(_vol(out)), None,
+                                          _stream(stream)))
+    return out, info
+
+
+def nifti_save(path, vol, vs=(1.0, 1.0, 1.0), srow=None, is_mni=False, descrip=None):
+    """nii << vs << T << I: writes a uint8 / uint16 / float32 (z, y, x) volume (host
+    array or CUDA tensor) as NIfTI-1, gzip-compressed when path ends in .gz."""
+    if srow is None:
+        srow = np.array([vs[0], 0, 0, 0, 0, vs[1], 0, 0, 0, 0, vs[2], 0], np.float32)
+    v = vol if _is_dev(vol) else np.ascontiguousarray(vol)
+    _lib.check(_lib.lib().regb_nifti_save(str(path).encode(), C.byref(_vol(v)),
+                                          _fptr(np.ascontiguousarray(vs, np.float32)),
+                                          _fptr(np.ascontiguousarray(srow, np.float32)), int(bool(is_mni)),
+                                          descrip.encode() if descrip else None))
 
 
 # ---------------------------------------------------------------- displacement algebra / CDM passes

@@ -60,6 +60,13 @@ class EngineConfig(C.Structure):
                 ("cdm_iters_per_round", C.c_int)]
 
 
+class NiftiInfo(C.Structure):
+    _fields_ = [("dim", C.c_int * 3), ("vs", C.c_float * 3), ("srow", C.c_float * 12), ("file_dim", C.c_int * 8),
+                ("datatype", C.c_int), ("bitpix", C.c_int), ("nvolumes", C.c_int), ("scl_slope", C.c_float),
+                ("scl_inter", C.c_float), ("sform_code", C.c_int), ("is_mni", C.c_int), ("big_endian", C.c_int),
+                ("nifti2", C.c_int), ("n_steps", C.c_int), ("steps", C.c_int * 8), ("descrip", C.c_char * 81)]
+
+
 class Job(C.Structure):
     _fields_ = [("template_id", C.c_int), ("fixed", Volume), ("fixed_vs", C.c_float * 3), ("moving", Volume),
                 ("moving_vs", C.c_float * 3), ("run_linear", C.c_int), ("linear", LinearParam),
@@ -112,6 +119,9 @@ _SIGS = {
     "regb_inv_displacement_to_mapping": (C.c_int, [C.c_void_p] * 4),
     "regb_compose_mapping": (C.c_int, [C.c_void_p] * 4),
     "regb_match_fov": (C.c_int, [C.c_void_p] * 5),
+    "regb_nifti_info_read": (C.c_int, [C.c_char_p, C.POINTER(NiftiInfo)]),
+    "regb_nifti_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(Volume), C.c_void_p, C.c_void_p]),
+    "regb_nifti_save": (C.c_int, [C.c_char_p, C.POINTER(Volume), C.c_void_p, C.c_void_p, C.c_int, C.c_char_p]),
     "regb_correlation": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     "regb_subject_image_pre": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "regb_estimate_affine_param": (C.c_int, [C.c_void_p] * 5),

@@ -71,7 +71,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose or ptxas_info, extra), srcs))
     tmp = OUT + ".tmp"
-    cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lpthread", "-ldl", "-lrt"]
+    cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lz", "-lpthread", "-ldl", "-lrt"]
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -1,6 +1,7 @@
 // extern "C" entry points of libregb200.so (declared in include/regb200.h).
 // Every entry validates its views, stages host memory through device buffers when
 // a view lives on the host, and turns failures into regb_status codes.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -8,6 +9,7 @@
 #include "affine_eval.h"
 #include "cdm_level.h"
 #include "host.h"
+#include "nifti.h"
 #include "mask_init.h"
 #include "preprocess.h"
 #include "stats.h"
@@ -468,6 +470,119 @@ regb_status regb_corr_cost(const regb_volume* fixed, const regb_volume* moving, 
                            void* stream)
 {
     return affine_cost(fixed, moving, T, K, cost, nullptr, REGB_COST_CORR, stream);
+}
+
+static void fill_nifti_info(const NiftiFile& f, regb_nifti_info* info)
+{
+    std::memset(info, 0, sizeof(*info));
+    const NiftiHeader& h = f.h;
+    for (int i = 0; i < 3; ++i) {
+        info->dim[i] = h.dim[i + 1];
+        info->vs[i] = h.pixdim[i + 1];
+    }
+    std::memcpy(info->srow, h.srow, sizeof(info->srow));
+    for (int i = 0; i < 8; ++i)
+        info->file_dim[i] = f.file_dim[i];
+    info->datatype = h.datatype;
+    info->bitpix = h.bitpix;
+    long long nvol = 1;
+    for (int i = 4; i <= 7 && i <= f.file_dim[0]; ++i)
+        nvol *= std::max<int>(f.file_dim[i], 1);
+    info->nvolumes = (int)nvol;
+    info->scl_slope = h.scl_slope;
+    info->scl_inter = h.scl_inter;
+    info->sform_code = h.sform_code;
+    const float* R = h.srow;
+    // gz_nifti::is_mni (io/nifti.hpp:856-864)
+    info->is_mni = h.sform_code >= 4 && R[3] != 0.0f && R[7] != 0.0f && R[11] != 0.0f && R[1] == 0.0f &&
+                   R[2] == 0.0f && R[4] == 0.0f && R[6] == 0.0f && R[8] == 0.0f && R[9] == 0.0f;
+    info->big_endian = h.big_endian ? 1 : 0;
+    info->nifti2 = h.nifti2 ? 1 : 0;
+    info->n_steps = (int)f.seq.size();
+    for (size_t i = 0; i < f.seq.size() && i < 8; ++i)
+        info->steps[i] = f.seq[i];
+    std::memcpy(info->descrip, h.descrip, 80);
+    info->descrip[80] = 0;
+}
+
+regb_status regb_nifti_info_read(const char* path, regb_nifti_info* info)
+{
+    return guarded([&] {
+        if (!path || !info)
+            throw Failure(REGB_ERR_ARG, "null argument");
+        fill_nifti_info(nifti_open(path), info);
+        return REGB_OK;
+    });
+}
+
+regb_status regb_nifti_load(const char* path, int volume, regb_volume* out, regb_nifti_info* info, void* stream)
+{
+    return guarded([&] {
+        if (!path)
+            throw Failure(REGB_ERR_ARG, "null path");
+        check_vol(out, "out");
+        if (out->dtype != REGB_F32)
+            throw Failure(REGB_ERR_ARG, "regb_nifti_load writes float32 volumes");
+        const NiftiFile f = nifti_open(path);
+        if (info)
+            fill_nifti_info(f, info);
+        for (int i = 0; i < 3; ++i)
+            if (out->dim[i] != f.h.dim[i + 1])
+                throw Failure(REGB_ERR_ARG, "out dims differ from the file's (LPS) dims");
+        const std::vector<uint8_t> bytes = nifti_read_voxels(path, f, volume);
+        cudaStream_t st = (cudaStream_t)stream;
+        DevBuf<uint8_t> raw(bytes.size(), st);
+        REGB_CK(cudaMemcpyAsync(raw.p, bytes.data(), bytes.size(), cudaMemcpyHostToDevice, st));
+        Staged o;
+        o.in(out->ptr, nvox(out->dim) * sizeof(float), out->location, st, false);
+        NiftiMap m;
+        m.file = Dim3{f.file_dim[1], f.file_dim[2], f.file_dim[3]};
+        m.out = Dim3{out->dim[0], out->dim[1], out->dim[2]};
+        std::memcpy(m.M, f.M, sizeof(m.M));
+        for (int i = 0; i < 3; ++i)
+            m.o[i] = f.o[i];
+        m.datatype = f.h.datatype;
+        m.big_endian = f.h.big_endian ? 1 : 0;
+        m.scl_slope = f.h.scl_slope;
+        m.scl_inter = f.h.scl_inter;
+        REGB_CK(launch_nifti_convert(raw.p, m, (float*)o.d, st));
+        o.out(out->ptr, st);
+        if (o.host)
+            REGB_CK(cudaStreamSynchronize(st));
+        return REGB_OK;
+    });
+}
+
+regb_status regb_nifti_save(const char* path, const regb_volume* vol, const float vs[3], const float srow[12],
+                            int is_mni, const char* descrip)
+{
+    return guarded([&] {
+        if (!path || !vs || !srow)
+            throw Failure(REGB_ERR_ARG, "null argument");
+        check_vol(vol, "vol", false);
+        // the reference's type table (io/nifti.hpp:264-330): uint16 is written with the
+        // int16 code
+        int dt = 0, bp = 0;
+        switch (vol->dtype) {
+        case REGB_U8: dt = 2; bp = 8; break;
+        case REGB_U16: dt = 4; bp = 16; break;
+        case REGB_F32: dt = 16; bp = 32; break;
+        default: throw Failure(REGB_ERR_ARG, "regb_nifti_save takes U8, U16 or F32 volumes");
+        }
+        for (int i = 0; i < 3; ++i)
+            if (vol->dim[i] > 32767)
+                throw Failure(REGB_ERR_ARG, "NIfTI-1 dims are at most 32767");
+        const size_t bytes = nvox(vol->dim) * (size_t)(bp / 8);
+        std::vector<uint8_t> h;
+        const void* data = vol->ptr;
+        if (vol->location == REGB_DEVICE) {
+            h.resize(bytes);
+            REGB_CK(cudaMemcpy(h.data(), vol->ptr, bytes, cudaMemcpyDeviceToHost));
+            data = h.data();
+        }
+        nifti_write(path, data, dt, bp, vol->dim, vs, srow, is_mni ? 4 : 1, descrip);
+        return REGB_OK;
+    });
 }
 
 regb_status regb_compose_displacement(const regb_volume* from, const regb_field* dis, regb_volume* to, void* stream)

@@ -174,6 +174,19 @@ cudaError_t launch_moments_u8(const uint8_t* x, const uint8_t* y, long long n, i
 // out = It where T(x) lies inside a volume of shape MD, else 0 (mm_reg's It_match_fov)
 cudaError_t launch_match_fov_u8(const uint8_t* It, Dim3 FD, const float* T, Dim3 MD, uint8_t* out, cudaStream_t st);
 
+// One NIfTI volume from its stored bytes to the float32 LPS volume (nifti_kernels.cu):
+// out voxel v reads file voxel M v + o; datatype is the NIfTI code.
+struct NiftiMap {
+    Dim3 file;  // dims as stored
+    Dim3 out;   // dims after the reorientation
+    int M[9];
+    long long o[3];
+    int datatype;
+    int big_endian;
+    float scl_slope, scl_inter;
+};
+cudaError_t launch_nifti_convert(const uint8_t* raw, const NiftiMap& m, float* out, cudaStream_t st);
+
 // Voxels > 0 per (x, y), (x, z), (y, z) line of a uint8 volume (zeroes the tables first).
 cudaError_t launch_mask_counts(const uint8_t* v, Dim3 dim, uint32_t* xy, uint32_t* xz, uint32_t* yz,
                                cudaStream_t st);
