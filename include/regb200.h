@@ -106,6 +106,8 @@ typedef struct {
     double mi_voxels, mi_bytes, mi_ms;
     long long corr_launches, corr_tasks;
     double corr_voxels, corr_bytes, corr_ms;
+    double mi_busy_ms;   /* union of the MI launches' device intervals (launches on two
+                            streams may overlap, so it can be below mi_ms) */
 } regb_stats;
 regb_status regb_stats_reset(int timing);
 regb_status regb_stats_get(regb_stats* out);

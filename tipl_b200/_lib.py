@@ -46,7 +46,7 @@ class Stats(C.Structure):
     _fields_ = [("launches", C.c_longlong), ("mi_launches", C.c_longlong), ("mi_tasks", C.c_longlong),
                 ("mi_voxels", C.c_double), ("mi_bytes", C.c_double), ("mi_ms", C.c_double),
                 ("corr_launches", C.c_longlong), ("corr_tasks", C.c_longlong), ("corr_voxels", C.c_double),
-                ("corr_bytes", C.c_double), ("corr_ms", C.c_double)]
+                ("corr_bytes", C.c_double), ("corr_ms", C.c_double), ("mi_busy_ms", C.c_double)]
 
 
 class RunnerState(C.Structure):

@@ -6,13 +6,15 @@ namespace regb {
 
 AffineBatcher::AffineBatcher(int gather_us) : gather_us_(gather_us)
 {
-    REGB_CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     int dev = 0;
     REGB_CK(cudaGetDevice(&dev));
-    th_ = std::thread([this, dev] {
-        cudaSetDevice(dev);
-        loop();
-    });
+    for (Worker& w : workers_)
+        REGB_CK(cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking));
+    for (Worker& w : workers_)
+        w.th = std::thread([this, dev, &w] {
+            cudaSetDevice(dev);
+            loop(w);
+        });
 }
 
 AffineBatcher::~AffineBatcher()
@@ -22,13 +24,16 @@ AffineBatcher::~AffineBatcher()
         stop_ = true;
     }
     cv_req_.notify_all();
-    if (th_.joinable())
-        th_.join();
-    for (TaskScratch& s : scratch_)
-        s.release();
-    if (st_) {
-        cudaStreamSynchronize(st_);
-        cudaStreamDestroy(st_);
+    for (Worker& w : workers_)
+        if (w.th.joinable())
+            w.th.join();
+    for (Worker& w : workers_) {
+        for (TaskScratch& s : w.scratch)
+            s.release();
+        if (w.st) {
+            cudaStreamSynchronize(w.st);
+            cudaStreamDestroy(w.st);
+        }
     }
 }
 
@@ -62,18 +67,23 @@ void AffineBatcher::eval(const AffineTask* tasks, int n, int cost_type, double* 
         std::rethrow_exception(r.err);
 }
 
-void AffineBatcher::loop()
+void AffineBatcher::loop(Worker& w)
 {
     std::unique_lock<std::mutex> lk(m_);
     for (;;) {
         cv_req_.wait(lk, [&] { return stop_ || !pending_.empty(); });
         if (stop_ && pending_.empty())
             return;
-        // the device is free: give the other jobs a moment to join this batch
+        // give the jobs that could still submit (those not waiting on the other
+        // worker's batch) a moment to join this one
         const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(gather_us_);
-        cv_req_.wait_until(lk, until, [&] { return stop_ || (int)pending_.size() >= clients_; });
+        cv_req_.wait_until(lk, until,
+                           [&] { return stop_ || (int)pending_.size() >= clients_ - inflight_; });
+        if (pending_.empty())
+            continue;  // the other worker took them
         std::vector<Req*> batch(pending_.begin(), pending_.end());
         pending_.clear();
+        inflight_ += (int)batch.size();
         lk.unlock();
         for (int ct = 0; ct < kCostTypes; ++ct) {
             int total = 0;
@@ -83,8 +93,8 @@ void AffineBatcher::loop()
             if (!total)
                 continue;
             try {
-                TaskScratch& s = scratch_[ct];
-                s.ensure(total, ct != REGB_COST_CORR, st_);
+                TaskScratch& s = w.scratch[ct];
+                s.ensure(total, ct != REGB_COST_CORR, w.st);
                 int k = 0;
                 for (Req* r : batch)
                     if (r->cost_type == ct) {
@@ -92,7 +102,7 @@ void AffineBatcher::loop()
                         k += r->n;
                     }
                 std::vector<double> c(total);
-                run_affine_tasks(s, total, ct, st_, c.data());
+                run_affine_tasks(s, total, ct, w.st, c.data());
                 k = 0;
                 for (Req* r : batch)
                     if (r->cost_type == ct) {
@@ -108,9 +118,11 @@ void AffineBatcher::loop()
             }
         }
         lk.lock();
+        inflight_ -= (int)batch.size();
         for (Req* r : batch)
             r->done = true;
         cv_done_.notify_all();
+        cv_req_.notify_all();  // the other worker may be waiting for jobs of this batch
     }
 }
 

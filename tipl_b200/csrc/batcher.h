@@ -1,5 +1,6 @@
 // Cross-job batching of affine cost evaluations (the serving engine's affine stage).
 #pragma once
+#include <atomic>
 #include <condition_variable>
 #include <deque>
 #include <exception>
@@ -13,7 +14,7 @@ namespace regb {
 constexpr int kCostTypes = 3;  // REGB_COST_CORR, REGB_COST_MI, REGB_COST_MI32
 
 // Collects cost-evaluation requests from many jobs and evaluates all pending ones
-// of a cost type in one launch.  A request's tasks carry their own volumes, so
+// of a cost type in one launch (two launches may be in flight, on two streams).  A request's tasks carry their own volumes, so
 // requests of different jobs, shapes and pyramid levels mix freely; every task's
 // cost depends only on its own inputs, whatever it is batched with.
 class AffineBatcher {
@@ -30,8 +31,8 @@ public:
     void add_client();
     void remove_client();
 
-    long long launches() const { return launches_; }
-    long long tasks_evaluated() const { return tasks_; }
+    long long launches() const { return launches_.load(); }
+    long long tasks_evaluated() const { return tasks_.load(); }
 
 private:
     struct Req {
@@ -42,17 +43,25 @@ private:
         bool done = false;
         std::exception_ptr err;
     };
-    void loop();
+    // Two workers, each with its own stream and scratch: while one batch runs on the
+    // device, the jobs it does not hold can form the next batch, which the other worker
+    // launches at once instead of after the first batch's results are back.
+    static constexpr int kWorkers = 2;
+    struct Worker {
+        TaskScratch scratch[kCostTypes];  // one per cost type (REGB_COST_CORR, _MI, _MI32)
+        cudaStream_t st = nullptr;
+        std::thread th;
+    };
+    void loop(Worker& w);
     std::mutex m_;
     std::condition_variable cv_req_, cv_done_;
     std::deque<Req*> pending_;
     int clients_ = 0;
+    int inflight_ = 0;  // requests taken by a worker and not yet answered
     bool stop_ = false;
     int gather_us_;
-    long long launches_ = 0, tasks_ = 0;
-    TaskScratch scratch_[kCostTypes];  // one per cost type (REGB_COST_CORR, _MI, _MI32)
-    cudaStream_t st_ = nullptr;
-    std::thread th_;
+    std::atomic<long long> launches_{0}, tasks_{0};
+    Worker workers_[kWorkers];
 };
 
 }  // namespace regb
