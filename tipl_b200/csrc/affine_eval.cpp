@@ -86,7 +86,13 @@ void TexVol::build(const uint8_t* v, Dim3 d, cudaStream_t st)
     td.filterMode = cudaFilterModePoint;
     td.readMode = cudaReadModeElementType;
     td.normalizedCoords = 0;
-    REGB_CK(cudaCreateTextureObject(&t, &rd, &td, nullptr));
+    if (cudaCreateTextureObject(&t, &rd, &td, nullptr) != cudaSuccess) {
+        // no texture (e.g. the device's texture objects are used up): the byte-load
+        // kernels read the volume instead, with the same results
+        (void)cudaGetLastError();
+        t = 0;
+        mem.reset();
+    }
 }
 
 void set_task_chunks(AffineTask& t, int cost_type)
