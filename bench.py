@@ -670,6 +670,98 @@ def run_served(args, rank, world, dist):
     return t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects, plain
 
 
+def poisson_case(args):
+    """Open-loop serving: registration jobs arrive as a Poisson stream (--rate per second for
+    --duration seconds).  Each job is affine + CDM of a random-shape subject (64^3 up to
+    256x256x200 voxels, uint16 or float32, phantoms as in the affine workload) against one
+    of four resident templates (64^3, 128^3, 182x218x182, 256^3), admitted under a 150 GB
+    device-memory budget.  Subjects are host arrays (each job copies its own in).
+    Reports completed jobs/s and the arrival-to-result latency percentiles, beside the
+    same kind of job run as plain single-job calls one after another."""
+    import threading
+
+    import torch
+
+    import tipl_b200 as tb
+    from tipl_b200 import phantom as ph
+
+    rng = np.random.default_rng(ph.seed_for(5, 100))
+    tshapes = [(64, 64, 64), (128, 128, 128), (182, 218, 182), (256, 256, 256)]
+    templates = [ph.normalize_to_u8(ph.class_phantom(s, rng)) for s in tshapes]
+    pool = []
+    for k in range(12):
+        shape = (int(rng.integers(64, 201)), int(rng.integers(64, 257)), int(rng.integers(64, 257)))
+        base = torch.from_numpy(ph.class_phantom(shape, rng)).cuda()
+        T = tb.affine_to_matrix(ph.random_affine(rng, rot_deg=10, trans_vox=10), shape, VS, shape, VS)
+        moved = tb.resample(base, shape, T).cpu().numpy()
+        noisy = ph.rician(moved, rng)
+        pool.append(np.round(np.clip(noisy, 0, 4095)).astype(np.uint16) if k % 2 == 0 else noisy.astype(np.float32))
+    cdm_p = tb.reg.cdm_param()
+
+    def plain(t, m):
+        q = lambda v: v if v.dtype == np.uint8 else tb.normalize_to_u8(v)[0]  # noqa: E731
+        _, arg, _ = tb.reg.linear(q(t), VS, q(m), VS)
+        T = tb.affine_to_matrix(arg, t.shape, VS, m.shape, VS)
+        w = lambda v: v if v.dtype == np.float32 else tb.widen_to_f32(v)  # noqa: E731
+        tb.reg.cdm(w(t), tb.resample(w(m), t.shape, T, allow_shift_copy=True), param=cdm_p)
+
+    plain_jobs = [(int(rng.integers(0, 4)), int(rng.integers(0, len(pool)))) for _ in range(4)]
+    plain(templates[0], pool[0])  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for ti, si in plain_jobs:
+        plain(templates[ti], pool[si])
+    torch.cuda.synchronize()
+    plain_rate = len(plain_jobs) / (time.perf_counter() - t0)
+
+    arrivals = []
+    t = 0.0
+    while True:
+        t += float(rng.exponential(1.0 / args.rate))
+        if t > args.duration:
+            break
+        arrivals.append((t, int(rng.integers(0, 4)), int(rng.integers(0, len(pool)))))
+    with tb.Engine(hbm_budget_bytes=150 << 30, max_active=32) as eng:
+        tids = [eng.add_template(tm) for tm in templates]
+        for ti in range(4):  # warm-up: one job per template
+            eng.wait(eng.submit(pool[ti], template=tids[ti], cdm=True, cdm_param=cdm_p))
+        ids = [None] * len(arrivals)
+        sub_t = [0.0] * len(arrivals)
+        start = time.perf_counter()
+
+        def feed():
+            for k, (ta, ti, si) in enumerate(arrivals):
+                dt = ta - (time.perf_counter() - start)
+                if dt > 0:
+                    time.sleep(dt)
+                sub_t[k] = time.perf_counter() - start
+                ids[k] = eng.submit(pool[si], template=tids[ti], cdm=True, cdm_param=cdm_p)
+
+        th = threading.Thread(target=feed)
+        th.start()
+        lat, done_at, ok = [], [], 0
+        for k in range(len(arrivals)):
+            while ids[k] is None:
+                time.sleep(0.0005)
+            r = eng.wait(ids[k])
+            ok += int(r["status"] == 0 and r["cdm_ok"])
+            lat.append(r["queued_ms"] + r["run_ms"])
+            done_at.append(sub_t[k] + (r["queued_ms"] + r["run_ms"]) / 1000.0)
+        th.join()
+    span = max(done_at) - sub_t[0]
+    lat_s = sorted(lat)
+    pct = lambda q: lat_s[min(len(lat_s) - 1, int(q * len(lat_s)))]  # noqa: E731
+    print(json.dumps({"workload": "poisson serving: affine + CDM, 4 resident templates, random-shape uint16/float32 "
+                                  "subjects, 150 GB budget",
+                      "metric": "registrations/s (open-loop Poisson arrivals) and latency",
+                      "rate_per_s": args.rate, "duration_s": args.duration, "jobs": len(arrivals), "ok": ok,
+                      "completed_per_s": len(arrivals) / span,
+                      "latency_ms": {"p50": pct(0.50), "p95": pct(0.95), "p99": pct(0.99), "max": lat_s[-1]},
+                      "plain_sequential_jobs_per_s": plain_rate,
+                      "template_shapes": [list(s) for s in tshapes], "data": "synthetic"}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -691,9 +783,15 @@ def main():
     ap.add_argument("--ref-gpu-sample", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--pipeline", choices=["mm_reg"], default=None,
                     help="serve the whole mm_reg pipeline (preprocessing, affine, bidirectional CDM, mappings)")
+    ap.add_argument("--workload", choices=["poisson"], default=None,
+                    help="open-loop serving of affine+CDM jobs arriving as a Poisson stream")
+    ap.add_argument("--rate", type=float, default=20.0, help="--workload poisson: arrivals per second")
+    ap.add_argument("--duration", type=float, default=15.0, help="--workload poisson: seconds of arrivals")
     args = ap.parse_args()
     if args.pipeline == "mm_reg":
         return mm_reg_case(args)
+    if args.workload == "poisson":
+        return poisson_case(args)
     if args.ref_gpu_sample:
         return ref_gpu_sample(args)
     if args.precision_report:
