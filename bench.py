@@ -721,7 +721,7 @@ def poisson_case(args):
         if t > args.duration:
             break
         arrivals.append((t, int(rng.integers(0, 4)), int(rng.integers(0, len(pool)))))
-    with tb.Engine(hbm_budget_bytes=150 << 30, max_active=32) as eng:
+    with tb.Engine(hbm_budget_bytes=150 << 30, max_active=args.max_active) as eng:
         tids = [eng.add_template(tm) for tm in templates]
         for ti in range(4):  # warm-up: one job per template
             eng.wait(eng.submit(pool[ti], template=tids[ti], cdm=True, cdm_param=cdm_p))
@@ -737,6 +737,10 @@ def poisson_case(args):
                 sub_t[k] = time.perf_counter() - start
                 ids[k] = eng.submit(pool[si], template=tids[ti], cdm=True, cdm_param=cdm_p)
 
+        from tipl_b200 import _lib
+
+        L = _lib.lib()
+        L.regb_stats_reset(1)
         th = threading.Thread(target=feed)
         th.start()
         lat, done_at, ok = [], [], 0
@@ -748,15 +752,28 @@ def poisson_case(args):
             lat.append(r["queued_ms"] + r["run_ms"])
             done_at.append(sub_t[k] + (r["queued_ms"] + r["run_ms"]) / 1000.0)
         th.join()
+        st = _lib.Stats()
+        L.regb_stats_get(st)
+        L.regb_stats_reset(0)
+        est = eng.stats()
     span = max(done_at) - sub_t[0]
+    by_t = {}
+    for (ta, ti, si), l in zip(arrivals, lat):
+        by_t.setdefault(ti, []).append(l)
     lat_s = sorted(lat)
     pct = lambda q: lat_s[min(len(lat_s) - 1, int(q * len(lat_s)))]  # noqa: E731
     print(json.dumps({"workload": "poisson serving: affine + CDM, 4 resident templates, random-shape uint16/float32 "
                                   "subjects, 150 GB budget",
                       "metric": "registrations/s (open-loop Poisson arrivals) and latency",
-                      "rate_per_s": args.rate, "duration_s": args.duration, "jobs": len(arrivals), "ok": ok,
+                      "rate_per_s": args.rate, "duration_s": args.duration, "max_active": args.max_active,
+                      "jobs": len(arrivals), "ok": ok,
                       "completed_per_s": len(arrivals) / span,
                       "latency_ms": {"p50": pct(0.50), "p95": pct(0.95), "p99": pct(0.99), "max": lat_s[-1]},
+                      "latency_p50_ms_by_template": {"x".join(str(v) for v in tshapes[ti][::-1]): float(np.median(v))
+                                                     for ti, v in sorted(by_t.items())},
+                      "mi_busy_fraction": st.mi_busy_ms / 1000.0 / span,
+                      "engine": {"affine_launches": est["affine_launches"], "affine_tasks": est["affine_tasks"],
+                                 "cdm_rounds": est["cdm_rounds"]},
                       "plain_sequential_jobs_per_s": plain_rate,
                       "template_shapes": [list(s) for s in tshapes], "data": "synthetic"}))
     return 0
@@ -787,6 +804,7 @@ def main():
                     help="open-loop serving of affine+CDM jobs arriving as a Poisson stream")
     ap.add_argument("--rate", type=float, default=20.0, help="--workload poisson: arrivals per second")
     ap.add_argument("--duration", type=float, default=15.0, help="--workload poisson: seconds of arrivals")
+    ap.add_argument("--max-active", type=int, default=32, help="--workload poisson: engine slots")
     args = ap.parse_args()
     if args.pipeline == "mm_reg":
         return mm_reg_case(args)
