@@ -45,9 +45,10 @@ FALLBACK_HBM_GBS = 6650.0
 # 12-candidate launch on the 182x218x182 pair (profiles/mi_kernel_affine_182x218x182.md:
 # 24.44544 MB / 86.65 M voxel evaluations); scaled to each bench launch by its voxels.
 MI_DRAM_BYTES_PER_VOXEL_EVAL = 24.44544e6 / (12 * 7221032)
-COST_NAME = {"mi": "MI", "mi32": "MI (32x32 bins)"}
+COST_NAME = {"mi": "MI", "mi32": "MI (32x32 bins)", "corr": "correlation"}
 COST_DESC = {"mi": "MI 256x256 joint histogram (the reference's)",
-             "mi32": "MI 32x32 joint histogram (both volumes quantised to 0..31 by normalize_upper_lower2(31.99))"}
+             "mi32": "MI 32x32 joint histogram (both volumes quantised to 0..31 by normalize_upper_lower2(31.99))",
+             "corr": "correlation, 1 - r^2 (the reference's corr cost)"}
 
 
 def env_rank():
@@ -451,7 +452,7 @@ def pre_case(args):
 def mm_reg_case(args):
     """The full mm_reg pipeline served: B float32 subjects (the 182x218x182 template under a
     random affine and one of four smooth displacement fields up to 4 voxels, 2% Rician
-    noise) against one resident float32 template, each job = subject_image_pre, affine MI,
+    noise) against one resident float32 template, each job = subject_image_pre, affine (correlation),
     linear r, FOV match, forward + reverse 3-level CDM (levels 23/46/91 iterate), both
     mappings, nonlinear r.  Against the same pipeline run as plain calls one subject at a
     time.  Prints one JSON line (registrations/s, latency percentiles)."""
@@ -472,10 +473,14 @@ def mm_reg_case(args):
     cdm_p = tb.reg.cdm_param(min_dimension=32)
     dev_subj = [torch.from_numpy(m).cuda() for m in subjects]
 
+    lp = tb.reg.linear_param(cost_type={"mi": tb.reg.MI, "mi32": tb.reg.MI32, "corr": tb.reg.CORR}[args.cost])
+
     def plain(m):
         q_t, _ = tb.normalize_to_u8(td)
         q_m = tb.subject_image_pre(m)
-        _, arg, _ = tb.reg.linear(q_t, VS, q_m, VS)
+        # the mm_reg class's affine stage uses correlation (reg/mm_reg.hpp:53), as the
+        # engine's mm_reg jobs do by default
+        _, arg, _ = tb.reg.linear(q_t, VS, q_m, VS, param=lp)
         T = tb.affine_to_matrix(arg, SHAPE, VS, SHAPE, VS)
         J = tb.resample(q_m, SHAPE, T)
         tb.correlation(J, q_t, masked=True)
@@ -498,7 +503,8 @@ def mm_reg_case(args):
         tid = eng.add_template(td)
 
         def step():
-            ids = [eng.submit(m, template=tid, cdm=True, cdm_param=cdm_p, subject_pre=True, mm_reg=True)
+            ids = [eng.submit(m, template=tid, cdm=True, cdm_param=cdm_p, subject_pre=True, mm_reg=True,
+                              linear_param=lp)
                    for m in dev_subj]
             return [eng.wait(i) for i in ids]
 
@@ -518,16 +524,21 @@ def mm_reg_case(args):
                 assert r["status"] == 0, r
                 lat.append(r["queued_ms"] + r["run_ms"])
                 rs.append((r["r_linear"], r["r_nonlinear"]))
+        est = eng.stats()
     lat.sort()
     pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
     served = args.batch * args.steps / sum(times)
-    print(json.dumps({"pipeline": "mm_reg", "metric": "registrations/s (mm_reg: preprocessing, affine MI, "
+    print(json.dumps({"pipeline": "mm_reg", "cost": args.cost,
+                      "metric": f"registrations/s (mm_reg: preprocessing, affine {COST_NAME[args.cost]}, "
                       "bidirectional 3-level CDM, mappings; 182x218x182 float32, 1 mm)", "value": served,
                       "unit": "registrations/s", "subjects_per_step": args.batch, "steps": args.steps,
                       "plain_registrations_per_s": 1.0 / plain_s, "served_over_plain": served * plain_s,
                       "latency_ms": {"p50": pct(0.5), "p95": pct(0.95), "p99": pct(0.99)},
                       "r_linear_mean": float(np.mean([r[0] for r in rs])),
-                      "r_nonlinear_mean": float(np.mean([r[1] for r in rs])), "data": "synthetic"}))
+                      "r_nonlinear_mean": float(np.mean([r[1] for r in rs])),
+                      "engine": {"affine_launches": est["affine_launches"], "affine_tasks": est["affine_tasks"],
+                                 "cdm_rounds": est["cdm_rounds"]},
+                      "data": "synthetic"}))
     return 0
 
 
@@ -603,7 +614,7 @@ def run_served(args, rank, world, dist):
     # the plain single-job path on the same subjects, one registration at a time
     fdev = torch.from_numpy(f8).cuda()
     plain_s = []
-    lp = tb.reg.linear_param(cost_type=tb.reg.MI32 if args.cost == "mi32" else tb.reg.MI)
+    lp = tb.reg.linear_param(cost_type={"mi": tb.reg.MI, "mi32": tb.reg.MI32, "corr": tb.reg.CORR}[args.cost])
     if args.plain_steps:
         tb.reg.linear(fdev, VS, dev_subj[0], VS, param=lp)  # warm-up
         for k in range(args.plain_steps):
@@ -790,7 +801,7 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=8,
                     help="served mode: plain single-job registrations timed afterwards for the served/plain ratio")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cost", choices=["mi", "mi32"], default="mi",
+    ap.add_argument("--cost", choices=["mi", "mi32", "corr"], default=None,
                     help="served / plain affine cost: the reference's 256x256-bin MI, or the 32x32-bin variant")
     ap.add_argument("--kernel-case", choices=["mi", "mi32", "corr", "cdm", "pre", "nifti"], default=None,
                     help="run only K-candidate cost batches of the full-size pair (for profiler captures)")
@@ -806,6 +817,10 @@ def main():
     ap.add_argument("--duration", type=float, default=15.0, help="--workload poisson: seconds of arrivals")
     ap.add_argument("--max-active", type=int, default=32, help="--workload poisson: engine slots")
     args = ap.parse_args()
+    # the affine cost: MI (the reference's linear() default) for the affine workloads,
+    # correlation (the mm_reg class's default, reg/mm_reg.hpp:53) for the mm_reg pipeline
+    if args.cost is None:
+        args.cost = "corr" if args.pipeline == "mm_reg" else "mi"
     if args.pipeline == "mm_reg":
         return mm_reg_case(args)
     if args.workload == "poisson":
@@ -848,7 +863,7 @@ def main():
     md = torch.from_numpy(m8).cuda()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    lp = tb.reg.linear_param(cost_type=tb.reg.MI32 if args.cost == "mi32" else tb.reg.MI)
+    lp = tb.reg.linear_param(cost_type={"mi": tb.reg.MI, "mi32": tb.reg.MI32, "corr": tb.reg.CORR}[args.cost])
 
     def one(fx, mx):
         return tb.reg.linear(fx, VS, mx, VS, param=lp)
@@ -943,8 +958,14 @@ def served_line(args, rank, world, dist, torch):
     hbm, hbm_kind = peaks()
     # the engine keeps up to two MI launches in flight on two streams, so the kernel's
     # rate is its algorithmic bytes over the union of its launches' device intervals
-    busy_ms = st.mi_busy_ms if st.mi_busy_ms > 0 else st.mi_ms
-    achieved = st.mi_bytes / (busy_ms / 1000.0) / 1e9 if st.mi_launches else 0
+    # (the correlation kernel's launches have no union record: their summed times)
+    if args.cost == "corr":
+        k_bytes, k_ms, k_launches, k_voxels, busy_ms = (st.corr_bytes, st.corr_ms, st.corr_launches,
+                                                         st.corr_voxels, st.corr_ms)
+    else:
+        k_bytes, k_ms, k_launches, k_voxels = st.mi_bytes, st.mi_ms, st.mi_launches, st.mi_voxels
+        busy_ms = st.mi_busy_ms if st.mi_busy_ms > 0 else st.mi_ms
+    achieved = k_bytes / (busy_ms / 1000.0) / 1e9 if k_launches else 0
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -984,16 +1005,19 @@ def served_line(args, rank, world, dist, torch):
                            "plain_single_job_ms": plain["ms"] if plain else None,
                            "served_over_plain": (regs / t_dev / world) / plain["median_rate"] if plain else None,
                            "parallelism": f"replicas x{world}"},
-                "roofline": {"bound": "hbm", "kernel": "mi32_kernel" if args.cost == "mi32" else "mi_kernel",
+                "roofline": {"bound": "hbm",
+                             "kernel": {"mi": "mi_kernel", "mi32": "mi32_kernel", "corr": "corr_kernel"}[args.cost],
                              "achieved": achieved, "peak": hbm,
                              "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
-                             "traffic": MI_DRAM_BYTES_PER_VOXEL_EVAL * st.mi_voxels / max(1, st.mi_launches),
+                             "traffic": (MI_DRAM_BYTES_PER_VOXEL_EVAL * k_voxels / max(1, k_launches)
+                                         if args.cost == "mi" else None),
                              "traffic_note": "ncu DRAM bytes per voxel evaluation x this run's voxels per launch",
-                             "launches": st.mi_launches, "avg_launch_ms": st.mi_ms / max(1, st.mi_launches),
+                             "launches": k_launches, "avg_launch_ms": k_ms / max(1, k_launches),
                              "busy_ms": busy_ms,
-                             "achieved_note": "algorithmic bytes of all MI launches / the union of their device "
-                                              "intervals (CUDA events; launches on the engine's two streams overlap)",
-                             "bytes_per_launch": st.mi_bytes / max(1, st.mi_launches)},
+                             "achieved_note": "algorithmic bytes of all the cost kernel's launches / the union of "
+                                              "their device intervals (CUDA events; launches on the engine's two "
+                                              "streams overlap)",
+                             "bytes_per_launch": k_bytes / max(1, k_launches)},
                 "cpu_baseline": cpu,
                 "reference_gpu": ref_gpu,
                 "e2e": {"value": regs / t_e2e, "unit": "registrations/s",

@@ -372,7 +372,10 @@ typedef struct {
     int mm_reg;                /* 1: the rest of the mm_reg pipeline (reg/mm_reg.hpp:286-416) after a
                                   uint8 CDM: the reverse CDM (subject on the template grid against the
                                   template), the mappings, and the linear / nonlinear correlations
-                                  (correlation_ygz) in the result */
+                                  (correlation_ygz) in the result.  The reference's mm_reg
+                                  registers with correlation (reg/mm_reg.hpp:53): set
+                                  linear.cost_type = REGB_COST_CORR to match it (the Python
+                                  Engine.submit does so when mm_reg is set) */
     float* field_rev_out;      /* optional: the reverse displacement (template dims x 3 floats) */
     float* mapping_out;        /* optional: template grid -> subject voxel mapping (template dims x 3) */
     float* inv_mapping_out;    /* optional: subject grid -> template voxel mapping (moving dims x 3) */

@@ -199,7 +199,9 @@ def test_mm_reg_job_outputs_equal_plain_calls(orc):
     m = ph.rician(ph.apply_matrix(ph.class_phantom(s, rng), T0, s), rng)
     q_t, _ = tb.normalize_to_u8(t)
     q_m = tb.subject_image_pre(m)
-    cost, arg, _ = tb.reg.linear(q_t, (1, 1, 1), q_m, (1, 1, 1))
+    # the mm_reg class's linear stage uses correlation (reg/mm_reg.hpp:53); an mm_reg job
+    # submitted without its own linear parameters does the same
+    cost, arg, _ = tb.reg.linear(q_t, (1, 1, 1), q_m, (1, 1, 1), param=tb.reg.linear_param(cost_type=tb.reg.CORR))
     T = tb.affine_to_matrix(arg, t.shape, (1, 1, 1), m.shape, (1, 1, 1))
     J = tb.resample(q_m, t.shape, T, allow_shift_copy=True)
     r_lin = tb.correlation(J, q_t, masked=True)

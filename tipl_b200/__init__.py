@@ -32,10 +32,10 @@ import numpy as np
 from . import _lib
 from ._lib import CdmParam, Field, LinearParam, RegbError, Volume  # noqa: F401
 
-__all__ = ["affine_to_matrix", "affine_to_matrix_f64", "matrix_inverse", "resample", "mi_cost", "mi32_cost", "corr_cost",
-           "nifti_info", "nifti_load", "nifti_save", "compose_displacement", "accumulate_displacement", "downsample",
-           "upsample_field_x2", "cdm_gradient",
-           "cdm_poisson", "cdm_max_length", "cdm_smooth", "reg", "Engine", "RegbError", "version"]
+__all__ = ["affine_to_matrix", "affine_to_matrix_f64", "matrix_inverse", "resample", "mi_cost", "mi32_cost",
+           "corr_cost", "nifti_info", "nifti_load", "nifti_save", "compose_displacement", "accumulate_displacement",
+           "downsample", "upsample_field_x2", "cdm_gradient", "cdm_poisson", "cdm_max_length", "cdm_smooth", "reg",
+           "Engine", "RegbError", "version"]
 
 
 def version() -> str:
@@ -518,6 +518,9 @@ class Engine:
         j.moving = _vol(moving)
         j.moving_vs[:] = [float(v) for v in moving_vs]
         j.run_linear = int(bool(linear))
+        if linear_param is None and mm_reg:
+            # the mm_reg class registers with correlation by default (reg/mm_reg.hpp:53)
+            linear_param = reg.linear_param(cost_type=reg.CORR)
         if linear_param is not None:
             j.linear = linear_param
         if arg is not None:
