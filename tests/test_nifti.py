@@ -180,3 +180,22 @@ def test_full_size_volume(orc, tmp_path):
     assert steps == [0, 1] and info["steps"] == [0, 1]
     assert np.array_equal(bits(I.cpu().numpy()), bits(ref))
     assert np.array_equal(bits(info["srow"]), bits(srow))
+
+
+def test_reader_rejects_truncated_and_unsupported(tmp_path):
+    """A file shorter than its header says, and an RGB file, fail with an error before
+    any device work (so this runs without a GPU)."""
+    sys.path.insert(0, GOLDEN)
+    from make_golden import nifti_bytes
+
+    v = np.arange(5 * 6 * 7, dtype=np.int16).reshape(5, 6, 7)
+    data, _ = nifti_bytes(v, 4, 16)
+    short = tmp_path / "short.nii"
+    short.write_bytes(data[:-10])
+    assert tb.nifti_info(str(short))["dim"] == (7, 6, 5)  # the header itself is fine
+    with pytest.raises(tb.RegbError):
+        tb.nifti_load(str(short))
+    rgb, _ = nifti_bytes(np.zeros((5, 6, 21), np.uint8), 128, 24)
+    (tmp_path / "rgb.nii").write_bytes(rgb)
+    with pytest.raises(tb.RegbError):
+        tb.nifti_load(str(tmp_path / "rgb.nii"))
