@@ -194,7 +194,7 @@ regb_status regb_mi32_cost(const regb_volume* fixed, const regb_volume* moving, 
  * must not take the device-wide synchronisation cudaMalloc/cudaFree can cause.
  * fixed/moving are uint8 DEVICE pointers (dims w,h,d), T is K host transforms, cost
  * is a DEVICE array of K doubles.  Nothing is allocated: all scratch lives in one
- * file-scope device array (4 MiB of joint histograms plus a few KiB), so K <= 16 and
+ * file-scope device array (4 MiB of joint histograms plus about 25 KiB), so K <= 16 and
  * larger K is rejected with REGB_ERR_ARG.  The first call on a device looks up that
  * array's device address, so make that first call before any stream capture.
  * Every call shares the array: calls that overlap on the GPU (different streams or

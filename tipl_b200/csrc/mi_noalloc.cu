@@ -11,7 +11,7 @@
 //
 // Limits and sharing:
 //   - at most kNoAllocMaxK = 16 transforms per call; scratch is 4 MiB of
-//     histograms plus a few KiB of counters, descriptors and the template's row
+//     histograms plus about 25 KiB of column sums, partial sums, counters, descriptors and the template's row
 //     histogram, held by every device that loads the library until the process
 //     exits;
 //   - every call uses the same array; it keeps the last call's contents, so each
