@@ -630,6 +630,7 @@ def run_served(args, rank, world, dist):
     # the plain path's rate: registrations / total time, and from the median registration
     plain = {"mean_rate": len(plain_s) / sum(plain_s), "median_rate": 1.0 / float(np.median(plain_s)),
              "ms": sorted(round(1000.0 * t, 2) for t in plain_s)} if plain_s else None
+    tuned = tb.autotune()  # the cost kernels' block sizes for this device
     eng = tb.Engine(max_active=max(args.batch, 1))
     tid = eng.add_template(torch.from_numpy(f8).cuda())
     lat, costs, evals = [], [], 0
@@ -678,7 +679,7 @@ def run_served(args, rank, world, dist):
     t_e2e, _ = timed(subjects, False)
     estats = eng.stats()
     eng.close()
-    return t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects, plain
+    return t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects, plain, tuned
 
 
 def batch_case(args):
@@ -1019,7 +1020,8 @@ def main():
 
 
 def served_line(args, rank, world, dist, torch):
-    t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects, plain = run_served(args, rank, world, dist)
+    t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects, plain, tuned = run_served(args, rank, world,
+                                                                                                 dist)
     lat = replicas.gather_lists(lat, dist)  # every rank's per-job latencies
     costs = replicas.gather_lists(costs, dist)
     evals = replicas.sum_over_ranks(evals, dist)
@@ -1076,7 +1078,8 @@ def served_line(args, rank, world, dist, torch):
                            "plain_single_job_median_registrations_per_s": plain["median_rate"] if plain else None,
                            "plain_single_job_ms": plain["ms"] if plain else None,
                            "served_over_plain": (regs / t_dev / world) / plain["median_rate"] if plain else None,
-                           "parallelism": f"replicas x{world}"},
+                           "parallelism": f"replicas x{world}",
+                           "autotuned_min_block_voxels": tuned},
                 "roofline": {"bound": "hbm",
                              "kernel": {"mi": "mi_kernel", "mi32": "mi32_kernel", "corr": "corr_kernel"}[args.cost],
                              "achieved": achieved, "peak": hbm,

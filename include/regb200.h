@@ -112,6 +112,17 @@ typedef struct {
 regb_status regb_stats_reset(int timing);
 regb_status regb_stats_get(regb_stats* out);
 
+/* ---- launch-shape autotuner (no counterpart in the reference) ---------------------- */
+/* Times the batched affine cost kernels (correlation, MI, 32-bin MI) on a 182x218x182
+ * pair with 12 candidate transforms for a few block sizes (minimum voxels per block) on
+ * the current device, and keeps the fastest of each for the rest of the process.  The
+ * choice only decides how voxels are split across blocks, so costs are identical under
+ * every choice.  tuned (optional, indexed by regb_cost_type) receives the choices,
+ * seconds (optional) the time the tuning took (about a second). */
+regb_status regb_autotune(int tuned[3], double* seconds);
+/* The block sizes in use (the defaults until regb_autotune runs). */
+regb_status regb_tuning_get(int tuned[3]);
+
 /* ---- transform algebra (host) -------------------------------------------------- */
 /* transformation_matrix(affine_param, from, from_vs, to, to_vs)
  * (numerical/transformation.hpp:636-701), in float as the reference computes it. */

@@ -35,7 +35,7 @@ from ._lib import CdmParam, Field, LinearParam, RegbError, Volume  # noqa: F401
 __all__ = ["affine_to_matrix", "affine_to_matrix_f64", "matrix_inverse", "resample", "mi_cost", "mi32_cost",
            "corr_cost", "nifti_info", "nifti_load", "nifti_save", "compose_displacement", "accumulate_displacement",
            "downsample", "upsample_field_x2", "cdm_gradient", "cdm_poisson", "cdm_max_length", "cdm_smooth", "reg",
-           "Engine", "RegbError", "version"]
+           "Engine", "RegbError", "version", "autotune", "tuning"]
 
 
 def version() -> str:
@@ -314,6 +314,27 @@ def corr_cost(fixed, moving, Ts, stream=None):
     _lib.check(_lib.lib().regb_corr_cost(C.byref(_vol(fixed)), C.byref(_vol(moving)), _fptr(Tm), K, _fptr(cost),
                                          _stream(stream)))
     return cost
+
+
+# ---------------------------------------------------------------- launch-shape autotuner
+_COST_NAMES = ("corr", "mi", "mi32")
+
+
+def autotune() -> dict:
+    """Times the batched cost kernels on this device for a few block sizes and keeps the
+    fastest (costs are identical under every choice); returns the choices (minimum voxels
+    per block, by cost) and the seconds the tuning took."""
+    tuned = np.zeros(3, np.int32)
+    sec = C.c_double(0.0)
+    _lib.check(_lib.lib().regb_autotune(_fptr(tuned), C.byref(sec)))
+    return {**{k: int(v) for k, v in zip(_COST_NAMES, tuned)}, "seconds": sec.value}
+
+
+def tuning() -> dict:
+    """The block sizes in use (defaults until autotune runs)."""
+    tuned = np.zeros(3, np.int32)
+    _lib.check(_lib.lib().regb_tuning_get(_fptr(tuned)))
+    return {k: int(v) for k, v in zip(_COST_NAMES, tuned)}
 
 
 # ---------------------------------------------------------------- NIfTI volumes (io/nifti.hpp)

@@ -119,6 +119,8 @@ _SIGS = {
     "regb_inv_displacement_to_mapping": (C.c_int, [C.c_void_p] * 4),
     "regb_compose_mapping": (C.c_int, [C.c_void_p] * 4),
     "regb_match_fov": (C.c_int, [C.c_void_p] * 5),
+    "regb_autotune": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "regb_tuning_get": (C.c_int, [C.c_void_p]),
     "regb_nifti_info_read": (C.c_int, [C.c_char_p, C.POINTER(NiftiInfo)]),
     "regb_nifti_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(Volume), C.c_void_p, C.c_void_p]),
     "regb_nifti_save": (C.c_int, [C.c_char_p, C.POINTER(Volume), C.c_void_p, C.c_void_p, C.c_int, C.c_char_p]),

@@ -2,6 +2,9 @@
 #include "batcher.h"
 #include "stats.h"
 #include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 
@@ -95,27 +98,103 @@ void TexVol::build(const uint8_t* v, Dim3 d, cudaStream_t st)
     }
 }
 
+// Minimum voxels per block of each cost kernel (index = cost type); the autotuner
+// replaces the defaults with the fastest measured choice.  Chunking only decides which
+// block counts which voxels, so every choice gives the same costs.
+static std::atomic<int> g_min_block_voxels[3] = {{32768}, {60000}, {60000}};
+
+int min_block_voxels(int cost_type) { return g_min_block_voxels[cost_type].load(); }
+void set_min_block_voxels(int cost_type, int v) { g_min_block_voxels[cost_type].store(v); }
+
 void set_task_chunks(AffineTask& t, int cost_type)
 {
     // a chunk is a run of whole rows of the fixed grid
     const long long w = t.fd.w, rows = (long long)t.fd.h * t.fd.d;
+    const long long mv = g_min_block_voxels[cost_type].load();
     long long rpc;
     if (cost_type == REGB_COST_MI) {
         // 16-bit per-block counters: at most 65535 voxels per block.  Blocks are made
-        // nearly that large (at least 60,000 voxels) because each one ends with a flush
-        // of its whole shared histogram: fewer, fuller blocks flush less often.
+        // large because each one ends with a flush of its whole shared histogram: fewer,
+        // fuller blocks flush less often.
         const long long hi = std::max<long long>(1, 65535 / w);
         rpc = (rows + 147) / 148;
-        rpc = std::max<long long>(rpc, (60000 + w - 1) / w);
+        rpc = std::max<long long>(rpc, (mv + w - 1) / w);
         rpc = std::min<long long>(rpc, hi);
     } else if (cost_type == REGB_COST_MI32)
         // 32-bit counters (no per-block voxel bound); about one block per SM for a large
-        // grid, at least 60,000 voxels per block for a small one
-        rpc = std::max<long long>((rows + 147) / 148, (60000 + w - 1) / w);
+        // grid, at least mv voxels per block for a small one
+        rpc = std::max<long long>((rows + 147) / 148, (mv + w - 1) / w);
     else
-        rpc = std::max<long long>(1, (32768 + w - 1) / w);
+        rpc = std::max<long long>(1, (mv + w - 1) / w);
     t.chunk = (int)rpc;
     t.nchunk = (int)std::max<long long>(1, (rows + rpc - 1) / rpc);
+}
+
+double autotune_cost_kernels(cudaStream_t st, int* chosen)
+{
+    const auto t_start = std::chrono::steady_clock::now();
+    // a 182 x 218 x 182 pair with smooth, many-valued content (the size of the affine
+    // workload's full-resolution level) and 12 small rigid candidates
+    const Dim3 d{182, 218, 182};
+    const size_t n = (size_t)d.n();
+    std::vector<uint8_t> hf(n), hm(n);
+    for (size_t i = 0; i < n; ++i) {
+        const int x = (int)(i % d.w), y = (int)((i / d.w) % d.h), z = (int)(i / d.wh());
+        hf[i] = (uint8_t)((x * 3 + y * 5 + z * 7) / 4 + ((x * y) >> 7));
+        hm[i] = (uint8_t)((x * 2 + y * 3 + z * 5) / 3 + ((y * z) >> 7));
+    }
+    DevBuf<uint8_t> f(n, st), m(n, st);
+    REGB_CK(cudaMemcpyAsync(f.p, hf.data(), n, cudaMemcpyHostToDevice, st));
+    REGB_CK(cudaMemcpyAsync(m.p, hm.data(), n, cudaMemcpyHostToDevice, st));
+    std::vector<float> T(12 * 12);
+    for (int k = 0; k < 12; ++k) {
+        const float a = 0.01f * (float)(k - 6), ca = std::cos(a), sa = std::sin(a);
+        const float R[9] = {ca, -sa, 0.0f, sa, ca, 0.0f, 0.0f, 0.0f, 1.0f};
+        const float c[3] = {d.w / 2.0f, d.h / 2.0f, d.d / 2.0f};
+        for (int r = 0; r < 3; ++r) {
+            float sh = c[r] + 0.3f * (float)(k % 3);
+            for (int j = 0; j < 3; ++j) {
+                T[12 * k + 3 * r + j] = R[3 * r + j];
+                sh -= R[3 * r + j] * c[j];
+            }
+            T[12 * k + 9 + r] = sh;
+        }
+    }
+    static const int cand[3][4] = {{16384, 32768, 65536, 131072},   // correlation
+                                   {32768, 49152, 60000, 65535},    // MI (16-bit counters)
+                                   {16384, 32768, 60000, 131072}};  // MI32
+    cudaEvent_t a, b;
+    REGB_CK(cudaEventCreate(&a));
+    REGB_CK(cudaEventCreate(&b));
+    for (int ct = 0; ct < 3; ++ct) {
+        AffineEvaluator ev({AffineEvaluator::Pair{f.p, d, m.p, d}}, ct, st);
+        int best = g_min_block_voxels[ct].load();
+        float best_ms = 1e30f;
+        for (int v : cand[ct]) {
+            g_min_block_voxels[ct].store(v);
+            ev.eval(0, T.data(), 12);  // warm-up
+            float ms_min = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {
+                REGB_CK(cudaEventRecord(a, st));
+                ev.eval(0, T.data(), 12);
+                REGB_CK(cudaEventRecord(b, st));
+                REGB_CK(cudaEventSynchronize(b));
+                float ms = 0.0f;
+                REGB_CK(cudaEventElapsedTime(&ms, a, b));
+                ms_min = std::min(ms_min, ms);
+            }
+            if (ms_min < best_ms) {
+                best_ms = ms_min;
+                best = v;
+            }
+        }
+        g_min_block_voxels[ct].store(best);
+        if (chosen)
+            chosen[ct] = best;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
 }
 
 void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, double* out)

@@ -60,6 +60,13 @@ void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, dou
 
 // Chunking of one task over its fixed-grid voxels.
 void set_task_chunks(AffineTask& t, int cost_type);
+// The chunking parameter per cost type (minimum voxels per block) and its autotuner:
+// times each cost kernel on a 182x218x182 pair with 12 candidates for a few block sizes
+// on the current device, keeps the fastest (results do not depend on the choice), writes
+// the choices to chosen[3] (optional) and returns the seconds it took.
+int min_block_voxels(int cost_type);
+void set_min_block_voxels(int cost_type, int v);
+double autotune_cost_kernels(cudaStream_t st, int* chosen);
 
 class AffineEvaluator {
 public:

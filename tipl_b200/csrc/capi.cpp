@@ -189,6 +189,30 @@ regb_status regb_release(void)
     });
 }
 
+regb_status regb_autotune(int tuned[3], double* seconds)
+{
+    return guarded([&] {
+        Stream s;
+        int chosen[3] = {0, 0, 0};
+        const double dt = autotune_cost_kernels(s.s, chosen);
+        s.sync();
+        if (tuned)
+            std::memcpy(tuned, chosen, sizeof(chosen));
+        if (seconds)
+            *seconds = dt;
+        return REGB_OK;
+    });
+}
+
+regb_status regb_tuning_get(int tuned[3])
+{
+    if (!tuned)
+        return REGB_ERR_ARG;
+    for (int c = 0; c < 3; ++c)
+        tuned[c] = min_block_voxels(c);
+    return REGB_OK;
+}
+
 regb_status regb_affine_to_matrix(const float param[12], const int from_dim[3], const float from_vs[3],
                                   const int to_dim[3], const float to_vs[3], float T[12])
 {
