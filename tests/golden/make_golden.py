@@ -31,7 +31,9 @@ def save(name, **arrays):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=os.environ.get("TIPL_REF_ROOT", oracle.DEFAULT_REF_ROOT))
-    ap.add_argument("--only", default=None, help="make one fixture group: core | mask_init | precision | preprocess | linear_runs | mapping | mi32 | nifti")
+    ap.add_argument("--only", default=None,
+                    help="make one fixture group: core | mask_init | precision | preprocess | linear_runs"
+                         " | mapping | mi32 | nifti")
     args = ap.parse_args()
     oracle.build(args.ref_root, with_ref=True)
     R = oracle.Reference()

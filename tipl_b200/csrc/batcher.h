@@ -14,9 +14,10 @@ namespace regb {
 constexpr int kCostTypes = 3;  // REGB_COST_CORR, REGB_COST_MI, REGB_COST_MI32
 
 // Collects cost-evaluation requests from many jobs and evaluates all pending ones
-// of a cost type in one launch (two launches may be in flight, on two streams).  A request's tasks carry their own volumes, so
-// requests of different jobs, shapes and pyramid levels mix freely; every task's
-// cost depends only on its own inputs, whatever it is batched with.
+// of a cost type in one launch (two launches may be in flight, on two streams).
+// A request's tasks carry their own volumes, so requests of different jobs, shapes
+// and pyramid levels mix freely; every task's cost depends only on its own inputs,
+// whatever it is batched with.
 class AffineBatcher {
 public:
     explicit AffineBatcher(int gather_us);
