@@ -303,11 +303,20 @@ regb_status regb_cdm_smooth(const regb_field* d, regb_field* dd, float smoothing
 
 /* ---- whole registrations ---------------------------------------------------------- */
 /* tipl::reg::cdm_common<out,T,3>(It, Is, dis, terminated, param) (reg/cdm.hpp:534-558,
- * the GPU path cdm_cuda 492-524): one modality; It/Is uint8 or float, same dims and
+ * the GPU path cdm_cuda 492-524) for one modality pair; It/Is uint8 or float, same dims and
  * dtype; dis_out receives the field.  Returns REGB_FALSE where the reference
  * returns false.  terminated (may be NULL) is polled between iterations. */
 regb_status regb_cdm(const regb_volume* It, const regb_volume* Is, regb_field* dis_out, const regb_cdm_param* param,
                      volatile const int* terminated);
+/* cdm_common over lists of modality pairs (reg/cdm.hpp:373-474, 534-558): It[i] / Is[i]
+ * for i < nmod (1..12), all of one dims and dtype (uint8 or float).  Each iteration
+ * composes and differentiates every modality, sums the gradients in modality order and
+ * takes the mean of their costs (reg/cdm.hpp:419-435); a partial cost sum of exactly
+ * zero returns REGB_FALSE.  gradient_types is cdm_param::gradient_type: modality i
+ * uses its i-th char ('r' or 'd'), 'r' past its end; NULL = param->gradient_type for
+ * modality 0 and 'r' for the others.  regb_cdm is this call with nmod = 1. */
+regb_status regb_cdm_multi(const regb_volume* It, const regb_volume* Is, int nmod, regb_field* dis_out,
+                           const regb_cdm_param* param, const char* gradient_types, volatile const int* terminated);
 /* tipl::reg::linear<out,3>(from, from_vs, to, to_vs, arg, param, terminated)
  * (reg/linear.hpp:622-700): uint8 volumes (one image pair), arg in/out, final cost
  * out.  cost_evals (may be NULL) receives the number of cost evaluations. */

@@ -18,6 +18,7 @@
 // used when the lists are longer, as TIPL's own single-modality callers do);
 // 3-D volumes; uint8 for linear, uint8 or float for cdm.
 #pragma once
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <memory>
@@ -127,14 +128,19 @@ bool cdm_cuda(const std::vector<tipl::const_pointer_image<dim, value_type> >& It
     if (It.empty() || Is.empty())
         return false;
     const int dtype = std::is_same<value_type, float>::value ? REGB_F32 : REGB_U8;
-    regb_volume vt = tipl_b200_detail::host_volume(It[0], dtype);
-    regb_volume vs = tipl_b200_detail::host_volume(Is[0], dtype);
+    // every modality pair of the lists (cdm_common has made them one length)
+    const size_t nmod = std::min(It.size(), Is.size());
+    std::vector<regb_volume> vt, vs;
+    for (size_t i = 0; i < nmod; ++i) {
+        vt.push_back(tipl_b200_detail::host_volume(It[i], dtype));
+        vs.push_back(tipl_b200_detail::host_volume(Is[i], dtype));
+    }
     d.resize(It[0].shape());
     regb_field f;
     f.ptr = &d[0][0];
-    f.dim[0] = vt.dim[0];
-    f.dim[1] = vt.dim[1];
-    f.dim[2] = vt.dim[2];
+    f.dim[0] = vt[0].dim[0];
+    f.dim[1] = vt[0].dim[1];
+    f.dim[2] = vt[0].dim[2];
     f.location = REGB_HOST;
     regb_cdm_param p;
     regb_cdm_param_default(&p);
@@ -146,11 +152,11 @@ bool cdm_cuda(const std::vector<tipl::const_pointer_image<dim, value_type> >& It
     regb_status st;
     {
         tipl_b200_detail::TerminateMirror mirror(terminated);
-        st = regb_cdm(&vt, &vs, &f, &p, mirror.flag());
+        st = regb_cdm_multi(vt.data(), vs.data(), (int)nmod, &f, &p, param.gradient_type.c_str(), mirror.flag());
     }
     if constexpr (!std::is_void<out_type>::value) {
         if (st != REGB_OK && st != REGB_FALSE && st != REGB_CANCELLED)
-            out_type() << "regb_cdm: " << regb_last_error();
+            out_type() << "regb_cdm_multi: " << regb_last_error();
     }
     return st == REGB_OK || st == REGB_CANCELLED;  // a terminated run still returns its field, as cdm() does
 }

@@ -179,6 +179,8 @@ class Oracle(_Lib):
         for sfx in ("u8", "f32", "f64"):
             getattr(L, f"orc_cdm_level_{sfx}").argtypes = [_P, _P, _P, _P, C.c_float, C.c_float, C.c_float,
                                                           C.c_uint, C.c_int, _P]
+            getattr(L, f"orc_cdm_multi_{sfx}").argtypes = [_P, _P, C.c_int, _P, _P, C.c_float, C.c_float,
+                                                          C.c_float, C.c_uint, C.c_char_p, _P]
 
     def normalize_to_u8(self, img, upper=255.999):
         """normalize_upper_lower2 of a float32 or uint16 volume; (out, ok)."""
@@ -341,6 +343,21 @@ class Oracle(_Lib):
                                                     ord(gradient_type), C.byref(iters))
         return d, bool(ok), iters.value
 
+    def cdm_multi(self, It, Is, resolution=2.0, speed=0.3, smoothing=0.05, min_dimension=16, gradient_types=""):
+        """The reference's cdm() driver over lists of modality pairs (reg/cdm.hpp:419-435);
+        returns (field, ok, iterations)."""
+        s = self._sfx(It[0])
+        It = [np.ascontiguousarray(a, It[0].dtype) for a in It]
+        Is = [np.ascontiguousarray(a, It[0].dtype) for a in Is]
+        pt = (C.c_void_p * len(It))(*[a.ctypes.data for a in It])
+        ps = (C.c_void_p * len(Is))(*[a.ctypes.data for a in Is])
+        d = np.zeros(It[0].shape + (3,), self._fdt(s))
+        iters = C.c_int(0)
+        ok = getattr(self.lib, f"orc_cdm_multi_{s}")(pt, ps, len(It), _ptr(_dims(It[0].shape)), _ptr(d), resolution,
+                                                    speed, smoothing, min_dimension, gradient_types.encode(),
+                                                    C.byref(iters))
+        return d, bool(ok), iters.value
+
 
 class Reference(_Lib):
     """The reference's own CPU implementation (compiled from its headers)."""
@@ -455,6 +472,20 @@ class Reference(_Lib):
         fn = self.lib.tiplref_cdm_u8 if It.dtype == np.uint8 else self.lib.tiplref_cdm_f32
         ok = fn(_ptr(np.ascontiguousarray(It)), _ptr(np.ascontiguousarray(Is, It.dtype)), _ptr(_dims(It.shape)),
                 _ptr(d), resolution, speed, smoothing, min_dimension)
+        return d, bool(ok)
+
+    def cdm_multi(self, It, Is, resolution=2.0, speed=0.3, smoothing=0.05, min_dimension=16, gradient_types=""):
+        """cdm_common over lists of modality pairs; returns (field, ok)."""
+        u8 = It[0].dtype == np.uint8
+        It = [np.ascontiguousarray(a, It[0].dtype) for a in It]
+        Is = [np.ascontiguousarray(a, It[0].dtype) for a in Is]
+        pt = (C.c_void_p * len(It))(*[a.ctypes.data for a in It])
+        ps = (C.c_void_p * len(Is))(*[a.ctypes.data for a in Is])
+        d = np.zeros(It[0].shape + (3,), np.float32)
+        fn = self.lib.tiplref_cdm_multi_u8 if u8 else self.lib.tiplref_cdm_multi_f32
+        fn.argtypes = [_P, _P, C.c_int, _P, _P, C.c_float, C.c_float, C.c_float, C.c_uint, C.c_char_p]
+        ok = fn(pt, ps, len(It), _ptr(_dims(It[0].shape)), _ptr(d), resolution, speed, smoothing, min_dimension,
+                gradient_types.encode())
         return d, bool(ok)
 
     def linear(self, fixed, fixed_vs, moving, moving_vs, arg=None, reg_type=15, cost_type=1):

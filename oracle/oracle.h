@@ -67,6 +67,15 @@ int orc_cdm_level_f32(const float* It, const float* Is, const int* dim, float* b
                       float smoothing, unsigned int min_dimension, int gradient_type, int* iters_out);
 int orc_cdm_level_f64(const double* It, const double* Is, const int* dim, double* best_d, float resolution,
                       float speed, float smoothing, unsigned int min_dimension, int gradient_type, int* iters_out);
+int orc_cdm_multi_u8(const uint8_t* const* It, const uint8_t* const* Is, int nmod, const int* dim, float* best_d,
+                     float resolution, float speed, float smoothing, unsigned int min_dimension, const char* gtypes,
+                     int* iters_out);
+int orc_cdm_multi_f32(const float* const* It, const float* const* Is, int nmod, const int* dim, float* best_d,
+                      float resolution, float speed, float smoothing, unsigned int min_dimension, const char* gtypes,
+                      int* iters_out);
+int orc_cdm_multi_f64(const double* const* It, const double* const* Is, int nmod, const int* dim, double* best_d,
+                      float resolution, float speed, float smoothing, unsigned int min_dimension, const char* gtypes,
+                      int* iters_out);
 
 int orc_normalize_to_u8_f32(const float* in, long long n, uint8_t* out, float upper);
 int orc_normalize_to_u8_u16(const uint16_t* in, long long n, uint8_t* out, float upper);

@@ -40,6 +40,30 @@ tipl::image<3, vec3> field_in(const float* p, const int* d)
 void field_out(const tipl::image<3, vec3>& f, float* p) { std::memcpy(p, &f[0][0], sizeof(float) * 3 * f.size()); }
 }  // namespace
 
+// cdm_common<void,T,3> over a list of nmod modalities (reg/cdm.hpp:418-435, 534-558):
+// gtypes is cdm_param::gradient_type (modality i uses gtypes[i], 'r' past its end).
+template <typename T>
+static int cdm_multi(const T* const* It, const T* const* Is, int nmod, const int* dim, float* dis_out,
+                     float resolution, float speed, float smoothing, unsigned int min_dimension, const char* gtypes)
+{
+    tipl::reg::cdm_param p;
+    p.resolution = resolution;
+    p.speed = speed;
+    p.smoothing = smoothing;
+    p.min_dimension = min_dimension;
+    p.gradient_type = gtypes ? gtypes : "";
+    std::vector<tipl::const_pointer_image<3, T> > lt, ls;
+    for (int i = 0; i < nmod; ++i) {
+        lt.push_back(cview(It[i], dim));
+        ls.push_back(cview(Is[i], dim));
+    }
+    tipl::image<3, vec3> dis;
+    bool terminated = false;
+    bool ok = tipl::reg::cdm_common<void, T, 3>(lt, ls, dis, terminated, p, false);
+    if (ok)
+        field_out(dis, dis_out);
+    return ok ? 1 : 0;
+}
 extern "C" {
 
 int tiplref_sizeof_vec3(void) { return int(sizeof(vec3)); }
@@ -230,6 +254,19 @@ int tiplref_cdm_f32(const float* It, const float* Is, const int* dim, float* dis
     if (ok)
         field_out(dis, dis_out);
     return ok ? 1 : 0;
+}
+
+int tiplref_cdm_multi_u8(const u8* const* It, const u8* const* Is, int nmod, const int* dim, float* dis_out,
+                         float resolution, float speed, float smoothing, unsigned int min_dimension,
+                         const char* gtypes)
+{
+    return cdm_multi(It, Is, nmod, dim, dis_out, resolution, speed, smoothing, min_dimension, gtypes);
+}
+int tiplref_cdm_multi_f32(const float* const* It, const float* const* Is, int nmod, const int* dim, float* dis_out,
+                          float resolution, float speed, float smoothing, unsigned int min_dimension,
+                          const char* gtypes)
+{
+    return cdm_multi(It, Is, nmod, dim, dis_out, resolution, speed, smoothing, min_dimension, gtypes);
 }
 
 // linear<void>(from, from_vs, to, to_vs, arg, param) (reg/linear.hpp:622-700); returns the final cost.

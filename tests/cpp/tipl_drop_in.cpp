@@ -3,7 +3,10 @@
 // include/tipl_b200/tipl_gpu.hpp (libregb200.so) or their CPU branch.
 //
 //   tipl_drop_in linear|cdm gpu|cpu w h d fixed.u8 moving.u8 out.bin
-// linear writes cost (float) + 12 params; cdm writes ok (int32) + the field.
+//   tipl_drop_in cdm2 gpu|cpu w h d fixed.u8 moving.u8 out.bin fixed2.u8 moving2.u8 gradient_types
+// linear writes cost (float) + 12 params; cdm writes ok (int32) + the field; cdm2 runs
+// cdm_common on the two-modality lists {fixed, fixed2} / {moving, moving2} at
+// resolution 1 with the given cdm_param::gradient_type string.
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -25,11 +28,12 @@ static std::vector<unsigned char> read_all(const char* p, size_t n)
 
 int main(int argc, char** argv)
 {
-    if (argc != 9) {
-        std::fprintf(stderr, "usage: %s linear|cdm gpu|cpu w h d fixed moving out\n", argv[0]);
+    const std::string what = argc > 1 ? argv[1] : "";
+    if (argc != (what == "cdm2" ? 12 : 9)) {
+        std::fprintf(stderr, "usage: %s linear|cdm|cdm2 gpu|cpu w h d fixed moving out [fixed2 moving2 types]\n",
+                     argv[0]);
         return 2;
     }
-    const std::string what = argv[1];
     const bool gpu = std::string(argv[2]) == "gpu";
     const tipl::shape<3> sh(std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]));
     auto fixed = read_all(argv[6], sh.size());
@@ -48,6 +52,20 @@ int main(int argc, char** argv)
         out.write((const char*)&cost, 4);
         out.write((const char*)arg.data(), 48);
         std::printf("linear %s cost %.6f\n", gpu ? "gpu" : "cpu", cost);
+    } else if (what == "cdm2") {
+        auto fixed2 = read_all(argv[9], sh.size());
+        auto moving2 = read_all(argv[10], sh.size());
+        tipl::const_pointer_image<3, unsigned char> F2(fixed2.data(), sh), M2(moving2.data(), sh);
+        tipl::reg::cdm_param param;
+        param.resolution = 1.0f;
+        param.gradient_type = argv[11];
+        tipl::image<3, tipl::vector<3>> dis;
+        bool ok = tipl::reg::cdm_common<void, unsigned char, 3>({F, F2}, {M, M2}, dis, terminated, param, gpu);
+        int32_t okv = ok ? 1 : 0;
+        out.write((const char*)&okv, 4);
+        if (ok)
+            out.write((const char*)&dis[0][0], (std::streamsize)(dis.size() * 12));
+        std::printf("cdm2 %s ok %d\n", gpu ? "gpu" : "cpu", okv);
     } else {
         tipl::image<3, tipl::vector<3>> dis;
         bool ok = tipl::reg::cdm_common<void, unsigned char, 3>({F}, {M}, dis, terminated, tipl::reg::cdm_param(), gpu);

@@ -33,7 +33,7 @@ def main():
     ap.add_argument("--ref-root", default=os.environ.get("TIPL_REF_ROOT", oracle.DEFAULT_REF_ROOT))
     ap.add_argument("--only", default=None,
                     help="make one fixture group: core | mask_init | precision | preprocess | linear_runs"
-                         " | mapping | mi32 | nifti")
+                         " | mapping | mi32 | nifti | cdm_multi")
     args = ap.parse_args()
     oracle.build(args.ref_root, with_ref=True)
     R = oracle.Reference()
@@ -54,9 +54,64 @@ def main():
         mi32(R)
     if args.only in (None, "nifti"):
         nifti(R)
+    if args.only in (None, "cdm_multi"):
+        cdm_multi(R)
 
 
 NIFTI_DIR = os.path.join(HERE, "nifti")
+
+
+def cdm_multi_inputs(shape, nmod, rng):
+    """nmod uint8 template contrasts of one anatomy (a class phantom, its inverted
+    contrast inside the head, a blob field masked to it) and the subject: every contrast
+    warped by one smooth field (sigma 6, max 3 voxels) with Rician noise."""
+    base = ph.class_phantom(shape, rng)
+    mask = (base > 0).astype(np.float32)
+    inv = np.where(base > 0, 4095.0 - base, 0.0).astype(np.float32)
+    blobs = (ph.blob_volume(shape, rng, noise=0.0) * mask).astype(np.float32)
+    It = [base, inv, blobs][:nmod]
+    d = ph.smooth_field(shape, rng, 6.0, 3.0)
+    Is = [ph.rician(ph.warp(t, d), rng) for t in It]
+    return [ph.normalize_to_u8(t) for t in It], [ph.normalize_to_u8(t) for t in Is]
+
+
+def cdm_f32_of(v):
+    """The float inputs of the float cases: uint8 values * 0.5 + 0.25 (exact in float32)."""
+    return v.astype(np.float32) * np.float32(0.5) + np.float32(0.25)
+
+
+def field_digest(d):
+    import hashlib
+
+    return hashlib.sha256(np.ascontiguousarray(d, np.float32).tobytes()).hexdigest()
+
+
+CDM_MULTI_CASES = [("u8", (36, 40, 34), 2, "", 1.0), ("u8", (30, 32, 28), 3, "rd", 1.0),
+                   ("f32", (32, 34, 30), 2, "dr", 1.0), ("u8", (18, 18, 18), 2, "", 1.0),
+                   ("u8", (36, 40, 34), 1, "", 1.0), ("f32", (36, 40, 34), 1, "d", 1.0)]
+
+
+def cdm_multi(R):
+    """cdm_common over modality lists (reg/cdm.hpp:419-435) through the reference's own
+    CPU cdm at resolution 1 (every level iterates): (dtype, shape, modalities,
+    gradient_type string, resolution).  Inputs are stored as uint8 (float cases use
+    cdm_f32_of); each field as its SHA-256 and max |d|.  c3 has a modality-0 template
+    of zeros, so its first partial cost sum is zero and the call returns false; c4 and
+    c5 are one-modality lists (the plain cdm_common call) whose fields move."""
+    rng = np.random.default_rng(ph.seed_for(3, 44))
+    out = {}
+    for k, (dt, shape, nmod, gt, res) in enumerate(CDM_MULTI_CASES):
+        It, Is = cdm_multi_inputs(shape, nmod, rng)
+        if k == 3:
+            It[0] = np.zeros_like(It[0])
+        cv = (lambda v: v) if dt == "u8" else cdm_f32_of
+        d, ok = R.cdm_multi([cv(v) for v in It], [cv(v) for v in Is], resolution=res, gradient_types=gt)
+        for i in range(nmod):
+            out[f"c{k}_It{i}"], out[f"c{k}_Is{i}"] = It[i], Is[i]
+        out[f"c{k}_ok"] = np.array(int(ok))
+        out[f"c{k}_sha256"] = np.array(field_digest(d) if ok else "")
+        out[f"c{k}_maxabs"] = np.array(float(np.abs(d).max()) if ok else 0.0)
+    save("cdm_multi", **out)
 
 
 def nifti_bytes(data, datatype, bitpix, srow=None, pixdim=(1.0, 1.0, 1.0), qform=None, big=False, version=1,

@@ -50,6 +50,30 @@ def test_cdm_common_gpu_branch_equals_cpu_branch(volumes):
     assert np.array_equal(g, c)
 
 
+@pytest.mark.parametrize("gtypes", ["", "dr"])
+def test_cdm_common_two_modalities_gpu_branch_equals_cpu_branch(volumes, golden, gtypes):
+    """cdm_common on two-modality lists (reg/cdm.hpp:419-435): the GPU branch passes
+    both pairs through regb_cdm_multi and its field equals the CPU branch's bit for bit
+    (inputs: the first case of the cdm_multi fixture, whose field moves)."""
+    d, _ = volumes
+    g = golden("cdm_multi")
+    for i in range(2):
+        g[f"c0_It{i}"].tofile(d / f"mm_f{i}.u8")
+        g[f"c0_Is{i}"].tofile(d / f"mm_m{i}.u8")
+    z, y, x = g["c0_It0"].shape
+    res = {}
+    for where in ("gpu", "cpu"):
+        out = d / f"cdm2_{where}.bin"
+        r = subprocess.run([BIN, "cdm2", where, str(x), str(y), str(z), str(d / "mm_f0.u8"), str(d / "mm_m0.u8"),
+                            str(out), str(d / "mm_f1.u8"), str(d / "mm_m1.u8"), gtypes],
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+        res[where] = np.fromfile(out, dtype=np.uint8)
+    assert res["gpu"][:4].view(np.int32)[0] == 1 and res["cpu"][:4].view(np.int32)[0] == 1
+    assert np.abs(res["cpu"][4:].view(np.float32)).max() > 0.5  # the field moves
+    assert np.array_equal(res["gpu"], res["cpu"])
+
+
 def test_linear_gpu_branch_close_to_cpu_branch(volumes):
     """The CPU branch's final cost depends on how its line search and L-BFGS threads
     interleave (4.52-4.56 on this pair over runs on one machine; on 23 seeded pairs

@@ -64,6 +64,42 @@ def test_mi32_variant(orc, golden, ci):
         assert cost == c
 
 
+def cdm_multi_case(g, ci):
+    """Inputs and settings of case ci of the cdm_multi fixture (float cases take the
+    stored uint8 values * 0.5 + 0.25, exact in float32)."""
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_golden import CDM_MULTI_CASES, cdm_f32_of
+
+    dt, _, nmod, gt, res = CDM_MULTI_CASES[ci]
+    cv = (lambda v: v) if dt == "u8" else cdm_f32_of
+    It = [cv(g[f"c{ci}_It{i}"]) for i in range(nmod)]
+    Is = [cv(g[f"c{ci}_Is{i}"]) for i in range(nmod)]
+    return It, Is, gt, res
+
+
+def field_digest(d):
+    import hashlib
+
+    return hashlib.sha256(np.ascontiguousarray(d, np.float32).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("ci", range(6))
+def test_cdm_multi_modality(orc, golden, ci):
+    """cdm over modality lists (reg/cdm.hpp:419-435): the field's SHA-256 equals the
+    reference's, and every passing case's field moves (at resolution 1 every level
+    iterates)."""
+    g = golden("cdm_multi")
+    It, Is, gt, res = cdm_multi_case(g, ci)
+    d, ok, _ = orc.cdm_multi(It, Is, resolution=res, gradient_types=gt)
+    assert ok == bool(g[f"c{ci}_ok"])
+    if ok:
+        assert float(np.abs(d).max()) == pytest.approx(float(g[f"c{ci}_maxabs"]))
+        assert float(g[f"c{ci}_maxabs"]) > 0.5
+        assert field_digest(d) == str(g[f"c{ci}_sha256"])
+
+
 @pytest.mark.parametrize("ci", range(4))
 def test_cdm_passes(orc, golden, ci):
     g = golden("cdm_passes")

@@ -481,12 +481,24 @@ class reg:
         return float(cost.value), a, int(evals.value)
 
     @staticmethod
-    def cdm(It, Is, param: CdmParam | None = None, terminated=None, out=None):
-        """tipl::reg::cdm_common: returns (field, ok)."""
-        d = _like(It, tuple(It.shape) + (3,), dtype=_f32_like(It)) if out is None else out
+    def cdm(It, Is, param: CdmParam | None = None, terminated=None, out=None, gradient_types=None):
+        """tipl::reg::cdm_common: returns (field, ok).  It / Is are one volume each or
+        equal-length lists of modality pairs (make_list(J), make_list(It) in mm_reg);
+        gradient_types is cdm_param::gradient_type, one 'r' / 'd' per modality ('r'
+        past its end; None = param.gradient_type for the first modality)."""
+        multi = isinstance(It, (list, tuple))
+        Its = list(It) if multi else [It]
+        Iss = list(Is) if isinstance(Is, (list, tuple)) else [Is]
+        n = min(len(Its), len(Iss))  # cdm_common truncates the longer list (reg/cdm.hpp:542-545)
+        if n < 1:
+            raise ValueError("cdm: empty modality list")
+        d = _like(Its[0], tuple(Its[0].shape) + (3,), dtype=_f32_like(Its[0])) if out is None else out
         p = param or reg.cdm_param()
         term = None if terminated is None else C.cast(terminated, C.c_void_p)
-        st = _lib.lib().regb_cdm(C.byref(_vol(It)), C.byref(_vol(Is)), C.byref(_field(d)), C.byref(p), term)
+        vt = (_lib.Volume * n)(*[_vol(a) for a in Its[:n]])
+        vs = (_lib.Volume * n)(*[_vol(a) for a in Iss[:n]])
+        gt = None if gradient_types is None else str(gradient_types).encode()
+        st = _lib.lib().regb_cdm_multi(vt, vs, n, C.byref(_field(d)), C.byref(p), gt, term)
         _lib.check(st, allow=(_lib.REGB_OK, _lib.REGB_FALSE, _lib.REGB_CANCELLED))
         return d, st != _lib.REGB_FALSE
 

@@ -147,6 +147,8 @@ _SIGS = {
     "regb_cdm_smooth": (C.c_int, [C.POINTER(Field), C.POINTER(Field), C.c_float, C.c_void_p]),
     "regb_cdm": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.POINTER(Field), C.POINTER(CdmParam),
                            C.c_void_p]),
+    "regb_cdm_multi": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_int, C.POINTER(Field),
+                                 C.POINTER(CdmParam), C.c_char_p, C.c_void_p]),
     "regb_runner_state_from_param": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.POINTER(LinearParam), C.POINTER(RunnerState)]),
     "regb_linear_run": (C.c_int, [C.POINTER(Volume), C.c_void_p, C.POINTER(Volume), C.c_void_p, C.c_void_p,

@@ -624,7 +624,7 @@ regb_status regb_compose_displacement(const regb_volume* from, const regb_field*
         f.in(dis->ptr, n * 12, dis->location, st, true);
         o.in(to->ptr, n * ps, to->location, st, false);
         OneSeg s(from->dim, st);
-        s.h.Is = a.d;
+        s.h.Is[0] = a.d;
         s.h.cur_d = (float*)f.d;
         s.h.Js = o.d;
         s.upload(st);
@@ -830,7 +830,7 @@ regb_status regb_cdm_gradient(const regb_volume* Js, const regb_volume* It, regb
         o.in(new_d->ptr, n * 12, new_d->location, st, false);
         OneSeg s(Js->dim, st);
         s.h.Js = a.d;
-        s.h.It = b.d;
+        s.h.It[0] = b.d;
         s.h.new_d = (float*)o.d;
         s.upload(st);
         REGB_CK(launch_cdm_gradient(s.seg.p, 1, s.h.nblk, pix_of(Js->dtype), gradient_type, st));
@@ -915,33 +915,51 @@ regb_status regb_cdm_smooth(const regb_field* d, regb_field* dd, float smoothing
     });
 }
 
-regb_status regb_cdm(const regb_volume* It, const regb_volume* Is, regb_field* dis_out, const regb_cdm_param* param,
-                     volatile const int* terminated)
+regb_status regb_cdm_multi(const regb_volume* It, const regb_volume* Is, int nmod, regb_field* dis_out,
+                           const regb_cdm_param* param, const char* gradient_types, volatile const int* terminated)
 {
     return guarded([&] {
-        check_vol(It, "It");
-        check_vol(Is, "Is");
+        if (!It || !Is || nmod < 1 || nmod > kCdmMaxModalities)
+            throw Failure(REGB_ERR_ARG, "cdm: 1 to 12 modality pairs");
         check_field(dis_out, "dis_out");
-        if (!same_dims(It->dim, Is->dim) || !same_dims(It->dim, dis_out->dim) || It->dtype != Is->dtype)
-            throw Failure(REGB_ERR_ARG, "cdm: It/Is/dis shapes or dtypes differ");
+        for (int m = 0; m < nmod; ++m) {
+            check_vol(&It[m], "It");
+            check_vol(&Is[m], "Is");
+            if (!same_dims(It[m].dim, dis_out->dim) || !same_dims(Is[m].dim, dis_out->dim) ||
+                It[m].dtype != It[0].dtype || Is[m].dtype != It[0].dtype)
+                throw Failure(REGB_ERR_ARG, "cdm: It/Is/dis shapes or dtypes differ");
+        }
         regb_cdm_param p;
         regb_cdm_param_default(&p);
         if (param)
             p = *param;
-        if (p.gradient_type != 'r' && p.gradient_type != 'd')
-            throw Failure(REGB_ERR_ARG, "gradient_type must be 'r' or 'd'");
+        const char one[2] = {(char)p.gradient_type, 0};
+        const char* gtypes = gradient_types ? gradient_types : one;
         Stream s;
-        const size_t n = nvox(It->dim), ps = pix_size(It->dtype);
-        Staged a, b, f;
-        a.in(It->ptr, n * ps, It->location, s.s, true);
-        b.in(Is->ptr, n * ps, Is->location, s.s, true);
+        const size_t n = nvox(It[0].dim), ps = pix_size(It[0].dtype);
+        Staged a[kCdmMaxModalities], b[kCdmMaxModalities], f;
+        const void* dt[kCdmMaxModalities];
+        const void* ds[kCdmMaxModalities];
+        for (int m = 0; m < nmod; ++m) {
+            a[m].in(It[m].ptr, n * ps, It[m].location, s.s, true);
+            b[m].in(Is[m].ptr, n * ps, Is[m].location, s.s, true);
+            dt[m] = a[m].d;
+            ds[m] = b[m].d;
+        }
         f.in(dis_out->ptr, n * 12, dis_out->location, s.s, false);
-        regb_status r = cdm_register(a.d, b.d, It->dim, pix_of(It->dtype), (float*)f.d, p, terminated, s.s);
+        regb_status r = cdm_register_multi(dt, ds, nmod, gtypes, It[0].dim, pix_of(It[0].dtype), (float*)f.d, p,
+                                           terminated, s.s);
         if (r == REGB_OK || r == REGB_CANCELLED)
             f.out(dis_out->ptr, s.s);
         s.sync();
         return r;
     });
+}
+
+regb_status regb_cdm(const regb_volume* It, const regb_volume* Is, regb_field* dis_out, const regb_cdm_param* param,
+                     volatile const int* terminated)
+{
+    return regb_cdm_multi(It, Is, 1, dis_out, param, nullptr, terminated);
 }
 
 regb_status regb_linear(const regb_volume* from, const float from_vs[3], const regb_volume* to, const float to_vs[3],

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstring>
+#include <string>
 #include <vector>
 #include "cdm_level.h"
 #include "host.h"
@@ -66,18 +67,22 @@ void GraphExec::reset()
     exec = nullptr;
 }
 
-void CdmLevel::init(const void* It_, const void* Is_, int w, int h, int d, int pix_, const regb_cdm_param& p,
-                    float* best, cudaStream_t st)
+void CdmLevel::init(const void* const* It_, const void* const* Is_, const std::string& gtypes_, int w, int h, int d,
+                    int pix_, const regb_cdm_param& p, float* best, cudaStream_t st)
 {
     pix = pix_;
+    gtypes = gtypes_;
     seg = CdmSeg{};
     seg.w = w;
     seg.h = h;
     seg.d = d;
     const long long n = (long long)w * h * d;
     seg.nblk = cdm_blocks_for(n);
-    seg.It = It_;
-    seg.Is = Is_;
+    seg.nmod = (int)gtypes.size();
+    for (int m = 0; m < seg.nmod; ++m) {
+        seg.It[m] = It_[m];
+        seg.Is[m] = Is_[m];
+    }
     js.alloc((size_t)n * (pix ? 4 : 1), st);
     cur.alloc(3 * n, st);
     nd.alloc(3 * n, st);
@@ -108,10 +113,15 @@ void CdmLevel::init(const void* It_, const void* Is_, int w, int h, int d, int p
     REGB_CK(cudaStreamSynchronize(st));  // h_ctl / seg are stack-staged: keep the copies ordered before reuse
 }
 
-void launch_iteration(const CdmSeg* d_segs, int nseg, int blocks, int pix, int gradient_type, cudaStream_t st)
+void launch_iteration(const CdmSeg* d_segs, int nseg, int blocks, int pix, const std::string& gtypes,
+                      cudaStream_t st)
 {
-    REGB_CK(launch_cdm_compose(d_segs, nseg, blocks, pix, st));
-    REGB_CK(launch_cdm_gradient(d_segs, nseg, blocks, pix, gradient_type, st));  // + loop decisions
+    // compose and differentiate each modality in turn (reg/cdm.hpp:422-434); the
+    // last gradient launch also makes the loop decisions
+    for (int m = 0; m < (int)gtypes.size(); ++m) {
+        REGB_CK(launch_cdm_compose(d_segs, nseg, blocks, pix, st, m));
+        REGB_CK(launch_cdm_gradient(d_segs, nseg, blocks, pix, gtypes[m], st, m));
+    }
     REGB_CK(launch_cdm_poisson(d_segs, nseg, blocks, 12, st));                    // + best_d copy, theta
     REGB_CK(launch_cdm_accumulate(d_segs, nseg, blocks, st));
     REGB_CK(launch_cdm_smooth(d_segs, nseg, blocks, st));
@@ -121,12 +131,30 @@ regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int
                          const regb_cdm_param& p, volatile const int* terminated, cudaStream_t st, int* iterations,
                          CdmScheduler* sched)
 {
+    const char gt[2] = {(char)p.gradient_type, 0};
+    return cdm_register_multi(&d_It, &d_Is, 1, gt, dim, pix, d_field, p, terminated, st, iterations, sched);
+}
+
+regb_status cdm_register_multi(const void* const* d_It, const void* const* d_Is, int nmod, const char* gtypes_in,
+                               const int* dim, int pix, float* d_field, const regb_cdm_param& p,
+                               volatile const int* terminated, cudaStream_t st, int* iterations, CdmScheduler* sched)
+{
+    if (nmod < 1 || nmod > kCdmMaxModalities)
+        throw Failure(REGB_ERR_ARG, "cdm: 1 to 12 modality pairs");
+    // cdm_param::gradient_type: modality i takes its i-th char, 'r' past the end
+    std::string gtypes(nmod, 'r');
+    const size_t ntype = gtypes_in ? std::strlen(gtypes_in) : 0;
+    for (int m = 0; m < nmod && (size_t)m < ntype; ++m)
+        gtypes[m] = gtypes_in[m];
+    for (char c : gtypes)
+        if (c != 'r' && c != 'd')
+            throw Failure(REGB_ERR_ARG, "gradient types must be 'r' or 'd'");
     const size_t psz = pix ? 4 : 1;
     struct Lv {
         int w, h, d;
-        const void* It;
-        const void* Is;
-        DevBuf<uint8_t> bt, bs;
+        const void* It[kCdmMaxModalities];
+        const void* Is[kCdmMaxModalities];
+        DevBuf<uint8_t> bt[kCdmMaxModalities], bs[kCdmMaxModalities];
         DevBuf<float> best;
         float resolution;
     };
@@ -135,8 +163,10 @@ regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int
     lv[0].w = dim[0];
     lv[0].h = dim[1];
     lv[0].d = dim[2];
-    lv[0].It = d_It;
-    lv[0].Is = d_Is;
+    for (int m = 0; m < nmod; ++m) {
+        lv[0].It[m] = d_It[m];
+        lv[0].Is[m] = d_Is[m];
+    }
     lv[0].resolution = p.resolution;
     for (;;) {
         Lv& c = lv.back();
@@ -148,12 +178,14 @@ regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int
         n.d = (c.d + 1) / 2;
         n.resolution = c.resolution / 2.0f;
         const size_t nn = (size_t)n.w * n.h * n.d;
-        n.bt.alloc(nn * psz, st);
-        n.bs.alloc(nn * psz, st);
-        REGB_CK(launch_downsample(c.It, n.bt.p, c.w, c.h, c.d, pix, st));
-        REGB_CK(launch_downsample(c.Is, n.bs.p, c.w, c.h, c.d, pix, st));
-        n.It = n.bt.p;
-        n.Is = n.bs.p;
+        for (int m = 0; m < nmod; ++m) {
+            n.bt[m].alloc(nn * psz, st);
+            n.bs[m].alloc(nn * psz, st);
+            REGB_CK(launch_downsample(c.It[m], n.bt[m].p, c.w, c.h, c.d, pix, st));
+            REGB_CK(launch_downsample(c.Is[m], n.bs[m].p, c.w, c.h, c.d, pix, st));
+            n.It[m] = n.bt[m].p;
+            n.Is[m] = n.bs[m].p;
+        }
         lv.push_back(std::move(n));
     }
     const int top = (int)lv.size() - 1;
@@ -179,11 +211,11 @@ regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int
         if (status != REGB_OK)
             continue;
         CdmLevel run;
-        run.init(L.It, L.Is, L.w, L.h, L.d, pix, p, best, st);
+        run.init(L.It, L.Is, gtypes, L.w, L.h, L.d, pix, p, best, st);
         if (sched) {
             // batched with the other jobs' levels; the scheduler returns once this
             // level's loop has ended
-            sched->run(run, p.gradient_type, terminated);
+            sched->run(run, terminated);
             REGB_CK(cudaMemcpyAsync(&run.h_ctl, run.ctl.p, sizeof(CdmCtl), cudaMemcpyDeviceToHost, st));
             REGB_CK(cudaStreamSynchronize(st));
             if (terminated && *terminated && !run.h_ctl.done)
@@ -196,7 +228,7 @@ regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int
             GraphExec g;
             g.capture([&](cudaStream_t cs) {
                 for (int k = 0; k < kIters; ++k)
-                    launch_iteration(run.d_seg.p, 1, run.seg.nblk, pix, p.gradient_type, cs);
+                    launch_iteration(run.d_seg.p, 1, run.seg.nblk, pix, gtypes, cs);
             });
             for (int it = 0; it < 201; it += kIters) {
                 if (terminated && *terminated) {

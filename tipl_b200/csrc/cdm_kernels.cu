@@ -36,16 +36,16 @@ int cdm_blocks_for(long long nvox)
     const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
 
 // ------------------------------------------------------------------ compose
-// compose_displacement (numerical/dif.hpp:90-107, 260-285): Js = Is where the
+// compose_displacement (numerical/dif.hpp:90-107, 260-285): Js = Is[mod] where the
 // displacement is exactly zero, else the trilinear sample at x + d; failed
 // samples are 0.
 template <typename T>
-__global__ void __launch_bounds__(kCdmThreads) cdm_compose_kernel(const CdmSeg* __restrict__ segs)
+__global__ void __launch_bounds__(kCdmThreads) cdm_compose_kernel(const CdmSeg* __restrict__ segs, int mod)
 {
     SEG_BEGIN
-    if (S.ctl->done)
+    if (S.ctl->done || mod >= max(S.nmod, 1))
         return;
-    const T* __restrict__ Is = (const T*)S.Is;
+    const T* __restrict__ Is = (const T*)S.Is[mod];
     T* __restrict__ Js = (T*)S.Js;
     const float* __restrict__ cd = S.cur_d;
     for (long long i = first; i < n; i += stride) {
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_compose_kernel(const CdmSeg* 
     }
 }
 
-__device__ void control_block(const CdmSeg& S);
+__device__ void control_block(const CdmSeg& S, int mod);
 __device__ __forceinline__ bool last_block_of_segment(const CdmSeg& S);
 
 // ------------------------------------------------------------------ gradient
@@ -170,16 +170,32 @@ __device__ __forceinline__ float3 grad_at(const T* __restrict__ I, const Dim3& D
     return g;
 }
 
-// cdm_get_gradient_r_imp / _d_imp (reg/cdm.hpp:46-78): new_d = 0 + gradient term;
-// the cost of every voxel (0 where skipped) is summed per block in double.
+// Stores modality mod's gradient term dd = 0 + g: new_d = dd for the first modality,
+// new_d += dd for the others (reg/cdm.hpp:430-433).
+__device__ __forceinline__ void store_term(float* __restrict__ nd, long long i, float3 out, int mod)
+{
+    if (mod) {
+        out.x = nd[3 * i] + out.x;
+        out.y = nd[3 * i + 1] + out.y;
+        out.z = nd[3 * i + 2] + out.z;
+    }
+    nd[3 * i] = out.x;
+    nd[3 * i + 1] = out.y;
+    nd[3 * i + 2] = out.z;
+}
+
+// cdm_get_gradient_r_imp / _d_imp (reg/cdm.hpp:46-78) of modality mod: the term is
+// 0 + gradient term; the cost of every voxel (0 where skipped) is summed per block in
+// double.
 template <typename T>
-__global__ void __launch_bounds__(kCdmThreads) cdm_gradient_kernel(const CdmSeg* __restrict__ segs, int gtype)
+__global__ void __launch_bounds__(kCdmThreads) cdm_gradient_kernel(const CdmSeg* __restrict__ segs, int gtype,
+                                                                   int mod)
 {
     SEG_BEGIN
-    if (S.ctl->done)
+    if (S.ctl->done || mod >= max(S.nmod, 1))
         return;
     const T* __restrict__ Js = (const T*)S.Js;
-    const T* __restrict__ It = (const T*)S.It;
+    const T* __restrict__ It = (const T*)S.It[mod];
     float* __restrict__ nd = S.new_d;
     double csum = 0.0;
     for (long long i = first; i < n; i += stride) {
@@ -234,9 +250,7 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_gradient_kernel(const CdmSeg*
                 cost = -r.r2;
             }
         }
-        nd[3 * i] = out.x;
-        nd[3 * i + 1] = out.y;
-        nd[3 * i + 2] = out.z;
+        store_term(nd, i, out, mod);
         csum += (double)cost;
     }
     __shared__ double red[32];
@@ -244,7 +258,7 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_gradient_kernel(const CdmSeg*
     if (threadIdx.x == 0)
         S.cost_part[blockIdx.x] = csum;
     if (last_block_of_segment(S))
-        control_block(S);
+        control_block(S, mod);
 }
 
 // Tiled uint8 'r' gradient.  For integer pixels the regression's window sums
@@ -262,18 +276,18 @@ struct BoxSmem {
     int p2[5][kHZ][kTY][kTX];  // x,y-summed
 };
 
-__global__ void __launch_bounds__(kBoxThreads) cdm_gradient_box_u8_kernel(const CdmSeg* __restrict__ segs)
+__global__ void __launch_bounds__(kBoxThreads) cdm_gradient_box_u8_kernel(const CdmSeg* __restrict__ segs, int mod)
 {
     const CdmSeg& S = segs[blockIdx.y];
     if ((int)blockIdx.x >= S.nblk)
         return;
-    if (S.ctl->done)
+    if (S.ctl->done || mod >= max(S.nmod, 1))
         return;
     extern __shared__ __align__(16) unsigned char smraw[];
     BoxSmem& sm = *reinterpret_cast<BoxSmem*>(smraw);
     const Dim3 D{S.w, S.h, S.d};
     const uint8_t* __restrict__ Js = (const uint8_t*)S.Js;
-    const uint8_t* __restrict__ It = (const uint8_t*)S.It;
+    const uint8_t* __restrict__ It = (const uint8_t*)S.It[mod];
     float* __restrict__ nd = S.new_d;
     const int ntx = (D.w + kTX - 1) / kTX, nty = (D.h + kTY - 1) / kTY, ntz = (D.d + kTZ - 1) / kTZ;
     const int ntiles = ntx * nty * ntz;
@@ -366,9 +380,7 @@ __global__ void __launch_bounds__(kBoxThreads) cdm_gradient_box_u8_kernel(const 
                     cost = -r.r2;
                 }
             }
-            nd[3 * i] = out.x;
-            nd[3 * i + 1] = out.y;
-            nd[3 * i + 2] = out.z;
+            store_term(nd, i, out, mod);
             csum += (double)cost;
         }
     }
@@ -377,7 +389,7 @@ __global__ void __launch_bounds__(kBoxThreads) cdm_gradient_box_u8_kernel(const 
     if (threadIdx.x == 0)
         S.cost_part[blockIdx.x] = csum;
     if (last_block_of_segment(S))
-        control_block(S);
+        control_block(S, mod);
 }
 
 // ------------------------------------------------------------------ control
@@ -434,12 +446,18 @@ __device__ float seg_cost_mean(const CdmSeg& S)
 
 // The body of the reference's iteration loop between the gradient and the
 // Poisson solve (reg/cdm.hpp:418-460), run by one block of the segment (the
-// gradient kernel's last block).
-__device__ void control_block(const CdmSeg& S)
+// gradient kernel's last block).  Each modality's launch keeps its mean cost; the
+// last modality's sums them in modality order (float), failing the level as soon
+// as a partial sum is exactly zero, and records sum / nmod.
+__device__ void control_block(const CdmSeg& S, int mod)
 {
     CdmCtl* c = S.ctl;
     const float mean_cost = seg_cost_mean(S);
     if (threadIdx.x != 0)
+        return;
+    const int nm = S.nmod > 1 ? S.nmod : 1;
+    c->mod_cost[mod] = mean_cost;
+    if (mod + 1 < nm)
         return;
     c->save_best = 0;
     c->restore = 0;
@@ -448,13 +466,16 @@ __device__ void control_block(const CdmSeg& S)
         return;
     }
     float sum_cost = 0.0f;
-    sum_cost += mean_cost;
-    c->last_cost = sum_cost;
-    if (sum_cost == 0.0f) {
-        c->done = 2;
-        return;
+    for (int k = 0; k < nm; ++k) {
+        sum_cost += c->mod_cost[k];
+        if (sum_cost == 0.0f) {
+            c->last_cost = sum_cost;
+            c->done = 2;
+            return;
+        }
     }
-    c->cost[c->ncost++] = sum_cost / 1.0f;
+    c->last_cost = sum_cost;
+    c->cost[c->ncost++] = sum_cost / (float)nm;
     const float cur = c->cost[c->ncost - 1];
     if (cur < c->best_cost) {
         c->best_cost = cur;
@@ -893,19 +914,23 @@ cudaError_t launch_cdm_status(const CdmSeg* segs, int nseg, int* out, cudaStream
 // ------------------------------------------------------------------ launchers
 #define SEG_GRID dim3(blocks, nseg)
 
-cudaError_t launch_cdm_compose(const CdmSeg* segs, int nseg, int blocks, int pix, cudaStream_t st)
+cudaError_t launch_cdm_compose(const CdmSeg* segs, int nseg, int blocks, int pix, cudaStream_t st, int mod)
 {
+    if (mod < 0 || mod >= kCdmMaxModalities)
+        return cudaErrorInvalidValue;
     if (pix == 0)
-        cdm_compose_kernel<uint8_t><<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+        cdm_compose_kernel<uint8_t><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, mod);
     else
-        cdm_compose_kernel<float><<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+        cdm_compose_kernel<float><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, mod);
     count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_cdm_gradient(const CdmSeg* segs, int nseg, int blocks, int pix, int gradient_type,
-                                cudaStream_t st)
+                                cudaStream_t st, int mod)
 {
+    if (mod < 0 || mod >= kCdmMaxModalities)
+        return cudaErrorInvalidValue;
     if (pix == 0 && gradient_type == 'r') {
         static std::atomic<unsigned long long> attr_set{0};
         int dev = 0;
@@ -920,11 +945,11 @@ cudaError_t launch_cdm_gradient(const CdmSeg* segs, int nseg, int blocks, int pi
                 return e;
             attr_set.fetch_or(bit);
         }
-        cdm_gradient_box_u8_kernel<<<SEG_GRID, kBoxThreads, sizeof(BoxSmem), st>>>(segs);
+        cdm_gradient_box_u8_kernel<<<SEG_GRID, kBoxThreads, sizeof(BoxSmem), st>>>(segs, mod);
     } else if (pix == 0)
-        cdm_gradient_kernel<uint8_t><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, gradient_type);
+        cdm_gradient_kernel<uint8_t><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, gradient_type, mod);
     else
-        cdm_gradient_kernel<float><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, gradient_type);
+        cdm_gradient_kernel<float><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, gradient_type, mod);
     count_launch();
     return cudaGetLastError();
 }

@@ -1,6 +1,7 @@
 // Device state of one CDM level of one job (fields, scratch, control block).
 #pragma once
 #include <functional>
+#include <string>
 #include "host.h"
 
 namespace regb {
@@ -20,6 +21,7 @@ struct GraphExec {
 
 struct CdmLevel {
     int pix = 0;
+    std::string gtypes;  // gradient type of each modality ('r' / 'd'), one char per pair
     CdmSeg seg{};
     CdmCtl h_ctl{};
     DevBuf<uint8_t> js;
@@ -27,12 +29,15 @@ struct CdmLevel {
     DevBuf<double> part;
     DevBuf<CdmCtl> ctl;
     DevBuf<CdmSeg> d_seg;
-    // best is the level's in/out field (starts as the upsampled coarser result).
-    void init(const void* It, const void* Is, int w, int h, int d, int pix, const regb_cdm_param& p, float* best,
-              cudaStream_t st);
+    // It / Is: gtypes.size() modality pairs of one shape.  best is the level's in/out
+    // field (starts as the upsampled coarser result).
+    void init(const void* const* It, const void* const* Is, const std::string& gtypes, int w, int h, int d, int pix,
+              const regb_cdm_param& p, float* best, cudaStream_t st);
 };
 
-// One iteration of every segment in d_segs (reg/cdm.hpp:418-470).
-void launch_iteration(const CdmSeg* d_segs, int nseg, int blocks, int pix, int gradient_type, cudaStream_t st);
+// One iteration of every segment in d_segs (reg/cdm.hpp:418-470); the segments
+// share pix and the gradient types of their modalities (gtypes, one char each).
+void launch_iteration(const CdmSeg* d_segs, int nseg, int blocks, int pix, const std::string& gtypes,
+                      cudaStream_t st);
 
 }  // namespace regb

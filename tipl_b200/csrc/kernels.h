@@ -44,6 +44,9 @@ struct AffineTask {
     double* cost;                  // output
 };
 
+// Modality pairs one CDM level takes (the reference's mm_reg holds at most 12).
+constexpr int kCdmMaxModalities = 12;
+
 // Device control block of one CDM level of one job (the reference's host-side
 // loop state, reg/cdm.hpp:408-470, kept on the device so iterations need no host
 // round trip).
@@ -65,6 +68,7 @@ struct CdmCtl {
     unsigned int ticket;
     float last_cost;
     int iters_run;
+    float mod_cost[kCdmMaxModalities];  // this iteration's mean cost of each modality
 };
 
 // One CDM job level as seen by the iteration kernels (blockIdx.y = segment).
@@ -72,8 +76,9 @@ struct CdmSeg {
     int w, h, d;
     int nblk;         // blocks this segment uses (a function of its size only, so a
                       // job's reduction order does not depend on what it is batched with)
-    const void* It;   // template (fixed) image at this level
-    const void* Is;   // subject (moving) image at this level
+    int nmod;         // modality pairs (1 when 0)
+    const void* It[kCdmMaxModalities];  // template (fixed) image of each modality at this level
+    const void* Is[kCdmMaxModalities];  // subject (moving) image of each modality at this level
     void* Js;         // composed subject (scratch, pixel type)
     float* cur_d;     // current field
     float* best_d;    // best field
@@ -111,10 +116,13 @@ cudaError_t launch_fixed_stats(const uint8_t* f, long long n, int32_t* hist, uns
 
 // CDM passes.  pix: 0 = uint8, 1 = float.  segs is a device array of nseg segments;
 // blocks is gridDim.x per segment.
-cudaError_t launch_cdm_compose(const CdmSeg* segs, int nseg, int blocks, int pix, cudaStream_t st);
-// The gradient's last block of each segment also runs the loop decisions.
+// mod selects the modality pair: compose reads Is[mod]; the gradient reads It[mod],
+// writes new_d for modality 0 and adds to it for the others, and its last block keeps
+// the modality's mean cost; after the last modality that block also runs the loop
+// decisions.
+cudaError_t launch_cdm_compose(const CdmSeg* segs, int nseg, int blocks, int pix, cudaStream_t st, int mod = 0);
 cudaError_t launch_cdm_gradient(const CdmSeg* segs, int nseg, int blocks, int pix, int gradient_type,
-                                cudaStream_t st);
+                                cudaStream_t st, int mod = 0);
 // 12 sweeps; the first also applies best_d save/restore, the last forms theta.
 cudaError_t launch_cdm_poisson(const CdmSeg* segs, int nseg, int blocks, int sweeps, cudaStream_t st);
 cudaError_t launch_cdm_theta(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st);

@@ -1,6 +1,7 @@
 #include "scheduler.h"
 #include <algorithm>
 #include <cstring>
+#include <string>
 
 namespace regb {
 
@@ -32,9 +33,9 @@ CdmScheduler::~CdmScheduler()
     }
 }
 
-void CdmScheduler::run(CdmLevel& lvl, int gradient_type, volatile const int* terminated)
+void CdmScheduler::run(CdmLevel& lvl, volatile const int* terminated)
 {
-    Entry e{&lvl, gradient_type, terminated};
+    Entry e{&lvl, terminated};
     std::unique_lock<std::mutex> lk(m_);
     active_.push_back(&e);
     cv_.notify_all();
@@ -60,11 +61,11 @@ void CdmScheduler::loop()
                 segs_.alloc(cap, st_);
                 status_.alloc(cap, st_);
             }
-            // segments sorted into groups of one (pixel type, gradient type)
+            // segments sorted into groups of one (pixel type, modality gradient types)
             std::vector<int> order(n);
             for (int i = 0; i < n; ++i)
                 order[i] = i;
-            auto key = [&](int i) { return cur[i]->lvl->pix * 256 + cur[i]->gtype; };
+            auto key = [&](int i) { return std::to_string(cur[i]->lvl->pix) + ":" + cur[i]->lvl->gtypes; };
             std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
             for (int i = 0; i < n; ++i)
                 h_segs_.p[i] = cur[order[i]]->lvl->seg;
@@ -78,7 +79,7 @@ void CdmScheduler::loop()
                         ++g1;
                     }
                     const Entry* e = cur[order[g0]];
-                    launch_iteration(segs_.p + g0, g1 - g0, blocks, e->lvl->pix, e->gtype, st_);
+                    launch_iteration(segs_.p + g0, g1 - g0, blocks, e->lvl->pix, e->lvl->gtypes, st_);
                     g0 = g1;
                 }
             }

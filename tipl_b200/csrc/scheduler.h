@@ -10,7 +10,7 @@ namespace regb {
 
 // Every registered CDM level is one segment.  A round launches the iteration
 // kernel sequence `iters_per_round` times for all active segments of the same
-// pixel type and gradient type at once, then reads back every segment's done flag
+// pixel type and modality gradient types at once, then reads back every segment's done flag
 // with one gather.  Levels join and leave between rounds; a level's decisions
 // live in its own control block, so its result does not depend on what it was
 // batched with.
@@ -21,13 +21,12 @@ public:
     CdmScheduler(const CdmScheduler&) = delete;
     CdmScheduler& operator=(const CdmScheduler&) = delete;
     // Iterates the level until its loop ends (or terminated is set); blocks the caller.
-    void run(CdmLevel& lvl, int gradient_type, volatile const int* terminated);
+    void run(CdmLevel& lvl, volatile const int* terminated);
     long long rounds() const { return rounds_; }
 
 private:
     struct Entry {
         CdmLevel* lvl;
-        int gtype;
         volatile const int* term;
         bool done = false;
     };
