@@ -323,6 +323,14 @@ regb_status regb_cdm_multi(const regb_volume* It, const regb_volume* Is, int nmo
 regb_status regb_linear(const regb_volume* from, const float from_vs[3], const regb_volume* to,
                         const float to_vs[3], float arg[12], const regb_linear_param* param,
                         volatile const int* terminated, float* cost_out, long long* cost_evals);
+/* tipl::reg::linear over lists of image pairs (reg/linear.hpp:421-440, 517-525;
+ * mm_reg's mm_linear): from[i] / to[i] for i < npairs (1..12), uint8, every from of one
+ * dims and every to of one dims.  A candidate's cost is the sum of the pairs' costs
+ * (0 + c0 + c1 + ..., in double) divided by 2 * npairs; the mask start looks at the
+ * first pair.  regb_linear is this call with npairs = 1. */
+regb_status regb_linear_multi(const regb_volume* from, const float from_vs[3], const regb_volume* to,
+                              const float to_vs[3], int npairs, float arg[12], const regb_linear_param* param,
+                              volatile const int* terminated, float* cost_out, long long* cost_evals);
 
 /* The state of the reference's linear_reg_runner when its GPU implementation is
  * entered: linear_reg_imp<out,mr,uint8,3>(std::true_type, runner, cost_type,
@@ -349,6 +357,11 @@ regb_status regb_runner_state_from_param(const int from_dim[3], const float from
 regb_status regb_linear_run(const regb_volume* from, const float from_vs[3], const regb_volume* to,
                             const float to_vs[3], float arg[12], const regb_runner_state* state,
                             volatile const int* terminated, float* cost_out, long long* cost_evals);
+/* The same over npairs image pairs (as regb_linear_multi): the GPU branch of a
+ * linear_reg_runner whose from / to lists hold several images. */
+regb_status regb_linear_run_multi(const regb_volume* from, const float from_vs[3], const regb_volume* to,
+                                  const float to_vs[3], int npairs, float arg[12], const regb_runner_state* state,
+                                  volatile const int* terminated, float* cost_out, long long* cost_evals);
 
 /* ---- serving engine ---------------------------------------------------------------
  * No counterpart in the reference (which registers one pair per call): registration

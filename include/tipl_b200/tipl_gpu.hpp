@@ -95,8 +95,12 @@ float linear_reg_imp(std::true_type, std::shared_ptr<tipl::reg::linear_reg_runne
     s.cost_type = (cost_type == tipl::reg::mutual_info) ? REGB_COST_MI : REGB_COST_CORR;
     s.precision = reg->precision;
     s.max_iterations = int(reg->max_iterations);
-    regb_volume from = tipl_b200_detail::host_volume(reg->from[0], REGB_U8);
-    regb_volume to = tipl_b200_detail::host_volume(reg->to[0], REGB_U8);
+    // every image pair of the runner's lists (run_optimize makes min(from, to) cost functions)
+    std::vector<regb_volume> from, to;
+    for (size_t i = 0; i < std::min(reg->from.size(), reg->to.size()); ++i) {
+        from.push_back(tipl_b200_detail::host_volume(reg->from[i], REGB_U8));
+        to.push_back(tipl_b200_detail::host_volume(reg->to[i], REGB_U8));
+    }
     const float fvs[3] = {reg->from_vs[0], reg->from_vs[1], reg->from_vs[2]};
     const float tvs[3] = {reg->to_vs[0], reg->to_vs[1], reg->to_vs[2]};
     float arg[12];
@@ -107,10 +111,11 @@ float linear_reg_imp(std::true_type, std::shared_ptr<tipl::reg::linear_reg_runne
     regb_status st;
     {
         tipl_b200_detail::TerminateMirror mirror(terminated);
-        st = regb_linear_run(&from, fvs, &to, tvs, arg, &s, mirror.flag(), &cost, &evals);
+        st = regb_linear_run_multi(from.data(), fvs, to.data(), tvs, (int)from.size(), arg, &s, mirror.flag(), &cost,
+                                   &evals);
     }
     if (st != REGB_OK && st != REGB_CANCELLED)
-        throw std::runtime_error(std::string("regb_linear_run: ") + regb_last_error());
+        throw std::runtime_error(std::string("regb_linear_run_multi: ") + regb_last_error());
     for (int i = 0; i < 12; ++i)
         reg->arg_min[i] = arg[i];
     reg->count += (unsigned int)evals;

@@ -4,9 +4,11 @@
 //
 //   tipl_drop_in linear|cdm gpu|cpu w h d fixed.u8 moving.u8 out.bin
 //   tipl_drop_in cdm2 gpu|cpu w h d fixed.u8 moving.u8 out.bin fixed2.u8 moving2.u8 gradient_types
+//   tipl_drop_in linear2 gpu|cpu w h d fixed.u8 moving.u8 out.bin fixed2.u8 moving2.u8
 // linear writes cost (float) + 12 params; cdm writes ok (int32) + the field; cdm2 runs
 // cdm_common on the two-modality lists {fixed, fixed2} / {moving, moving2} at
-// resolution 1 with the given cdm_param::gradient_type string.
+// resolution 1 with the given cdm_param::gradient_type string; linear2 runs linear on
+// the two-pair lists (mm_reg's mm_linear).
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -29,7 +31,7 @@ static std::vector<unsigned char> read_all(const char* p, size_t n)
 int main(int argc, char** argv)
 {
     const std::string what = argc > 1 ? argv[1] : "";
-    if (argc != (what == "cdm2" ? 12 : 9)) {
+    if (argc != (what == "cdm2" ? 12 : what == "linear2" ? 11 : 9)) {
         std::fprintf(stderr, "usage: %s linear|cdm|cdm2 gpu|cpu w h d fixed moving out [fixed2 moving2 types]\n",
                      argv[0]);
         return 2;
@@ -41,7 +43,21 @@ int main(int argc, char** argv)
     tipl::const_pointer_image<3, unsigned char> F(fixed.data(), sh), M(moving.data(), sh);
     std::ofstream out(argv[8], std::ios::binary);
     bool terminated = false;
-    if (what == "linear") {
+    if (what == "linear2") {
+        auto fixed2 = read_all(argv[9], sh.size());
+        auto moving2 = read_all(argv[10], sh.size());
+        tipl::const_pointer_image<3, unsigned char> F2(fixed2.data(), sh), M2(moving2.data(), sh);
+        tipl::affine_param<float, 3> arg;
+        tipl::reg::linear_reg_param param;
+        param.cuda = gpu;
+        float cost = tipl::reg::linear<void>(std::vector<tipl::const_pointer_image<3, unsigned char>>{F, F2},
+                                             tipl::vector<3>(1, 1, 1),
+                                             std::vector<tipl::const_pointer_image<3, unsigned char>>{M, M2},
+                                             tipl::vector<3>(1, 1, 1), arg, param, terminated);
+        out.write((const char*)&cost, 4);
+        out.write((const char*)arg.data(), 48);
+        std::printf("linear2 %s cost %.6f\n", gpu ? "gpu" : "cpu", cost);
+    } else if (what == "linear") {
         tipl::affine_param<float, 3> arg;
         tipl::reg::linear_reg_param param;
         param.cuda = gpu;

@@ -84,3 +84,28 @@ def test_linear_gpu_branch_close_to_cpu_branch(volumes):
     g = run(d, shape, "linear", "gpu").view(np.float32)
     c = [run(d, shape, "linear", "cpu").view(np.float32)[0] for _ in range(3)]
     assert g[0] <= max(c) * 1.025, (g[0], c)
+
+
+def test_linear_two_pairs_gpu_branch_close_to_cpu_branch(volumes):
+    """linear on two-pair lists (mm_reg's mm_linear, reg/linear.hpp:421-440): the GPU
+    branch passes both pairs through regb_linear_run_multi; its final cost (the pairs'
+    summed cost / 4) must be within 2.5 % of the worst of three CPU-branch runs, the same
+    bar as the one-pair search.  Second pair: the inverted contrast inside the head."""
+    d, shape = volumes
+    f = np.fromfile(d / "f.u8", dtype=np.uint8)
+    m = np.fromfile(d / "m.u8", dtype=np.uint8)
+    np.where(f > 0, 255 - f, 0).astype(np.uint8).tofile(d / "f2.u8")
+    np.where(m > 0, 255 - m, 0).astype(np.uint8).tofile(d / "m2.u8")
+    z, y, x = shape
+
+    def run2(where):
+        out = d / f"linear2_{where}.bin"
+        r = subprocess.run([BIN, "linear2", where, str(x), str(y), str(z), str(d / "f.u8"), str(d / "m.u8"), str(out),
+                            str(d / "f2.u8"), str(d / "m2.u8")], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+        return np.fromfile(out, dtype=np.float32)
+
+    g = run2("gpu")
+    c = [run2("cpu")[0] for _ in range(3)]
+    assert np.isfinite(g).all()
+    assert g[0] <= max(c) * 1.025, (g[0], c)

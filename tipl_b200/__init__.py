@@ -467,16 +467,25 @@ class reg:
 
     @staticmethod
     def linear(from_, from_vs, to, to_vs, arg=None, param: LinearParam | None = None, terminated=None):
-        """tipl::reg::linear: returns (cost, arg[12], cost_evaluations)."""
+        """tipl::reg::linear: returns (cost, arg[12], cost_evaluations).  from_ / to are
+        one volume each or lists of image pairs (make_list(It), make_list(I) of mm_reg's
+        mm_linear); the longer list is cut to the shorter one's length."""
+        fl = list(from_) if isinstance(from_, (list, tuple)) else [from_]
+        tl = list(to) if isinstance(to, (list, tuple)) else [to]
+        n = min(len(fl), len(tl))  # run_optimize: min(from.size(), to.size()) cost functions
+        if n < 1:
+            raise ValueError("linear: empty image list")
         a = (np.array([0, 0, 0, 0, 0, 0, 1, 1, 1, 0, 0, 0], np.float32) if arg is None
              else np.array(arg, np.float32, copy=True))
         p = param or reg.linear_param()
         cost = C.c_float(0)
         evals = C.c_longlong(0)
         term = None if terminated is None else C.cast(terminated, C.c_void_p)
-        st = _lib.lib().regb_linear(C.byref(_vol(from_)), _fptr(np.asarray(from_vs, np.float32)), C.byref(_vol(to)),
-                                    _fptr(np.asarray(to_vs, np.float32)), _fptr(a), C.byref(p), term,
-                                    C.byref(cost), C.byref(evals))
+        vf = (_lib.Volume * n)(*[_vol(v) for v in fl[:n]])
+        vt = (_lib.Volume * n)(*[_vol(v) for v in tl[:n]])
+        st = _lib.lib().regb_linear_multi(vf, _fptr(np.asarray(from_vs, np.float32)), vt,
+                                          _fptr(np.asarray(to_vs, np.float32)), n, _fptr(a), C.byref(p), term,
+                                          C.byref(cost), C.byref(evals))
         _lib.check(st, allow=(_lib.REGB_OK, _lib.REGB_CANCELLED))
         return float(cost.value), a, int(evals.value)
 

@@ -154,6 +154,9 @@ _SIGS = {
     "regb_linear_run": (C.c_int, [C.POINTER(Volume), C.c_void_p, C.POINTER(Volume), C.c_void_p, C.c_void_p,
                                   C.POINTER(RunnerState), C.c_void_p, C.POINTER(C.c_float),
                                   C.POINTER(C.c_longlong)]),
+    "regb_linear_run_multi": (C.c_int, [C.POINTER(Volume), C.c_void_p, C.POINTER(Volume), C.c_void_p, C.c_int,
+                                        C.c_void_p, C.POINTER(RunnerState), C.c_void_p, C.POINTER(C.c_float),
+                                        C.POINTER(C.c_longlong)]),
     "regb_engine_config_default": (None, [C.POINTER(EngineConfig)]),
     "regb_job_default": (None, [C.POINTER(Job)]),
     "regb_engine_create": (C.c_int, [C.POINTER(EngineConfig), C.POINTER(C.c_void_p)]),
@@ -168,6 +171,9 @@ _SIGS = {
     "regb_linear": (C.c_int, [C.POINTER(Volume), C.c_void_p, C.POINTER(Volume), C.c_void_p, C.c_void_p,
                               C.POINTER(LinearParam), C.c_void_p, C.POINTER(C.c_float),
                               C.POINTER(C.c_longlong)]),
+    "regb_linear_multi": (C.c_int, [C.POINTER(Volume), C.c_void_p, C.POINTER(Volume), C.c_void_p, C.c_int,
+                                    C.c_void_p, C.POINTER(LinearParam), C.c_void_p, C.POINTER(C.c_float),
+                                    C.POINTER(C.c_longlong)]),
 }
 
 

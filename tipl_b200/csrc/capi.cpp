@@ -56,6 +56,9 @@ bool same_dims(const int* a, const int* b) { return a[0] == b[0] && a[1] == b[1]
 size_t nvox(const int* d) { return (size_t)d[0] * d[1] * d[2]; }
 
 // Device view of a volume or field; host data is staged through an owned buffer.
+// Image pairs one affine search takes (the reference's mm_reg holds at most 12 modalities).
+constexpr int kMaxLinearPairs = 12;
+
 struct Staged {
     DevBuf<uint8_t> own;
     void* d = nullptr;
@@ -962,15 +965,21 @@ regb_status regb_cdm(const regb_volume* It, const regb_volume* Is, regb_field* d
     return regb_cdm_multi(It, Is, 1, dis_out, param, nullptr, terminated);
 }
 
-regb_status regb_linear(const regb_volume* from, const float from_vs[3], const regb_volume* to, const float to_vs[3],
-                        float arg[12], const regb_linear_param* param, volatile const int* terminated,
-                        float* cost_out, long long* cost_evals)
+regb_status regb_linear_multi(const regb_volume* from, const float from_vs[3], const regb_volume* to,
+                              const float to_vs[3], int npairs, float arg[12], const regb_linear_param* param,
+                              volatile const int* terminated, float* cost_out, long long* cost_evals)
 {
     return guarded([&] {
-        check_vol(from, "from");
-        check_vol(to, "to");
-        if (from->dtype != REGB_U8 || to->dtype != REGB_U8)
-            throw Failure(REGB_ERR_ARG, "linear takes uint8 volumes (reg/linear.hpp:622-629)");
+        if (!from || !to || npairs < 1 || npairs > kMaxLinearPairs)
+            throw Failure(REGB_ERR_ARG, "linear: 1 to 12 image pairs");
+        for (int k = 0; k < npairs; ++k) {
+            check_vol(&from[k], "from");
+            check_vol(&to[k], "to");
+            if (from[k].dtype != REGB_U8 || to[k].dtype != REGB_U8)
+                throw Failure(REGB_ERR_ARG, "linear takes uint8 volumes (reg/linear.hpp:622-629)");
+            if (!same_dims(from[k].dim, from[0].dim) || !same_dims(to[k].dim, to[0].dim))
+                throw Failure(REGB_ERR_ARG, "linear: the pairs' from (to) volumes must share dims");
+        }
         if (!from_vs || !to_vs || !arg)
             throw Failure(REGB_ERR_ARG, "null voxel size / arg");
         regb_linear_param p;
@@ -980,11 +989,17 @@ regb_status regb_linear(const regb_volume* from, const float from_vs[3], const r
         if (p.cost_type != REGB_COST_MI && p.cost_type != REGB_COST_CORR && p.cost_type != REGB_COST_MI32)
             throw Failure(REGB_ERR_ARG, "cost_type must be MI, MI32 or CORR");
         Stream s;
-        Staged a, b;
-        a.in(from->ptr, nvox(from->dim), from->location, s.s, true);
-        b.in(to->ptr, nvox(to->dim), to->location, s.s, true);
-        LinearResult r = linear_register((const uint8_t*)a.d, from->dim, from_vs, (const uint8_t*)b.d, to->dim, to_vs,
-                                         arg, p, terminated, s.s);
+        Staged a[kMaxLinearPairs], b[kMaxLinearPairs];
+        const uint8_t* df[kMaxLinearPairs];
+        const uint8_t* dt[kMaxLinearPairs];
+        for (int k = 0; k < npairs; ++k) {
+            a[k].in(from[k].ptr, nvox(from[k].dim), from[k].location, s.s, true);
+            b[k].in(to[k].ptr, nvox(to[k].dim), to[k].location, s.s, true);
+            df[k] = (const uint8_t*)a[k].d;
+            dt[k] = (const uint8_t*)b[k].d;
+        }
+        LinearResult r = linear_register_multi(df, dt, npairs, from[0].dim, from_vs, to[0].dim, to_vs, arg, p,
+                                               terminated, s.s);
         s.sync();
         if (cost_out)
             *cost_out = r.cost;
@@ -992,6 +1007,13 @@ regb_status regb_linear(const regb_volume* from, const float from_vs[3], const r
             *cost_evals = r.evals;
         return (terminated && *terminated) ? REGB_CANCELLED : REGB_OK;
     });
+}
+
+regb_status regb_linear(const regb_volume* from, const float from_vs[3], const regb_volume* to, const float to_vs[3],
+                        float arg[12], const regb_linear_param* param, volatile const int* terminated,
+                        float* cost_out, long long* cost_evals)
+{
+    return regb_linear_multi(from, from_vs, to, to_vs, 1, arg, param, terminated, cost_out, cost_evals);
 }
 
 regb_status regb_runner_state_from_param(const int from_dim[3], const float from_vs[3], const int to_dim[3],
@@ -1010,25 +1032,37 @@ regb_status regb_runner_state_from_param(const int from_dim[3], const float from
     });
 }
 
-regb_status regb_linear_run(const regb_volume* from, const float from_vs[3], const regb_volume* to,
-                            const float to_vs[3], float arg[12], const regb_runner_state* state,
-                            volatile const int* terminated, float* cost_out, long long* cost_evals)
+regb_status regb_linear_run_multi(const regb_volume* from, const float from_vs[3], const regb_volume* to,
+                                  const float to_vs[3], int npairs, float arg[12], const regb_runner_state* state,
+                                  volatile const int* terminated, float* cost_out, long long* cost_evals)
 {
     return guarded([&] {
-        check_vol(from, "from");
-        check_vol(to, "to");
-        if (from->dtype != REGB_U8 || to->dtype != REGB_U8)
-            throw Failure(REGB_ERR_ARG, "linear takes uint8 volumes (reg/linear.hpp:622-629)");
+        if (!from || !to || npairs < 1 || npairs > kMaxLinearPairs)
+            throw Failure(REGB_ERR_ARG, "linear: 1 to 12 image pairs");
+        for (int k = 0; k < npairs; ++k) {
+            check_vol(&from[k], "from");
+            check_vol(&to[k], "to");
+            if (from[k].dtype != REGB_U8 || to[k].dtype != REGB_U8)
+                throw Failure(REGB_ERR_ARG, "linear takes uint8 volumes (reg/linear.hpp:622-629)");
+            if (!same_dims(from[k].dim, from[0].dim) || !same_dims(to[k].dim, to[0].dim))
+                throw Failure(REGB_ERR_ARG, "linear: the pairs' from (to) volumes must share dims");
+        }
         if (!from_vs || !to_vs || !arg || !state)
             throw Failure(REGB_ERR_ARG, "null voxel size / arg / state");
         if (state->cost_type != REGB_COST_MI && state->cost_type != REGB_COST_CORR && state->cost_type != REGB_COST_MI32)
             throw Failure(REGB_ERR_ARG, "cost_type must be MI, MI32 or CORR");
         Stream s;
-        Staged a, b;
-        a.in(from->ptr, nvox(from->dim), from->location, s.s, true);
-        b.in(to->ptr, nvox(to->dim), to->location, s.s, true);
-        LinearResult r = linear_register_state((const uint8_t*)a.d, from->dim, from_vs, (const uint8_t*)b.d, to->dim,
-                                               to_vs, arg, *state, terminated, s.s);
+        Staged a[kMaxLinearPairs], b[kMaxLinearPairs];
+        const uint8_t* df[kMaxLinearPairs];
+        const uint8_t* dt[kMaxLinearPairs];
+        for (int k = 0; k < npairs; ++k) {
+            a[k].in(from[k].ptr, nvox(from[k].dim), from[k].location, s.s, true);
+            b[k].in(to[k].ptr, nvox(to[k].dim), to[k].location, s.s, true);
+            df[k] = (const uint8_t*)a[k].d;
+            dt[k] = (const uint8_t*)b[k].d;
+        }
+        LinearResult r = linear_register_state_multi(df, dt, npairs, from[0].dim, from_vs, to[0].dim, to_vs, arg,
+                                                     *state, terminated, s.s);
         s.sync();
         if (cost_out)
             *cost_out = r.cost;
@@ -1036,6 +1070,13 @@ regb_status regb_linear_run(const regb_volume* from, const float from_vs[3], con
             *cost_evals = r.evals;
         return (terminated && *terminated) ? REGB_CANCELLED : REGB_OK;
     });
+}
+
+regb_status regb_linear_run(const regb_volume* from, const float from_vs[3], const regb_volume* to,
+                            const float to_vs[3], float arg[12], const regb_runner_state* state,
+                            volatile const int* terminated, float* cost_out, long long* cost_evals)
+{
+    return regb_linear_run_multi(from, from_vs, to, to_vs, 1, arg, state, terminated, cost_out, cost_evals);
 }
 
 }  // extern "C"

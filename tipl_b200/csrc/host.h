@@ -157,10 +157,21 @@ class CdmScheduler;
 LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
                              const int* tdim, const float* to_vs, float* arg, const regb_linear_param& p,
                              volatile const int* terminated, cudaStream_t st, AffineBatcher* batcher = nullptr);
+// The same over npairs image pairs d_from[i] / d_to[i] (tipl::reg::linear with
+// make_list(It), make_list(I): every from-volume of dims fdim, every to-volume of dims
+// tdim); a candidate's cost is the sum over pairs divided by 2 * npairs.
+LinearResult linear_register_multi(const uint8_t* const* d_from, const uint8_t* const* d_to, int npairs,
+                                   const int* fdim, const float* from_vs, const int* tdim, const float* to_vs,
+                                   float* arg, const regb_linear_param& p, volatile const int* terminated,
+                                   cudaStream_t st, AffineBatcher* batcher = nullptr);
 
 LinearResult linear_register_state(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
                                    const int* tdim, const float* to_vs, float* arg, const regb_runner_state& s,
                                    volatile const int* terminated, cudaStream_t st);
+LinearResult linear_register_state_multi(const uint8_t* const* d_from, const uint8_t* const* d_to, int npairs,
+                                         const int* fdim, const float* from_vs, const int* tdim, const float* to_vs,
+                                         float* arg, const regb_runner_state& s, volatile const int* terminated,
+                                         cudaStream_t st);
 void runner_state_from_param(const int* fdim, const float* from_vs, const int* tdim, const float* to_vs,
                              const float* arg, const regb_linear_param& p, regb_runner_state& s);
 

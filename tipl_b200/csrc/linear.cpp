@@ -18,6 +18,7 @@
 #include <cstring>
 #include <mutex>
 #include <thread>
+#include <memory>
 #include "affine_eval.h"
 #include "host.h"
 #include "linear_runner.h"
@@ -40,12 +41,16 @@ static const float kBound[3][3][8] = {
 
 // Runs the runner from an explicit state: the reference runner's fields at the
 // point its GPU implementation is entered (reg/linear.hpp:597-604).
-static LinearResult run_state(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
-                              const int* tdim, const float* to_vs, float* arg, const regb_runner_state& s,
-                              volatile const int* terminated, cudaStream_t st, AffineBatcher* batcher)
+// npairs image pairs d_from[i] / d_to[i] share the dims fdim / tdim; each has its
+// own pyramid and evaluator, and a candidate's cost is their sum in pair order.
+static LinearResult run_state(const uint8_t* const* d_from, const uint8_t* const* d_to, int npairs, const int* fdim,
+                              const float* from_vs, const int* tdim, const float* to_vs, float* arg,
+                              const regb_runner_state& s, volatile const int* terminated, cudaStream_t st,
+                              AffineBatcher* batcher)
 {
     opt::Vec a(arg, arg + 12);
     LinearRunner R(a);
+    R.npairs = npairs;
     R.terminated = terminated;
     R.cost_type = s.cost_type;
     R.arg_upper.assign(s.arg_upper, s.arg_upper + 12);
@@ -59,9 +64,12 @@ static LinearResult run_state(const uint8_t* d_from, const int* fdim, const floa
 
     // pyramid: a level below while the fixed volume exceeds 96^3 (reg/linear.hpp:309-322, 527-545)
     std::vector<DevBuf<uint8_t>> bufs;
+    std::vector<std::vector<const uint8_t*>> pf(1), pt(1);  // [level][pair]
+    pf[0].assign(d_from, d_from + npairs);
+    pt[0].assign(d_to, d_to + npairs);
     LinearRunner::Level L0;
-    L0.from = d_from;
-    L0.to = d_to;
+    L0.from = d_from[0];
+    L0.to = d_to[0];
     for (int i = 0; i < 3; ++i) {
         L0.fd[i] = fdim[i];
         L0.td[i] = tdim[i];
@@ -82,21 +90,42 @@ static LinearResult run_state(const uint8_t* d_from, const int* fdim, const floa
                 n.fvs[i] = c.fvs[i] * 2.0f;
                 n.tvs[i] = c.tvs[i] * 2.0f;
             }
-            bufs.emplace_back((size_t)n.fd[0] * n.fd[1] * n.fd[2], st);
-            bufs.emplace_back((size_t)n.td[0] * n.td[1] * n.td[2], st);
-            REGB_CK(launch_downsample(c.from, bufs[bufs.size() - 2].p, c.fd[0], c.fd[1], c.fd[2], 0, st));
-            REGB_CK(launch_downsample(c.to, bufs.back().p, c.td[0], c.td[1], c.td[2], 0, st));
-            n.from = bufs[bufs.size() - 2].p;
-            n.to = bufs.back().p;
+            std::vector<const uint8_t*> nf(npairs), nt(npairs);
+            for (int k = 0; k < npairs; ++k) {
+                bufs.emplace_back((size_t)n.fd[0] * n.fd[1] * n.fd[2], st);
+                bufs.emplace_back((size_t)n.td[0] * n.td[1] * n.td[2], st);
+                REGB_CK(launch_downsample(pf.back()[k], bufs[bufs.size() - 2].p, c.fd[0], c.fd[1], c.fd[2], 0, st));
+                REGB_CK(launch_downsample(pt.back()[k], bufs.back().p, c.td[0], c.td[1], c.td[2], 0, st));
+                nf[k] = bufs[bufs.size() - 2].p;
+                nt[k] = bufs.back().p;
+            }
+            n.from = nf[0];
+            n.to = nt[0];
+            pf.push_back(nf);
+            pt.push_back(nt);
             R.levels.push_back(n);
         }
     }
-    std::vector<AffineEvaluator::Pair> pairs;
-    for (auto& L : R.levels)
-        pairs.push_back({L.from, Dim3{L.fd[0], L.fd[1], L.fd[2]}, L.to, Dim3{L.td[0], L.td[1], L.td[2]}});
-    AffineEvaluator ev(pairs, s.cost_type, st);
-    ev.set_batcher(batcher);
-    R.eval = [&ev](int level, const float* T, int n) { return ev.eval(level, T, n); };
+    std::vector<std::unique_ptr<AffineEvaluator>> evs;
+    for (int k = 0; k < npairs; ++k) {
+        std::vector<AffineEvaluator::Pair> pairs;
+        for (size_t l = 0; l < R.levels.size(); ++l) {
+            const LinearRunner::Level& L = R.levels[l];
+            pairs.push_back({pf[l][k], Dim3{L.fd[0], L.fd[1], L.fd[2]}, pt[l][k], Dim3{L.td[0], L.td[1], L.td[2]}});
+        }
+        evs.emplace_back(new AffineEvaluator(pairs, s.cost_type, st));
+        evs.back()->set_batcher(batcher);
+    }
+    // run_optimize's fun (reg/linear.hpp:427-440): double cost = 0; cost += each pair's
+    R.eval = [&evs](int level, const float* T, int n) {
+        std::vector<double> c((size_t)n, 0.0);
+        for (auto& ev : evs) {
+            const std::vector<double> ck = ev->eval(level, T, n);
+            for (int k = 0; k < n; ++k)
+                c[k] += ck[k];
+        }
+        return c;
+    };
     // optimize<cost, mr> (reg/linear.hpp:552-560)
     const double cost = s.multi_resolution ? R.run_optimize_mr(0) : R.run_optimize(0, 0);
     std::copy(a.begin(), a.end(), arg);
@@ -148,11 +177,22 @@ LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float
                              const int* tdim, const float* to_vs, float* arg, const regb_linear_param& p,
                              volatile const int* terminated, cudaStream_t st, AffineBatcher* batcher)
 {
+    return linear_register_multi(&d_from, &d_to, 1, fdim, from_vs, tdim, to_vs, arg, p, terminated, st, batcher);
+}
+
+LinearResult linear_register_multi(const uint8_t* const* d_from, const uint8_t* const* d_to, int npairs,
+                                   const int* fdim, const float* from_vs, const int* tdim, const float* to_vs,
+                                   float* arg, const regb_linear_param& p, volatile const int* terminated,
+                                   cudaStream_t st, AffineBatcher* batcher)
+{
+    if (npairs < 1)
+        throw Failure(REGB_ERR_ARG, "linear: no image pair");
+    // the mask start looks at the first pair only (reg/linear.hpp:661-663)
     if (p.reg_type == REGB_REG_AFFINE && p.bound != REGB_BOUND_NARROW) {
         MaskCounts cf, ct;
-        mask_counts(d_from, fdim, cf, st);
+        mask_counts(d_from[0], fdim, cf, st);
         if (has_mask(cf)) {
-            mask_counts(d_to, tdim, ct, st);
+            mask_counts(d_to[0], tdim, ct, st);
             if (has_mask(ct)) {
                 float sur[12], new_to_vs[3];
                 estimate_affine_param(cf, from_vs, ct, to_vs, sur);
@@ -162,7 +202,8 @@ LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float
                 }
                 regb_runner_state s;
                 runner_state_from_param(fdim, from_vs, tdim, new_to_vs, sur, p, s);
-                LinearResult r = run_state(d_from, fdim, from_vs, d_to, tdim, new_to_vs, sur, s, terminated, st, batcher);
+                LinearResult r = run_state(d_from, d_to, npairs, fdim, from_vs, tdim, new_to_vs, sur, s, terminated,
+                                           st, batcher);
                 float T[12];
                 affine_to_matrix(sur, fdim, from_vs, tdim, new_to_vs, T);
                 matrix_to_affine_param(T, fdim, from_vs, tdim, to_vs, arg);
@@ -172,14 +213,22 @@ LinearResult linear_register(const uint8_t* d_from, const int* fdim, const float
     }
     regb_runner_state s;
     runner_state_from_param(fdim, from_vs, tdim, to_vs, arg, p, s);
-    return run_state(d_from, fdim, from_vs, d_to, tdim, to_vs, arg, s, terminated, st, batcher);
+    return run_state(d_from, d_to, npairs, fdim, from_vs, tdim, to_vs, arg, s, terminated, st, batcher);
 }
 
 LinearResult linear_register_state(const uint8_t* d_from, const int* fdim, const float* from_vs, const uint8_t* d_to,
                                    const int* tdim, const float* to_vs, float* arg, const regb_runner_state& s,
                                    volatile const int* terminated, cudaStream_t st)
 {
-    return run_state(d_from, fdim, from_vs, d_to, tdim, to_vs, arg, s, terminated, st, nullptr);
+    return run_state(&d_from, &d_to, 1, fdim, from_vs, tdim, to_vs, arg, s, terminated, st, nullptr);
+}
+
+LinearResult linear_register_state_multi(const uint8_t* const* d_from, const uint8_t* const* d_to, int npairs,
+                                         const int* fdim, const float* from_vs, const int* tdim, const float* to_vs,
+                                         float* arg, const regb_runner_state& s, volatile const int* terminated,
+                                         cudaStream_t st)
+{
+    return run_state(d_from, d_to, npairs, fdim, from_vs, tdim, to_vs, arg, s, terminated, st, nullptr);
 }
 
 }  // namespace regb

@@ -179,7 +179,9 @@ public:
     int cost_type = REGB_COST_MI;
     volatile const int* terminated = nullptr;
     // costs of n matrices (12 floats each) on pyramid level `level`
+    // the summed cost of every image pair, 0.0 + c0 + c1 + ... in pair order
     std::function<std::vector<double>(int level, const float* T, int n)> eval;
+    int npairs = 1;
     long long evals = 0;
     // called after each DOF stage with the stage's type, cost and parameters
     std::function<void(int reg, double cost, const opt::Vec& arg)> on_stage;
@@ -249,8 +251,9 @@ public:
             affine_to_matrix(params[k].data(), L.fd, L.fvs, L.td, L.tvs, &T[12 * k]);
         std::vector<double> c = eval(level, T.data(), (int)params.size());
         evals += (long long)params.size();
+        const float div = (float)npairs * 2.0f;  // cost_fun.size() * 2.0f, a float
         for (double& v : c)
-            v /= 1 * 2.0f;
+            v /= div;
         return c;
     }
 
