@@ -65,7 +65,10 @@ void CdmScheduler::loop()
             std::vector<int> order(n);
             for (int i = 0; i < n; ++i)
                 order[i] = i;
-            auto key = [&](int i) { return std::to_string(cur[i]->lvl->pix) + ":" + cur[i]->lvl->gtypes; };
+            std::vector<std::string> keys(n);
+            for (int i = 0; i < n; ++i)
+                keys[i] = std::to_string(cur[i]->lvl->pix) + ":" + cur[i]->lvl->gtypes;
+            auto key = [&](int i) -> const std::string& { return keys[i]; };
             std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
             for (int i = 0; i < n; ++i)
                 h_segs_.p[i] = cur[order[i]]->lvl->seg;
