@@ -42,8 +42,8 @@ VS = (1.0, 1.0, 1.0)
 METRIC = "registrations/s (affine 12-DOF MI, 182x218x182 uint8, 1 mm)"
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per voxel evaluation of mi_kernel, from one ncu capture of a
-# 12-candidate launch on the 182x218x182 pair (profiles/mi_kernel_affine_182x218x182.md:
-# 24.44544 MB / 86.65 M voxel evaluations); scaled to each bench launch by its voxels.
+# 12-candidate launch on the 182x218x182 pair (24.44544 MB / 86.65 M voxel evaluations);
+# scaled to each bench launch by its voxels.
 MI_DRAM_BYTES_PER_VOXEL_EVAL = 24.44544e6 / (12 * 7221032)
 COST_NAME = {"mi": "MI", "mi32": "MI (32x32 bins)", "corr": "correlation"}
 COST_DESC = {"mi": "MI 256x256 joint histogram (the reference's)",
@@ -229,10 +229,7 @@ def cdm_case(args):
     from tipl_b200 import _lib
     from tipl_b200 import phantom as ph
 
-    rng = np.random.default_rng(ph.seed_for(4, 0))
-    t = ph.class_phantom(SHAPE, rng)
-    d = ph.smooth_field(SHAPE, rng, 6.0, 4.0)
-    m = ph.rician(ph.warp(t, d), rng)
+    t, m = ph.cdm_workload_pair(SHAPE)
     It = torch.from_numpy(ph.normalize_to_u8(t)).cuda()
     Is = torch.from_numpy(ph.normalize_to_u8(m)).cuda()
     p = tb.reg.cdm_param(min_dimension=32)

@@ -22,15 +22,25 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libtipl_ref.so")
 REF_GPU_SO = os.path.join(HERE, "_ref", "libtipl_ref_gpu.so")
-DEFAULT_REF_ROOT = "/root/reference"
+
+
+def ref_root_from_env() -> str | None:
+    """The reference source tree named by TIPL_REF_ROOT (None when unset)."""
+    return os.environ.get("TIPL_REF_ROOT") or None
 
 
 def build(ref_root: str | None = None, with_ref: bool = True) -> None:
-    """Compile liboracle.so and, when the reference tree exists, the reference driver."""
+    """Compile liboracle.so and, with with_ref, the reference driver from the source tree
+    ref_root (or TIPL_REF_ROOT).  Asking for the reference build without naming a tree
+    that holds the reference's reg/ headers is an error."""
     subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
-    root = ref_root or os.environ.get("TIPL_REF_ROOT", DEFAULT_REF_ROOT)
-    if with_ref and os.path.isdir(os.path.join(root, "reg")):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref", "refgpu", f"REF_ROOT={root}"])
+    if not with_ref:
+        return
+    root = ref_root or ref_root_from_env()
+    if not root or not os.path.isdir(os.path.join(root, "reg")):
+        raise RuntimeError(f"reference source tree not found (ref_root={root!r}); pass ref_root or set "
+                           "TIPL_REF_ROOT to the directory that holds reg/linear.hpp")
+    subprocess.check_call(["make", "-s", "-C", HERE, "ref", "refgpu", f"REF_ROOT={root}"])
 
 
 _P = C.c_void_p

@@ -30,10 +30,11 @@ def save(name, **arrays):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default=os.environ.get("TIPL_REF_ROOT", oracle.DEFAULT_REF_ROOT))
+    ap.add_argument("--ref-root", default=oracle.ref_root_from_env(), required=oracle.ref_root_from_env() is None,
+                    help="the reference source tree (default: $TIPL_REF_ROOT)")
     ap.add_argument("--only", default=None,
                     help="make one fixture group: core | mask_init | precision | preprocess | linear_runs"
-                         " | mapping | mi32 | nifti | cdm_multi")
+                         " | mapping | mi32 | nifti | cdm_multi | cdm_full")
     args = ap.parse_args()
     oracle.build(args.ref_root, with_ref=True)
     R = oracle.Reference()
@@ -56,6 +57,8 @@ def main():
         nifti(R)
     if args.only in (None, "cdm_multi"):
         cdm_multi(R)
+    if args.only in (None, "cdm_full"):
+        cdm_full(R)
 
 
 NIFTI_DIR = os.path.join(HERE, "nifti")
@@ -112,6 +115,56 @@ def cdm_multi(R):
         out[f"c{k}_sha256"] = np.array(field_digest(d) if ok else "")
         out[f"c{k}_maxabs"] = np.array(float(np.abs(d).max()) if ok else 0.0)
     save("cdm_multi", **out)
+
+
+def input_digest(v):
+    import hashlib
+
+    return hashlib.sha256(np.ascontiguousarray(v).tobytes()).hexdigest()
+
+
+# (name, generator, dtype, cdm_param overrides): the inputs are regenerated from their
+# seeds by the tests, which first check them against the stored input digests.
+CDM_FULL_CASES = [("full", "workload", "u8", {"min_dimension": 32}),
+                  ("c1_blob", "blob", "f32", {}),
+                  ("c1_class", "class", "f32", {}),
+                  ("c1_class_u8", "class", "u8", {})]
+
+
+def cdm_full_inputs(gen, dt):
+    """The inputs of a CDM_FULL_CASES entry: 'workload' is the 182x218x182 pair of the
+    nonlinear workload, 'blob' the 64^3 float pair of the plain CDM workload (its blob
+    generator), 'class' a 64^3 class-phantom pair; 'u8' cases are quantised with
+    normalize_upper_lower2 (255.999)."""
+    if gen == "workload":
+        t, m = ph.cdm_workload_pair((182, 218, 182))
+    elif gen == "blob":
+        t, m, _ = ph.cdm_pair((64, 64, 64), seed=ph.seed_for(1, 0))
+    else:
+        t, m = ph.cdm_class_pair((64, 64, 64))
+    if dt == "u8":
+        return ph.normalize_to_u8(t), ph.normalize_to_u8(m)
+    return np.ascontiguousarray(t, np.float32), np.ascontiguousarray(m, np.float32)
+
+
+def cdm_full(R):
+    """The reference's own CPU cdm_common (one thread) at the workloads' shapes: the
+    182x218x182 uint8 pair at min_dimension 32 (levels 23/46/91 iterate; the field moves),
+    the 64^3 float blob pair of the plain CDM workload at the default cdm_param (the
+    reference returns the zero field: it never improves on its first iteration there),
+    and a 64^3 class-phantom pair at the default cdm_param, float and uint8 (the field
+    moves).  Stored: input digests, the field's SHA-256, max |d|, ok."""
+    out = {}
+    for name, gen, dt, kw in CDM_FULL_CASES:
+        It, Is = cdm_full_inputs(gen, dt)
+        d, ok = R.cdm(It, Is, **kw)
+        out[f"{name}_It_sha256"] = np.array(input_digest(It))
+        out[f"{name}_Is_sha256"] = np.array(input_digest(Is))
+        out[f"{name}_ok"] = np.array(int(ok))
+        out[f"{name}_sha256"] = np.array(field_digest(d) if ok else "")
+        out[f"{name}_maxabs"] = np.array(float(np.abs(d).max()) if ok else 0.0)
+        print(name, ok, float(np.abs(d).max()), flush=True)
+    save("cdm_full", **out)
 
 
 def nifti_bytes(data, datatype, bitpix, srow=None, pixdim=(1.0, 1.0, 1.0), qform=None, big=False, version=1,

@@ -111,3 +111,23 @@ def test_runner_state_from_param(L):
                                    fd.ctypes.data_as(C.c_void_p), vs.ctypes.data_as(C.c_void_p),
                                    arg.ctypes.data_as(C.c_void_p), C.byref(p), C.byref(s))
     assert s.search_count == 0 and s.multi_resolution == 0
+
+
+def test_mi_rejects_rows_wider_than_16_bit_counters(L):
+    """The 256-bin MI counts in 16-bit per-block counters and a block holds at least one
+    row of the fixed grid, so a fixed width above 65535 is an argument error (checked
+    before anything reaches the device), for regb_mi_cost and regb_mi_cost_noalloc."""
+    buf = np.zeros(70000, np.uint8)
+    wide = _lib.Volume(buf.ctypes.data_as(C.c_void_p), (C.c_int * 3)(70000, 1, 1), _lib.U8, _lib.HOST)
+    small = _lib.Volume(buf.ctypes.data_as(C.c_void_p), (C.c_int * 3)(8, 8, 8), _lib.U8, _lib.HOST)
+    T = np.zeros(12, np.float32)
+    cost = np.zeros(1, np.float64)
+    st = L.regb_mi_cost(C.byref(wide), C.byref(small), T.ctypes.data_as(C.c_void_p), 1,
+                        cost.ctypes.data_as(C.c_void_p), None, None)
+    assert st == _lib.REGB_ERR_ARG and b"65535" in L.regb_last_error()
+    fd = np.array([70000, 1, 1], np.int32)
+    md = np.array([8, 8, 8], np.int32)
+    st = L.regb_mi_cost_noalloc(buf.ctypes.data_as(C.c_void_p), fd.ctypes.data_as(C.c_void_p),
+                                buf.ctypes.data_as(C.c_void_p), md.ctypes.data_as(C.c_void_p),
+                                T.ctypes.data_as(C.c_void_p), 1, cost.ctypes.data_as(C.c_void_p), None)
+    assert st == _lib.REGB_ERR_ARG and b"65535" in L.regb_last_error()

@@ -155,3 +155,25 @@ def test_live_against_reference(orc):
         assert same(T, R.affine_to_matrix(p, t8.shape, (1, 1, 1), m8.shape, (1, 1, 1)))
         assert same(orc.mi_hist(t8, m8, T), R.mi_hist(t8, m8, T))
         assert orc.corr_cost(t8, m8, T) == R.corr_cost(t8, m8, T)
+
+
+@pytest.mark.parametrize("name", ["full", "c1_blob", "c1_class", "c1_class_u8"])
+def test_oracle_cdm_full_matches_reference(orc, golden, name):
+    """The oracle's CDM driver against the reference's own cdm_common at the workloads'
+    shapes (cdm_full fixture: the 182x218x182 uint8 pair at min_dimension 32, the 64^3
+    blob pair of the plain CDM workload -- the zero field -- and a 64^3 class-phantom
+    pair, float and uint8); inputs regenerated from their seeds and checked first."""
+    import hashlib
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_golden import CDM_FULL_CASES, cdm_full_inputs
+
+    g = golden("cdm_full")
+    gen, dt, kw = {c[0]: (c[1], c[2], c[3]) for c in CDM_FULL_CASES}[name]
+    It, Is = cdm_full_inputs(gen, dt)
+    dig = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()  # noqa: E731
+    assert dig(It) == str(g[f"{name}_It_sha256"]) and dig(Is) == str(g[f"{name}_Is_sha256"])
+    d, ok, _ = orc.cdm(It, Is, **kw)
+    assert int(ok) == int(g[f"{name}_ok"])
+    assert dig(np.ascontiguousarray(d, np.float32)) == str(g[f"{name}_sha256"])

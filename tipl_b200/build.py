@@ -42,8 +42,10 @@ def _newest(paths):
     return max(os.path.getmtime(p) for p in paths) if paths else 0.0
 
 
-def _compile(src, verbose, extra):
+def _compile(src, verbose, extra, hdr_time=0.0):
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    if not extra and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_time):
+        return obj  # up to date (every header counts as a dependency of every source)
     if src.endswith(".cu"):
         cmd = [NVCC] + NVCC_FLAGS + extra + [f"-I{INCLUDE}", "-c", src, "-o", obj]
     else:
@@ -68,8 +70,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         raise RuntimeError(f"nvcc not found at {NVCC}")
     os.makedirs(BUILD, exist_ok=True)
     extra = ["-Xptxas", "-v"] if ptxas_info else []
+    hdr_time = float("inf") if force else _newest([os.path.join(CSRC, f) for f in hdr] +
+                                                  [os.path.join(INCLUDE, "regb200.h"), __file__])
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose or ptxas_info, extra), srcs))
+        objs = list(ex.map(lambda s: _compile(s, verbose or ptxas_info, extra, hdr_time), srcs))
     tmp = OUT + ".tmp"
     cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lz", "-lpthread", "-ldl", "-lrt"]
     if verbose:

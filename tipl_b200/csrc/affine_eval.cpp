@@ -103,6 +103,13 @@ void TexVol::build(const uint8_t* v, Dim3 d, cudaStream_t st)
 // block counts which voxels, so every choice gives the same costs.
 static std::atomic<int> g_min_block_voxels[3] = {{32768}, {60000}, {60000}};
 
+void check_mi_width(int fixed_width, const char* who)
+{
+    if (fixed_width > kMiMaxWidth)
+        throw Failure(REGB_ERR_ARG, std::string(who) + ": the 256-bin MI takes fixed volumes at most 65535 voxels "
+                                                       "wide (16-bit per-block counters)");
+}
+
 int min_block_voxels(int cost_type) { return g_min_block_voxels[cost_type].load(); }
 void set_min_block_voxels(int cost_type, int v) { g_min_block_voxels[cost_type].store(v); }
 
@@ -274,6 +281,8 @@ AffineEvaluator::AffineEvaluator(const std::vector<Pair>& levels, int cost_type,
             L.p.from = L.qf.p;
             L.p.to = L.qt.p;
         }
+        if (cost_type == REGB_COST_MI)
+            check_mi_width(L.p.fd.w, "MI cost");
         const uint8_t* grid = L.p.from;
         long long n = L.p.fd.n();
         if (cost_type == REGB_COST_CORR && L.p.fd.n() > L.p.td.n()) {  // reg/linear.hpp:28-33

@@ -53,6 +53,11 @@ struct TexVol {
 
 // normalize_upper_lower2 bound of the 32-bin MI: float(32) - 0.01f (reg/linear.hpp:195-196)
 constexpr float kMi32Upper = 32.0f - 0.01f;
+// The 256-bin MI kernel counts in 16-bit shared-memory counters and a block holds at
+// least one whole row of the fixed grid, so a row may hold at most 65535 voxels.
+constexpr int kMiMaxWidth = 65535;
+// Throws REGB_ERR_ARG when a 256-bin MI grid's rows are wider than kMiMaxWidth.
+void check_mi_width(int fixed_width, const char* who);
 
 // Fills the scratch pointers of h_tasks[0..K), launches the MI or correlation
 // kernel for all of them, and copies the costs back (synchronises st).

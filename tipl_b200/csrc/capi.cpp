@@ -431,6 +431,8 @@ static regb_status affine_cost(const regb_volume* fixed, const regb_volume* movi
             throw Failure(REGB_ERR_ARG, "affine costs take uint8 volumes (reg/linear.hpp:622-629)");
         if (!T || !cost || K < 0)
             throw Failure(REGB_ERR_ARG, "bad transform/cost arguments");
+        if (cost_type == REGB_COST_MI)
+            check_mi_width(fixed->dim[0], "regb_mi_cost");
         if (K == 0)
             return REGB_OK;
         cudaStream_t st = (cudaStream_t)stream;

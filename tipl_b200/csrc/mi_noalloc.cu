@@ -17,7 +17,12 @@
 //   - every call uses the same array; it keeps the last call's contents, so each
 //     call first clears the counters it relies on.  Calls that overlap on the GPU
 //     (issued on different streams, or from different host threads, without
-//     ordering between them) race on the array and give wrong costs.
+//     ordering between them) race on the array and give wrong costs;
+//   - the first call on a device looks up the array's address and, because the CUDA
+//     runtime loads device code lazily, is the call on which this library's kernels
+//     and the array itself are loaded into device memory: make it at initialisation;
+//   - each call synchronises its stream before returning (the transform descriptors
+//     are copied from a host stack array).
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -83,6 +88,7 @@ extern "C" regb_status regb_mi_cost_noalloc(const uint8_t* fixed, const int fixe
         for (int i = 0; i < 3; ++i)
             if (fixed_dim[i] <= 0 || moving_dim[i] <= 0)
                 throw Failure(REGB_ERR_ARG, "regb_mi_cost_noalloc: non-positive dimension");
+        check_mi_width(fixed_dim[0], "regb_mi_cost_noalloc");
         const long long nf = (long long)fixed_dim[0] * fixed_dim[1] * fixed_dim[2];
         const long long nm = (long long)moving_dim[0] * moving_dim[1] * moving_dim[2];
         if (nf > (1LL << 31) - 1 || nm > (1LL << 31) - 1)
@@ -119,7 +125,7 @@ extern "C" regb_status regb_mi_cost_noalloc(const uint8_t* fixed, const int fixe
         }
         REGB_CK(cudaMemcpyAsync(s->tasks, h, sizeof(AffineTask) * K, cudaMemcpyHostToDevice, st));
         REGB_CK(launch_mi(s->tasks, K, max_chunks, st));
-        count_launch(3);  // the fixed-volume statistics, the histogram and the reduction
+        count_launch(2);  // the histogram and the reduction (launch_fixed_stats counts its own)
         // h is a stack array: the copy must have read it before returning
         REGB_CK(cudaStreamSynchronize(st));
         return REGB_OK;

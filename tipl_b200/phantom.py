@@ -185,3 +185,28 @@ def affine_matrix_f32(p, from_shape, from_vs, to_shape, to_vs) -> np.ndarray:
     tz, ty, tx = to_shape
     sh = sh + np.array([tx, ty, tz], f32) * f32(0.5)
     return np.concatenate([m.reshape(-1), sh]).astype(np.float32)
+
+
+def cdm_workload_pair(shape=(182, 218, 182), seed=None):
+    """Template/moving float32 pair of the nonlinear workloads: a class phantom and the
+    same phantom warped by a smooth field (sigma 6, max 4 voxels) with 2% Rician noise.
+    At 182x218x182 with min_dimension 32 its CDM iterates the 23, 46 and 91 levels and
+    the field moves (max |d| about 2 voxels)."""
+    rng = np.random.default_rng(seed if seed is not None else seed_for(4))
+    t = class_phantom(shape, rng)
+    d = smooth_field(shape, rng, 6.0, 4.0)
+    m = rician(warp(t, d), rng)
+    return t.astype(np.float32), m.astype(np.float32)
+
+
+def cdm_class_pair(shape=(64, 64, 64), seed=None):
+    """Config-1-shaped CDM pair whose field moves at the default cdm_param: a class
+    phantom and the same phantom warped by a smooth field (sigma 6, max 3 voxels) with
+    2% Rician noise, float32.  (The blob pair of cdm_pair has smooth, nearly linear 5^3
+    windows everywhere, and the reference's CDM never improves on its first iteration
+    there: it returns the zero field.)"""
+    rng = np.random.default_rng(seed if seed is not None else seed_for(1, 100))
+    t = class_phantom(shape, rng)
+    d = smooth_field(shape, rng, 6.0, 3.0)
+    m = rician(warp(t, d), rng)
+    return t.astype(np.float32), m.astype(np.float32)
