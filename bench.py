@@ -255,6 +255,71 @@ def cdm_case(args):
     return 0
 
 
+def l2_copy_gbs(torch):
+    """Device-to-device copy bandwidth of an L2-resident pair of 32 MB buffers (read +
+    write bytes), CUDA events over 200 copies: the denominator for CDM levels whose
+    fields fit in the 126 MB L2."""
+    a = torch.ones(32 << 20, dtype=torch.uint8, device="cuda")
+    b = torch.empty_like(a)
+    for _ in range(20):
+        b.copy_(a)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(200):
+        b.copy_(a)
+    e1.record()
+    torch.cuda.synchronize()
+    return 200 * 2 * a.numel() / (e0.elapsed_time(e1) / 1000.0) / 1e9
+
+
+def cdm_result(hbm, hbm_kind, runs=3):
+    """The nonlinear workload's CDM: cdm_common of the 182x218x182 uint8 pair (a class
+    phantom and the same phantom warped by a smooth field of up to 4 voxels, Rician
+    noise) at min_dimension 32, so the 23, 46 and 91 levels iterate.  Device-timed per
+    registration (device-resident inputs, L2 flushed before each run), with the CDM pass
+    model's bytes against the measured HBM peak and an L2-resident copy bandwidth."""
+    import torch
+
+    import tipl_b200 as tb
+    from tipl_b200 import _lib
+    from tipl_b200 import phantom as ph
+
+    t, m = ph.cdm_workload_pair(SHAPE)
+    It = torch.from_numpy(ph.normalize_to_u8(t)).cuda()
+    Is = torch.from_numpy(ph.normalize_to_u8(m)).cuda()
+    p = tb.reg.cdm_param(min_dimension=32)
+    field, ok = tb.reg.cdm(It, Is, p)  # warm-up
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    L = _lib.lib()
+    ms, st = [], None
+    for _ in range(runs):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        L.regb_stats_reset(0)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        field, ok = tb.reg.cdm(It, Is, p, out=field)
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+        st = _lib.Stats()
+        L.regb_stats_get(st)
+    med = statistics.median(ms)
+    achieved = st.cdm_model_bytes / (med / 1000.0) / 1e9
+    l2 = l2_copy_gbs(torch)
+    return {"workload": "CDM (cdm_common, 'r' gradient) of the 182x218x182 uint8 nonlinear-workload pair, "
+                        "min_dimension 32 (levels 23/46/91 iterate)",
+            "ok": bool(ok), "ms_per_registration": med, "ms_runs": ms, "iterations": int(st.cdm_iterations),
+            "voxel_iterations": st.cdm_voxel_iterations, "pass_model_bytes": st.cdm_model_bytes,
+            "pass_model_note": "600 B per voxel and iteration for uint8: compose 14, gradient 18, cost mean 4, "
+                               "Poisson init 24 + 12 sweeps x 36, scale 24, accumulate 60, smooth 24",
+            "achieved_gbs": achieved, "hbm_peak_gbs": hbm, "hbm_peak_kind": hbm_kind, "hbm_frac": achieved / hbm,
+            "l2_copy_gbs": l2, "l2_frac": achieved / l2,
+            "field_max_abs": float(field.abs().max()), "gpu_launches": int(st.launches)}
+
+
 def precision_report(args):
     """The mixed-precision workload: a 182x218x182 template and a subject (random affine,
     smooth displacement up to 4 voxels, 2% Rician-like noise) stored as uint16 and as
@@ -679,14 +744,14 @@ def run_served(args, rank, world, dist):
     return t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects, plain, tuned
 
 
-def batch_case(args):
+def batch_result(args, n_subjects):
     """A batch of --subjects registrations submitted at once: moving volumes of uneven
     shape (each dimension 96-256 voxels, isotropic voxel size U(0.8, 2.0) mm, uint16), each
     the 182x218x182 template phantom under its own random affine (resampled to its grid)
     with 2% Rician noise, registered to the one resident 182x218x182 template at 1 mm:
     affine (MI) then 3-level CDM (min_dimension 32).  Reports registrations/s for the
     whole batch and the per-job latency percentiles, beside the same jobs run as plain
-    single-job calls one after another (a sample of 4)."""
+    single-job calls one after another (a sample of 4).  Returns the result as a dict."""
     import torch
 
     import tipl_b200 as tb
@@ -697,7 +762,7 @@ def batch_case(args):
     td = torch.from_numpy(t).cuda()
     tmpl = ph.normalize_to_u8(t)
     subjects, vss = [], []
-    for k in range(args.subjects):
+    for k in range(n_subjects):
         shape = tuple(int(v) for v in rng.integers(96, 257, 3))
         vs = float(rng.uniform(0.8, 2.0))
         # subject voxel -> template voxel: the template's grid seen through the subject's
@@ -721,7 +786,7 @@ def batch_case(args):
         plain(subjects[k], vss[k])
     torch.cuda.synchronize()
     plain_rate = 4 / (time.perf_counter() - t0)
-    with tb.Engine(hbm_budget_bytes=150 << 30, max_active=args.subjects) as eng:
+    with tb.Engine(hbm_budget_bytes=150 << 30, max_active=n_subjects) as eng:
         tid = eng.add_template(t)
         for k in range(2):  # warm-up
             eng.wait(eng.submit(subjects[k], vss[k], template=tid, cdm=True, cdm_param=cdm_p))
@@ -734,16 +799,21 @@ def batch_case(args):
         est = eng.stats()
     lat = sorted(r["queued_ms"] + r["run_ms"] for r in res)
     pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]  # noqa: E731
-    print(json.dumps({"workload": f"batch of {args.subjects} uneven-shape uint16 subjects (96-256 voxels a side, "
-                                  "voxel size 0.8-2.0 mm) to one resident 182x218x182 template: affine MI + 3-level CDM",
-                      "metric": "registrations/s (whole batch, subjects from host memory) and latency",
-                      "value": args.subjects / dt, "unit": "registrations/s", "seconds": dt,
-                      "ok": sum(int(r["status"] == 0 and r["cdm_ok"]) for r in res),
-                      "latency_ms": {"p50": pct(0.5), "p95": pct(0.95), "p99": pct(0.99)},
-                      "plain_sequential_registrations_per_s": plain_rate,
-                      "engine": {"affine_launches": est["affine_launches"], "affine_tasks": est["affine_tasks"],
-                                 "cdm_rounds": est["cdm_rounds"]},
-                      "data": "synthetic"}))
+    return {"workload": f"batch of {n_subjects} uneven-shape uint16 subjects (96-256 voxels a side, "
+                        "voxel size 0.8-2.0 mm) to one resident 182x218x182 template: affine MI + 3-level CDM",
+            "metric": "registrations/s (whole batch, subjects from host memory) and latency",
+            "value": n_subjects / dt, "unit": "registrations/s", "seconds": dt,
+            "ok": sum(int(r["status"] == 0 and r["cdm_ok"]) for r in res),
+            "latency_ms": {"p50": pct(0.5), "p95": pct(0.95), "p99": pct(0.99)},
+            "plain_sequential_registrations_per_s": plain_rate,
+            "batched_over_plain": (n_subjects / dt) / plain_rate,
+            "engine": {"affine_launches": est["affine_launches"], "affine_tasks": est["affine_tasks"],
+                       "cdm_rounds": est["cdm_rounds"]},
+            "data": "synthetic"}
+
+
+def batch_case(args):
+    print(json.dumps(batch_result(args, args.subjects)))
     return 0
 
 
@@ -867,6 +937,8 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=8,
                     help="served mode: plain single-job registrations timed afterwards for the served/plain ratio")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave the cdm and batch objects (the nonlinear and batched workloads) out of the line")
     ap.add_argument("--cost", choices=["mi", "mi32", "corr"], default=None,
                     help="served / plain affine cost: the reference's 256x256-bin MI, or the 32x32-bin variant")
     ap.add_argument("--kernel-case", choices=["mi", "mi32", "corr", "cdm", "pre", "nifti"], default=None,
@@ -1052,6 +1124,10 @@ def served_line(args, rank, world, dist, torch):
             ref_gpu = {"value": 1.0 / g["linear_s"], "unit": "registrations/s", "final_cost": g["linear_cost"],
                        "kind": "the reference's own CUDA path (tipl::reg::linear, cuda = true) built for sm_100a",
                        "sample": "one registration of the first subject from host buffers, wall clock"}
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras["cdm"] = cdm_result(hbm, hbm_kind)
+        extras["batch"] = batch_result(args, 64)
     if rank == 0:
         lat_s = sorted(lat)
 
@@ -1096,6 +1172,7 @@ def served_line(args, rank, world, dist, torch):
                         "h2d_bytes_per_step": int(sum(m.nbytes for m in subjects)),
                         "d2h_bytes_per_step": 56 * args.batch},
                 "gpu_launches": int(st.launches), "clocks": clocks}
+        line.update(extras)
         print(json.dumps(line))
     if dist:
         dist.barrier()

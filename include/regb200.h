@@ -108,6 +108,12 @@ typedef struct {
     double corr_voxels, corr_bytes, corr_ms;
     double mi_busy_ms;   /* union of the MI launches' device intervals (launches on two
                             streams may overlap, so it can be below mi_ms) */
+    long long cdm_iterations;  /* CDM iterations run (every level, every job) */
+    double cdm_voxel_iterations;  /* sum over CDM levels of iterations x voxels of the level */
+    double cdm_model_bytes;  /* the CDM pass model's bytes: voxel iterations x (596 + 4 x
+                                bytes per pixel) -- compose, gradient, cost mean, Poisson
+                                init and 12 sweeps, scale, accumulate, smooth, each pass
+                                reading its inputs and writing its outputs once */
 } regb_stats;
 regb_status regb_stats_reset(int timing);
 regb_status regb_stats_get(regb_stats* out);
@@ -321,6 +327,16 @@ regb_status regb_cdm(const regb_volume* It, const regb_volume* Is, regb_field* d
  * modality 0 and 'r' for the others.  regb_cdm is this call with nmod = 1. */
 regb_status regb_cdm_multi(const regb_volume* It, const regb_volume* Is, int nmod, regb_field* dis_out,
                            const regb_cdm_param* param, const char* gradient_types, volatile const int* terminated);
+/* cdm_common<out, unsigned char, 2> over lists of 2-D modality pairs (reg/cdm.hpp:373-474,
+ * 534-558 at dimension 2; the GPU instantiation it replaces is cdm_cuda<tipl::out,
+ * unsigned char, 2> of reg/cdm_cu.hpp:12-17): It[i] / Is[i] uint8 images of dims
+ * (w, h, 1), all alike.  dis_out has dims (w, h, 1) and receives the field as
+ * interleaved x, y floats (tipl::vector<2>), 2*w*h of them.  The 2-D stencils are the
+ * reference's: bilinear samples, a 5x5 regression window, Poisson and smoothing over
+ * the four flat-index neighbours +-1, +-w with weights -1/4 and smoothing/4, and a
+ * pyramid that recurses while min(w, h) > min_dimension.  Otherwise as regb_cdm_multi. */
+regb_status regb_cdm2d_multi(const regb_volume* It, const regb_volume* Is, int nmod, regb_field* dis_out,
+                             const regb_cdm_param* param, const char* gradient_types, volatile const int* terminated);
 /* tipl::reg::linear<out,3>(from, from_vs, to, to_vs, arg, param, terminated)
  * (reg/linear.hpp:622-700): uint8 volumes (one image pair), arg in/out, final cost
  * out.  cost_evals (may be NULL) receives the number of cost evaluations. */

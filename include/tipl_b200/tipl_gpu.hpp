@@ -5,7 +5,7 @@
 // reg/linear_cu.hpp:1-19; reg/cdm.hpp:525-532 with reg/cdm_cu.hpp:1-19):
 //
 //   tipl::reg::linear_reg_imp<out, mr, unsigned char, 3>(std::true_type, runner, cost_type, terminated)
-//   tipl::reg::cdm_cuda<out, T, 3>(It, Is, d, terminated, param)
+//   tipl::reg::cdm_cuda<out, T, dim>(It, Is, d, terminated, param)
 //
 // This header defines both.  Include it in ONE translation unit after the TIPL
 // headers, compile that unit with -DTIPL_USE_CUDA by the host compiler (no nvcc),
@@ -14,9 +14,10 @@
 // behaviour unchanged: CUDA failures throw std::runtime_error from linear, and
 // make cdm_cuda return false.
 //
-// Coverage: one image pair / one modality per call (the first of each list is
-// used when the lists are longer, as TIPL's own single-modality callers do);
-// 3-D volumes; uint8 for linear, uint8 or float for cdm.
+// Coverage: every image pair of linear's lists and every modality pair of
+// cdm_common's lists; linear on 3-D uint8 volumes (the instantiations of
+// reg/linear_cu.hpp); cdm on 3-D uint8 or float volumes and on 2-D uint8 images
+// (cdm_cuda<out, unsigned char, 2>, the 2-D instantiation of reg/cdm_cu.hpp:12-17).
 #pragma once
 #include <algorithm>
 #include <atomic>
@@ -65,7 +66,10 @@ regb_volume host_volume(const image_type& I, int dtype)
     v.ptr = const_cast<void*>(static_cast<const void*>(&*I.begin()));
     v.dim[0] = int(I.width());
     v.dim[1] = int(I.height());
-    v.dim[2] = int(I.depth());
+    if constexpr (image_type::dimension == 3)
+        v.dim[2] = int(I.depth());
+    else
+        v.dim[2] = 1;  // a 2-D image is (w, h, 1)
     v.dtype = dtype;
     v.location = REGB_HOST;
     return v;
@@ -127,9 +131,11 @@ bool cdm_cuda(const std::vector<tipl::const_pointer_image<dim, value_type> >& It
               const std::vector<tipl::const_pointer_image<dim, value_type> >& Is, tipl::image<dim, tipl::vector<dim> >& d,
               bool& terminated, const cdm_param& param)
 {
-    static_assert(dim == 3, "the GPU registration path is 3-D");
+    static_assert(dim == 2 || dim == 3, "cdm registers 2-D or 3-D images");
     static_assert(std::is_same<value_type, unsigned char>::value || std::is_same<value_type, float>::value,
                   "cdm takes uint8 or float volumes");
+    static_assert(dim == 3 || std::is_same<value_type, unsigned char>::value,
+                  "the 2-D GPU cdm takes uint8 images (cdm_cuda<out, unsigned char, 2>)");
     if (It.empty() || Is.empty())
         return false;
     const int dtype = std::is_same<value_type, float>::value ? REGB_F32 : REGB_U8;
@@ -142,7 +148,7 @@ bool cdm_cuda(const std::vector<tipl::const_pointer_image<dim, value_type> >& It
     }
     d.resize(It[0].shape());
     regb_field f;
-    f.ptr = &d[0][0];
+    f.ptr = &d[0][0];  // tipl::vector<dim> is dim packed floats
     f.dim[0] = vt[0].dim[0];
     f.dim[1] = vt[0].dim[1];
     f.dim[2] = vt[0].dim[2];
@@ -157,11 +163,14 @@ bool cdm_cuda(const std::vector<tipl::const_pointer_image<dim, value_type> >& It
     regb_status st;
     {
         tipl_b200_detail::TerminateMirror mirror(terminated);
-        st = regb_cdm_multi(vt.data(), vs.data(), (int)nmod, &f, &p, param.gradient_type.c_str(), mirror.flag());
+        if constexpr (dim == 2)
+            st = regb_cdm2d_multi(vt.data(), vs.data(), (int)nmod, &f, &p, param.gradient_type.c_str(), mirror.flag());
+        else
+            st = regb_cdm_multi(vt.data(), vs.data(), (int)nmod, &f, &p, param.gradient_type.c_str(), mirror.flag());
     }
     if constexpr (!std::is_void<out_type>::value) {
         if (st != REGB_OK && st != REGB_FALSE && st != REGB_CANCELLED)
-            out_type() << "regb_cdm_multi: " << regb_last_error();
+            out_type() << "cdm: " << regb_last_error();
     }
     return st == REGB_OK || st == REGB_CANCELLED;  // a terminated run still returns its field, as cdm() does
 }

@@ -353,6 +353,22 @@ class Oracle(_Lib):
                                                     ord(gradient_type), C.byref(iters))
         return d, bool(ok), iters.value
 
+    def cdm2d(self, It, Is, resolution=2.0, speed=0.3, smoothing=0.05, min_dimension=16, gradient_types=""):
+        """The reference's cdm() driver at dimension 2 over lists of uint8 image pairs of
+        shape (h, w); returns (field (h, w, 2), ok, iterations)."""
+        It = [np.ascontiguousarray(a, np.uint8) for a in It]
+        Is = [np.ascontiguousarray(a, np.uint8) for a in Is]
+        h, w = It[0].shape
+        pt = (C.c_void_p * len(It))(*[a.ctypes.data for a in It])
+        ps = (C.c_void_p * len(Is))(*[a.ctypes.data for a in Is])
+        d = np.zeros((h, w, 2), np.float32)
+        iters = C.c_int(0)
+        fn = self.lib.orc2_cdm_multi_u8
+        fn.argtypes = [_P, _P, C.c_int, _P, _P, C.c_float, C.c_float, C.c_float, C.c_uint, C.c_char_p, _P]
+        ok = fn(pt, ps, len(It), _ptr(np.array([w, h], np.int32)), _ptr(d), resolution, speed, smoothing,
+                min_dimension, gradient_types.encode(), C.byref(iters))
+        return d, bool(ok), iters.value
+
     def cdm_multi(self, It, Is, resolution=2.0, speed=0.3, smoothing=0.05, min_dimension=16, gradient_types=""):
         """The reference's cdm() driver over lists of modality pairs (reg/cdm.hpp:419-435);
         returns (field, ok, iterations)."""
@@ -482,6 +498,21 @@ class Reference(_Lib):
         fn = self.lib.tiplref_cdm_u8 if It.dtype == np.uint8 else self.lib.tiplref_cdm_f32
         ok = fn(_ptr(np.ascontiguousarray(It)), _ptr(np.ascontiguousarray(Is, It.dtype)), _ptr(_dims(It.shape)),
                 _ptr(d), resolution, speed, smoothing, min_dimension)
+        return d, bool(ok)
+
+    def cdm2d(self, It, Is, resolution=2.0, speed=0.3, smoothing=0.05, min_dimension=16, gradient_types=""):
+        """cdm_common<void, unsigned char, 2> over lists of uint8 image pairs of shape
+        (h, w); returns (field (h, w, 2), ok)."""
+        It = [np.ascontiguousarray(a, np.uint8) for a in It]
+        Is = [np.ascontiguousarray(a, np.uint8) for a in Is]
+        h, w = It[0].shape
+        pt = (C.c_void_p * len(It))(*[a.ctypes.data for a in It])
+        ps = (C.c_void_p * len(Is))(*[a.ctypes.data for a in Is])
+        d = np.zeros((h, w, 2), np.float32)
+        fn = self.lib.tiplref_cdm2d_multi_u8
+        fn.argtypes = [_P, _P, C.c_int, _P, _P, C.c_float, C.c_float, C.c_float, C.c_uint, C.c_char_p]
+        ok = fn(pt, ps, len(It), _ptr(np.array([w, h], np.int32)), _ptr(d), resolution, speed, smoothing,
+                min_dimension, gradient_types.encode())
         return d, bool(ok)
 
     def cdm_multi(self, It, Is, resolution=2.0, speed=0.3, smoothing=0.05, min_dimension=16, gradient_types=""):

@@ -225,6 +225,9 @@ int orc_is_integer_shift(const float* T, int* shift)
 #undef PIX
 #undef R
 
+/* the 2-D CDM (uint8 images; uses regress_u8 and cdm_improved_u8 from above) */
+#include "oracle_cdm2d.h"
+
 #define SFX _f32
 #define FSFX _f32
 #define PIX float

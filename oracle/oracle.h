@@ -77,6 +77,20 @@ int orc_cdm_multi_f64(const double* const* It, const double* const* Is, int nmod
                       float resolution, float speed, float smoothing, unsigned int min_dimension, const char* gtypes,
                       int* iters_out);
 
+/* The CDM at dimension 2 (oracle_cdm2d.h): uint8 images of dims (w, h), fields as
+ * interleaved (x, y) floats. */
+void orc2_downsample_u8(const uint8_t* in, const int* dim, uint8_t* out);
+void orc2_upsample_field_x2(const float* in, const int* in_dim, float* out, const int* out_dim);
+void orc2_compose_u8(const uint8_t* Is, const int* dim, const float* d, uint8_t* Js);
+float orc2_cdm_gradient_u8(const uint8_t* Js, const uint8_t* It, const int* dim, float* new_d, int gradient_type);
+void orc2_cdm_poisson(float* new_d, const int* dim, int sweeps);
+float orc2_cdm_max_len(const float* d, const int* dim);
+void orc2_accumulate(const float* cur_d, float* new_d, const int* dim);
+void orc2_cdm_smooth(const float* d, float* dd, const int* dim, float smoothing);
+int orc2_cdm_multi_u8(const uint8_t* const* It, const uint8_t* const* Is, int nmod, const int* dim, float* best_d,
+                      float resolution, float speed, float smoothing, unsigned int min_dimension, const char* gtypes,
+                      int* iters_out);
+
 int orc_normalize_to_u8_f32(const float* in, long long n, uint8_t* out, float upper);
 int orc_normalize_to_u8_u16(const uint16_t* in, long long n, uint8_t* out, float upper);
 int orc_normalize_to_u8_u8(const uint8_t* in, long long n, uint8_t* out, float upper);

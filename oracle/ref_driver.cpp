@@ -269,6 +269,33 @@ int tiplref_cdm_multi_f32(const float* const* It, const float* const* Is, int nm
     return cdm_multi(It, Is, nmod, dim, dis_out, resolution, speed, smoothing, min_dimension, gtypes);
 }
 
+// cdm_common<void, unsigned char, 2>(It, Is, dis, terminated, param, cuda = false)
+// (reg/cdm.hpp:534-558 at dimension 2): 2-D uint8 images of dims (w, h); the field
+// out as interleaved (x, y) floats.
+int tiplref_cdm2d_multi_u8(const u8* const* It, const u8* const* Is, int nmod, const int* dim, float* dis_out,
+                           float resolution, float speed, float smoothing, unsigned int min_dimension,
+                           const char* gtypes)
+{
+    tipl::reg::cdm_param p;
+    p.resolution = resolution;
+    p.speed = speed;
+    p.smoothing = smoothing;
+    p.min_dimension = min_dimension;
+    p.gradient_type = gtypes ? gtypes : "";
+    const tipl::shape<2> sh(dim[0], dim[1]);
+    std::vector<tipl::const_pointer_image<2, u8> > lt, ls;
+    for (int i = 0; i < nmod; ++i) {
+        lt.push_back(tipl::const_pointer_image<2, u8>(It[i], sh));
+        ls.push_back(tipl::const_pointer_image<2, u8>(Is[i], sh));
+    }
+    tipl::image<2, tipl::vector<2> > dis;
+    bool terminated = false;
+    const bool ok = tipl::reg::cdm_common<void, u8, 2>(lt, ls, dis, terminated, p, false);
+    if (ok)
+        std::memcpy(dis_out, &dis[0][0], sizeof(float) * 2 * dis.size());
+    return ok ? 1 : 0;
+}
+
 // linear<void>(from, from_vs, to, to_vs, arg, param) (reg/linear.hpp:622-700); returns the final cost.
 float tiplref_linear(const u8* from, const int* from_dim, const float* from_vs, const u8* to, const int* to_dim,
                      const float* to_vs, float* arg_inout, int reg_type, int cost_type)

@@ -5,10 +5,13 @@
 //   tipl_drop_in linear|cdm gpu|cpu w h d fixed.u8 moving.u8 out.bin
 //   tipl_drop_in cdm2 gpu|cpu w h d fixed.u8 moving.u8 out.bin fixed2.u8 moving2.u8 gradient_types
 //   tipl_drop_in linear2 gpu|cpu w h d fixed.u8 moving.u8 out.bin fixed2.u8 moving2.u8
+//   tipl_drop_in cdm2d gpu|cpu w h 1 fixed.u8 moving.u8 out.bin resolution min_dimension gradient_types
+//                [fixed2.u8 moving2.u8]
 // linear writes cost (float) + 12 params; cdm writes ok (int32) + the field; cdm2 runs
 // cdm_common on the two-modality lists {fixed, fixed2} / {moving, moving2} at
 // resolution 1 with the given cdm_param::gradient_type string; linear2 runs linear on
-// the two-pair lists (mm_reg's mm_linear).
+// the two-pair lists (mm_reg's mm_linear); cdm2d runs cdm_common<void, unsigned char, 2>
+// on 2-D images (one or two modality pairs) and writes ok (int32) + the vector<2> field.
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -31,6 +34,35 @@ static std::vector<unsigned char> read_all(const char* p, size_t n)
 int main(int argc, char** argv)
 {
     const std::string what = argc > 1 ? argv[1] : "";
+    if (what == "cdm2d") {
+        if (argc != 12 && argc != 14) {
+            std::fprintf(stderr, "usage: %s cdm2d gpu|cpu w h 1 fixed moving out res min_dim types [fixed2 moving2]\n",
+                         argv[0]);
+            return 2;
+        }
+        const bool gpu = std::string(argv[2]) == "gpu";
+        const tipl::shape<2> sh(std::atoi(argv[3]), std::atoi(argv[4]));
+        std::vector<std::vector<unsigned char>> bufs;
+        std::vector<tipl::const_pointer_image<2, unsigned char>> F, M;
+        for (int k = 6; k < argc; k += (k == 7 ? 5 : 1)) {
+            bufs.push_back(read_all(argv[k], sh.size()));
+            (bufs.size() % 2 ? F : M).push_back(tipl::const_pointer_image<2, unsigned char>(bufs.back().data(), sh));
+        }
+        tipl::reg::cdm_param param;
+        param.resolution = (float)std::atof(argv[9]);
+        param.min_dimension = (unsigned int)std::atoi(argv[10]);
+        param.gradient_type = std::string(argv[11]) == "-" ? "" : argv[11];
+        tipl::image<2, tipl::vector<2>> dis;
+        bool terminated = false;
+        bool ok = tipl::reg::cdm_common<void, unsigned char, 2>(F, M, dis, terminated, param, gpu);
+        std::ofstream out(argv[8], std::ios::binary);
+        int32_t okv = ok ? 1 : 0;
+        out.write((const char*)&okv, 4);
+        if (ok)
+            out.write((const char*)&dis[0][0], (std::streamsize)(dis.size() * 8));
+        std::printf("cdm2d %s ok %d\n", gpu ? "gpu" : "cpu", okv);
+        return 0;
+    }
     if (argc != (what == "cdm2" ? 12 : what == "linear2" ? 11 : 9)) {
         std::fprintf(stderr, "usage: %s linear|cdm|cdm2 gpu|cpu w h d fixed moving out [fixed2 moving2 types]\n",
                      argv[0]);

@@ -34,7 +34,7 @@ def main():
                     help="the reference source tree (default: $TIPL_REF_ROOT)")
     ap.add_argument("--only", default=None,
                     help="make one fixture group: core | mask_init | precision | preprocess | linear_runs"
-                         " | mapping | mi32 | nifti | cdm_multi | cdm_full")
+                         " | mapping | mi32 | nifti | cdm_multi | cdm_full | cdm2d")
     args = ap.parse_args()
     oracle.build(args.ref_root, with_ref=True)
     R = oracle.Reference()
@@ -59,6 +59,8 @@ def main():
         cdm_multi(R)
     if args.only in (None, "cdm_full"):
         cdm_full(R)
+    if args.only in (None, "cdm2d"):
+        cdm2d(R)
 
 
 NIFTI_DIR = os.path.join(HERE, "nifti")
@@ -165,6 +167,52 @@ def cdm_full(R):
         out[f"{name}_maxabs"] = np.array(float(np.abs(d).max()) if ok else 0.0)
         print(name, ok, float(np.abs(d).max()), flush=True)
     save("cdm_full", **out)
+
+
+# (shape (h, w), resolution, min_dimension, gradient types, modalities, variant)
+CDM2D_CASES = [((64, 72), 2.0, 16, "", 1, ""), ((96, 80), 1.0, 16, "", 1, ""), ((33, 47), 1.0, 8, "d", 1, ""),
+               ((64, 64), 1.0, 16, "rd", 2, ""), ((128, 120), 2.0, 16, "", 1, ""), ((256, 256), 2.0, 16, "", 1, ""),
+               ((40, 2), 1.0, 1, "", 1, ""), ((1, 30), 1.0, 1, "", 1, ""), ((48, 40), 1.0, 16, "", 2, "zero0")]
+
+
+def cdm2d_inputs(shape, nmod, rng):
+    """2-D uint8 pairs: a slice of a class phantom and the same slice warped in-plane by
+    a smooth 2-D field (the x, y components of a sigma-4 field, max 3 pixels) with
+    Rician noise; the second modality is the inverted contrast inside the head."""
+    from scipy import ndimage
+
+    t = ph.class_phantom((3,) + tuple(shape), rng)[1]
+    d = ph.smooth_field((3,) + tuple(shape), rng, 4.0, 3.0)[1]
+    y, x = np.meshgrid(np.arange(shape[0], dtype=np.float32), np.arange(shape[1], dtype=np.float32), indexing="ij")
+    m = ndimage.map_coordinates(t, np.stack([y + d[..., 1], x + d[..., 0]]), order=1, mode="constant")
+    m = ph.rician(m.astype(np.float32), rng)
+    It, Is = [ph.normalize_to_u8(t)], [ph.normalize_to_u8(m)]
+    if nmod > 1:
+        It.append(ph.normalize_to_u8(np.where(t > 0, 4095 - t, 0).astype(np.float32)))
+        Is.append(ph.normalize_to_u8(np.where(m > 50, 4095 - m, 0).astype(np.float32)))
+    return It, Is
+
+
+def cdm2d(R):
+    """cdm_common<void, unsigned char, 2> (reg/cdm.hpp:373-474, 534-558 at dimension 2;
+    the reference's CPU branch, one thread) on 2-D uint8 pairs: default and full
+    resolution, gradient types 'r' / 'd' / "rd", one and two modalities, odd shapes,
+    1- and 2-pixel axes, and a zero modality-0 template (false).  Stored: the inputs,
+    the field's SHA-256 and max |d|, ok."""
+    rng = np.random.default_rng(ph.seed_for(7, 2))
+    out = {}
+    for k, (shape, res, md, gt, nmod, var) in enumerate(CDM2D_CASES):
+        It, Is = cdm2d_inputs(shape, nmod, rng)
+        if var == "zero0":
+            It[0] = np.zeros_like(It[0])
+        d, ok = R.cdm2d(It, Is, resolution=res, min_dimension=md, gradient_types=gt)
+        for i in range(nmod):
+            out[f"c{k}_It{i}"], out[f"c{k}_Is{i}"] = It[i], Is[i]
+        out[f"c{k}_ok"] = np.array(int(ok))
+        out[f"c{k}_sha256"] = np.array(field_digest(d) if ok else "")
+        out[f"c{k}_maxabs"] = np.array(float(np.abs(d).max()) if ok else 0.0)
+        print(k, shape, ok, float(np.abs(d).max()) if ok else None, flush=True)
+    save("cdm2d", **out)
 
 
 def nifti_bytes(data, datatype, bitpix, srow=None, pixdim=(1.0, 1.0, 1.0), qform=None, big=False, version=1,

@@ -111,3 +111,36 @@ def test_linear_two_pairs_gpu_branch_close_to_cpu_branch(volumes):
     c = [run2("cpu")[0] for _ in range(3)]
     assert np.isfinite(g).all()
     assert g[0] <= max(c) * 1.025, (g[0], c)
+
+
+@pytest.mark.parametrize("k", [0, 2, 3, 5])
+def test_cdm_common_2d_gpu_branch_equals_cpu_branch(volumes, golden, k):
+    """cdm_common<void, unsigned char, 2> (the reference's cdm_cuda<tipl::out, unsigned
+    char, 2> instantiation, reg/cdm_cu.hpp:12-17): its GPU branch runs through the
+    shim's 2-D cdm_cuda on regb_cdm2d_multi and its field equals the CPU branch's bit
+    for bit (cdm2d fixture cases: default parameters, a 'd' gradient on an odd shape,
+    two modalities "rd", 256 x 256)."""
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_golden import CDM2D_CASES
+
+    d, _ = volumes
+    g = golden("cdm2d")
+    (h, w), res, md, gt, nmod, _ = CDM2D_CASES[k]
+    for i in range(nmod):
+        g[f"c{k}_It{i}"].tofile(d / f"f2d_{i}.u8")
+        g[f"c{k}_Is{i}"].tofile(d / f"m2d_{i}.u8")
+    res_out = {}
+    for where in ("gpu", "cpu"):
+        out = d / f"cdm2d_{where}.bin"
+        args = [BIN, "cdm2d", where, str(w), str(h), "1", str(d / "f2d_0.u8"), str(d / "m2d_0.u8"), str(out), str(res),
+                str(md), gt or "-"]
+        if nmod == 2:
+            args += [str(d / "f2d_1.u8"), str(d / "m2d_1.u8")]
+        r = subprocess.run(args, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+        res_out[where] = np.fromfile(out, dtype=np.uint8)
+    assert res_out["gpu"][:4].view(np.int32)[0] == 1 and res_out["cpu"][:4].view(np.int32)[0] == 1
+    assert np.abs(res_out["cpu"][4:].view(np.float32)).max() > 0.5  # the field moves
+    assert np.array_equal(res_out["gpu"], res_out["cpu"])

@@ -177,3 +177,23 @@ def test_oracle_cdm_full_matches_reference(orc, golden, name):
     d, ok, _ = orc.cdm(It, Is, **kw)
     assert int(ok) == int(g[f"{name}_ok"])
     assert dig(np.ascontiguousarray(d, np.float32)) == str(g[f"{name}_sha256"])
+
+
+def test_oracle_cdm2d_matches_reference(orc, golden):
+    """The oracle's 2-D CDM (oracle_cdm2d.h) against the reference's own
+    cdm_common<void, unsigned char, 2> on every cdm2d case: field digests bit for bit,
+    ok, and the false return of a zero modality-0 template."""
+    import hashlib
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_golden import CDM2D_CASES
+
+    g = golden("cdm2d")
+    for k, (shape, res, md, gt, nmod, _) in enumerate(CDM2D_CASES):
+        It = [g[f"c{k}_It{i}"] for i in range(nmod)]
+        Is = [g[f"c{k}_Is{i}"] for i in range(nmod)]
+        d, ok, _ = orc.cdm2d(It, Is, resolution=res, min_dimension=md, gradient_types=gt)
+        assert int(ok) == int(g[f"c{k}_ok"]), k
+        if ok:
+            assert hashlib.sha256(d.tobytes()).hexdigest() == str(g[f"c{k}_sha256"]), k

@@ -494,19 +494,40 @@ class reg:
         """tipl::reg::cdm_common: returns (field, ok).  It / Is are one volume each or
         equal-length lists of modality pairs (make_list(J), make_list(It) in mm_reg);
         gradient_types is cdm_param::gradient_type, one 'r' / 'd' per modality ('r'
-        past its end; None = param.gradient_type for the first modality)."""
+        past its end; None = param.gradient_type for the first modality).  2-D uint8
+        images (shape (h, w)) take the reference's dimension-2 path; their field has
+        shape (h, w, 2)."""
         multi = isinstance(It, (list, tuple))
         Its = list(It) if multi else [It]
         Iss = list(Is) if isinstance(Is, (list, tuple)) else [Is]
         n = min(len(Its), len(Iss))  # cdm_common truncates the longer list (reg/cdm.hpp:542-545)
         if n < 1:
             raise ValueError("cdm: empty modality list")
-        d = _like(Its[0], tuple(Its[0].shape) + (3,), dtype=_f32_like(Its[0])) if out is None else out
+        two_d = len(Its[0].shape) == 2
         p = param or reg.cdm_param()
         term = None if terminated is None else C.cast(terminated, C.c_void_p)
+        gt = None if gradient_types is None else str(gradient_types).encode()
+        if two_d:
+            h, w = Its[0].shape
+            d = _like(Its[0], (h, w, 2), dtype=_f32_like(Its[0])) if out is None else out
+
+            def vol2(a):  # a 2-D image as a volume of dims (w, h, 1)
+                return _vol(a.reshape(1, *a.shape))
+
+            vt = (_lib.Volume * n)(*[vol2(a) for a in Its[:n]])
+            vs = (_lib.Volume * n)(*[vol2(a) for a in Iss[:n]])
+            if _is_dev(d):
+                assert d.is_contiguous() and tuple(d.shape) == (h, w, 2)
+                f = _lib.Field(d.data_ptr(), (C.c_int * 3)(w, h, 1), _lib.DEVICE)
+            else:
+                assert d.flags["C_CONTIGUOUS"] and d.dtype == np.float32 and d.shape == (h, w, 2)
+                f = _lib.Field(d.ctypes.data, (C.c_int * 3)(w, h, 1), _lib.HOST)
+            st = _lib.lib().regb_cdm2d_multi(vt, vs, n, C.byref(f), C.byref(p), gt, term)
+            _lib.check(st, allow=(_lib.REGB_OK, _lib.REGB_FALSE, _lib.REGB_CANCELLED))
+            return d, st != _lib.REGB_FALSE
+        d = _like(Its[0], tuple(Its[0].shape) + (3,), dtype=_f32_like(Its[0])) if out is None else out
         vt = (_lib.Volume * n)(*[_vol(a) for a in Its[:n]])
         vs = (_lib.Volume * n)(*[_vol(a) for a in Iss[:n]])
-        gt = None if gradient_types is None else str(gradient_types).encode()
         st = _lib.lib().regb_cdm_multi(vt, vs, n, C.byref(_field(d)), C.byref(p), gt, term)
         _lib.check(st, allow=(_lib.REGB_OK, _lib.REGB_FALSE, _lib.REGB_CANCELLED))
         return d, st != _lib.REGB_FALSE

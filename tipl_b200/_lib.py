@@ -46,7 +46,9 @@ class Stats(C.Structure):
     _fields_ = [("launches", C.c_longlong), ("mi_launches", C.c_longlong), ("mi_tasks", C.c_longlong),
                 ("mi_voxels", C.c_double), ("mi_bytes", C.c_double), ("mi_ms", C.c_double),
                 ("corr_launches", C.c_longlong), ("corr_tasks", C.c_longlong), ("corr_voxels", C.c_double),
-                ("corr_bytes", C.c_double), ("corr_ms", C.c_double), ("mi_busy_ms", C.c_double)]
+                ("corr_bytes", C.c_double), ("corr_ms", C.c_double), ("mi_busy_ms", C.c_double),
+                ("cdm_iterations", C.c_longlong), ("cdm_voxel_iterations", C.c_double),
+                ("cdm_model_bytes", C.c_double)]
 
 
 class RunnerState(C.Structure):
@@ -149,6 +151,8 @@ _SIGS = {
                            C.c_void_p]),
     "regb_cdm_multi": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_int, C.POINTER(Field),
                                  C.POINTER(CdmParam), C.c_char_p, C.c_void_p]),
+    "regb_cdm2d_multi": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_int, C.POINTER(Field),
+                                   C.POINTER(CdmParam), C.c_char_p, C.c_void_p]),
     "regb_runner_state_from_param": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.POINTER(LinearParam), C.POINTER(RunnerState)]),
     "regb_linear_run": (C.c_int, [C.POINTER(Volume), C.c_void_p, C.POINTER(Volume), C.c_void_p, C.c_void_p,

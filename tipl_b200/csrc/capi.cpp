@@ -961,6 +961,54 @@ regb_status regb_cdm_multi(const regb_volume* It, const regb_volume* Is, int nmo
     });
 }
 
+regb_status regb_cdm2d_multi(const regb_volume* It, const regb_volume* Is, int nmod, regb_field* dis_out,
+                             const regb_cdm_param* param, const char* gradient_types, volatile const int* terminated)
+{
+    return guarded([&] {
+        if (!It || !Is || nmod < 1 || nmod > kCdmMaxModalities)
+            throw Failure(REGB_ERR_ARG, "cdm2d: 1 to 12 modality pairs");
+        check_field(dis_out, "dis_out");
+        if (dis_out->dim[2] != 1)
+            throw Failure(REGB_ERR_ARG, "cdm2d: 2-D images have dims (w, h, 1)");
+        for (int m = 0; m < nmod; ++m) {
+            check_vol(&It[m], "It");
+            check_vol(&Is[m], "Is");
+            if (!same_dims(It[m].dim, dis_out->dim) || !same_dims(Is[m].dim, dis_out->dim))
+                throw Failure(REGB_ERR_ARG, "cdm2d: It/Is/dis shapes differ");
+            if (It[m].dtype != REGB_U8 || Is[m].dtype != REGB_U8)
+                throw Failure(REGB_ERR_ARG, "cdm2d takes uint8 images (cdm_cuda<out, unsigned char, 2>)");
+        }
+        regb_cdm_param p;
+        regb_cdm_param_default(&p);
+        if (param)
+            p = *param;
+        const char one[2] = {(char)p.gradient_type, 0};
+        const char* gtypes = gradient_types ? gradient_types : one;
+        Stream s;
+        const size_t n = nvox(It[0].dim);
+        Staged a[kCdmMaxModalities], b[kCdmMaxModalities], f;
+        const void* dt[kCdmMaxModalities];
+        const void* ds[kCdmMaxModalities];
+        for (int m = 0; m < nmod; ++m) {
+            a[m].in(It[m].ptr, n, It[m].location, s.s, true);
+            b[m].in(Is[m].ptr, n, Is[m].location, s.s, true);
+            dt[m] = a[m].d;
+            ds[m] = b[m].d;
+        }
+        // the levels hold xyz fields whose z stays 0; the caller's field is x, y pairs
+        DevBuf<float> xyz(3 * n, s.s);
+        f.in(dis_out->ptr, n * 8, dis_out->location, s.s, false);
+        regb_status r = cdm_register_multi(dt, ds, nmod, gtypes, It[0].dim, 0, xyz.p, p, terminated, s.s, nullptr,
+                                           nullptr, 2);
+        if (r == REGB_OK || r == REGB_CANCELLED) {
+            REGB_CK(launch_field_xy(xyz.p, (long long)n, (float*)f.d, s.s));
+            f.out(dis_out->ptr, s.s);
+        }
+        s.sync();
+        return r;
+    });
+}
+
 regb_status regb_cdm(const regb_volume* It, const regb_volume* Is, regb_field* dis_out, const regb_cdm_param* param,
                      volatile const int* terminated)
 {

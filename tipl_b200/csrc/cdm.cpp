@@ -68,7 +68,7 @@ void GraphExec::reset()
 }
 
 void CdmLevel::init(const void* const* It_, const void* const* Is_, const std::string& gtypes_, int w, int h, int d,
-                    int pix_, const regb_cdm_param& p, float* best, cudaStream_t st)
+                    int pix_, const regb_cdm_param& p, float* best, cudaStream_t st, int ndim)
 {
     pix = pix_;
     gtypes = gtypes_;
@@ -79,6 +79,7 @@ void CdmLevel::init(const void* const* It_, const void* const* Is_, const std::s
     const long long n = (long long)w * h * d;
     seg.nblk = cdm_blocks_for(n);
     seg.nmod = (int)gtypes.size();
+    seg.ndim = ndim;
     for (int m = 0; m < seg.nmod; ++m) {
         seg.It[m] = It_[m];
         seg.Is[m] = Is_[m];
@@ -137,10 +138,13 @@ regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int
 
 regb_status cdm_register_multi(const void* const* d_It, const void* const* d_Is, int nmod, const char* gtypes_in,
                                const int* dim, int pix, float* d_field, const regb_cdm_param& p,
-                               volatile const int* terminated, cudaStream_t st, int* iterations, CdmScheduler* sched)
+                               volatile const int* terminated, cudaStream_t st, int* iterations, CdmScheduler* sched,
+                               int ndim)
 {
     if (nmod < 1 || nmod > kCdmMaxModalities)
         throw Failure(REGB_ERR_ARG, "cdm: 1 to 12 modality pairs");
+    if (ndim == 2 && dim[2] != 1)
+        throw Failure(REGB_ERR_ARG, "cdm: a 2-D registration takes images of depth 1");
     // cdm_param::gradient_type: modality i takes its i-th char, 'r' past the end
     std::string gtypes(nmod, 'r');
     const size_t ntype = gtypes_in ? std::strlen(gtypes_in) : 0;
@@ -170,12 +174,18 @@ regb_status cdm_register_multi(const void* const* d_It, const void* const* d_Is,
     lv[0].resolution = p.resolution;
     for (;;) {
         Lv& c = lv.back();
-        if (!((unsigned int)std::min(c.w, std::min(c.h, c.d)) > p.min_dimension))
+        // min_value(It[0].shape()) over the image's own dimensions (reg/cdm.hpp:382)
+        const int mn = ndim == 2 ? std::min(c.w, c.h) : std::min(c.w, std::min(c.h, c.d));
+        if (!((unsigned int)mn > p.min_dimension))
             break;
         Lv n;
         n.w = (c.w + 1) / 2;
         n.h = (c.h + 1) / 2;
         n.d = (c.d + 1) / 2;
+        if (n.w == c.w && n.h == c.h && n.d == c.d)
+            // only min_dimension 0 gets here (an axis of 1 voxel passes "min > 0" forever);
+            // the reference recurses without end and overflows its stack
+            throw Failure(REGB_ERR_ARG, "cdm: min_dimension 0 with a one-voxel axis never stops downsampling");
         n.resolution = c.resolution / 2.0f;
         const size_t nn = (size_t)n.w * n.h * n.d;
         for (int m = 0; m < nmod; ++m) {
@@ -204,14 +214,14 @@ regb_status cdm_register_multi(const void* const* d_It, const void* const* d_Is,
         else {
             const Lv& C = lv[k + 1];
             const float* cb = C.best.p;
-            REGB_CK(launch_upsample_field_x2(cb, C.w, C.h, C.d, best, L.w, L.h, L.d, st));
+            REGB_CK(launch_upsample_field_x2(cb, C.w, C.h, C.d, best, L.w, L.h, L.d, st, ndim));
             if (L.resolution > 1.0f)
                 continue;  // reg/cdm.hpp:404-405
         }
         if (status != REGB_OK)
             continue;
         CdmLevel run;
-        run.init(L.It, L.Is, gtypes, L.w, L.h, L.d, pix, p, best, st);
+        run.init(L.It, L.Is, gtypes, L.w, L.h, L.d, pix, p, best, st, ndim);
         if (sched) {
             // batched with the other jobs' levels; the scheduler returns once this
             // level's loop has ended
@@ -243,6 +253,7 @@ regb_status cdm_register_multi(const void* const* d_It, const void* const* d_Is,
             }
         }
         iters += run.h_ctl.iters_run;
+        count_cdm_level(run.h_ctl.iters_run, (long long)n, pix ? 4 : 1);
         if (run.h_ctl.done == 2)
             return REGB_FALSE;  // reg/cdm.hpp:428-429: a zero cost sum fails the whole call
     }

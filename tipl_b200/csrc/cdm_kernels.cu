@@ -48,6 +48,27 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_compose_kernel(const CdmSeg* 
     const T* __restrict__ Is = (const T*)S.Is[mod];
     T* __restrict__ Js = (T*)S.Js;
     const float* __restrict__ cd = S.cur_d;
+    if (S.ndim == 2) {
+        // the 2-D form: vector<2> field, bilinear sample at (x + dx, y + dy)
+        for (long long i = first; i < n; i += stride) {
+            const float dx = cd[3 * i], dy = cd[3 * i + 1];
+            T v;
+            if (dx == 0.0f && dy == 0.0f)
+                v = Is[i];
+            else {
+                const int x = (int)(i % D.w), y = (int)(i / D.w);
+                float px = (float)x, py = (float)y;
+                px += dx;
+                py += dy;
+                Cell2 c;
+                v = T(0);
+                if (bilinear_cell(D, px, py, c))
+                    v = assign_pix<T>(cell_sum2(Is, D, c));
+            }
+            Js[i] = v;
+        }
+        return;
+    }
     for (long long i = first; i < n; i += stride) {
         const float dx = cd[3 * i], dy = cd[3 * i + 1], dz = cd[3 * i + 2];
         T v;
@@ -517,7 +538,8 @@ __device__ __forceinline__ bool last_block_of_segment(const CdmSeg& S)
 // ------------------------------------------------------------------ Poisson
 // cdm_solve_poisson (reg/cdm.hpp:158-253): s0 = new_d * (-1/6); then Jacobi sweeps
 // s' = (new_d - s[-1] - s[+1] - s[-w] - s[+w] - s[-wh] - s[+wh]) * (-1/6) with the
-// neighbours taken by flat index, bounds on the flat index only.
+// neighbours taken by flat index, bounds on the flat index only (2-D: -1/4 and no
+// +-wh taps).
 // mode 0: the first sweep, reading s0 = new_d * (-1/6) formed on the fly (the same
 //         float product the reference stores), writing B; it also applies this
 //         iteration's best_d save / restore (reg/cdm.hpp:447-457), which the
@@ -527,9 +549,8 @@ __device__ __forceinline__ bool last_block_of_segment(const CdmSeg& S)
 // mode 2: the last sweep (B->A) with the first-iteration max |result| (theta,
 //         reg/cdm.hpp:463-467) formed from the values it writes.
 __device__ __forceinline__ void poisson_point(const float* __restrict__ s, const float* __restrict__ rhs, long long p,
-                                              long long n, long long w, long long wh, bool scale_s, float* v)
+                                              long long n, long long w, long long wh, bool scale_s, float c6, float* v)
 {
-    const float c6 = -0.5f / 3.0f;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         float acc = rhs[3 * p + c];
@@ -551,6 +572,14 @@ __device__ __forceinline__ void poisson_point(const float* __restrict__ s, const
         acc *= c6;
         v[c] = acc;
     }
+}
+
+// inv_d2 = -0.5 / dimension (reg/cdm.hpp:163,175): -1/6 in 3-D, -1/4 in 2-D.  A 2-D
+// level's plane is the whole image (d == 1), so its +-wh taps fall outside the flat
+// index range and drop out, as the reference's 2-D stencil has none.
+__device__ __forceinline__ float poisson_weight(const CdmSeg& S)
+{
+    return S.ndim == 2 ? -0.5f / 2.0f : -0.5f / 3.0f;
 }
 
 __global__ void __launch_bounds__(kCdmThreads) cdm_poisson_kernel(const CdmSeg* __restrict__ segs, int mode,
@@ -593,7 +622,7 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_poisson_kernel(const CdmSeg* 
         // neighbours at voxel offsets 1, w, wh are float offsets 3, 3w, 3wh, and
         // the reference's flat-index bounds p >= k / p < n - k are f >= 3k / f < 3(n - k)
         // -- every tap is a coalesced load, the arithmetic per component unchanged
-        const float c6 = -0.5f / 3.0f;
+        const float c6 = poisson_weight(S);
         const long long N3 = 3 * n, w3 = 3 * w, wh3 = 3 * wh;
         const bool sc = (mode == 0);
         for (long long f = first; f < N3; f += stride) {
@@ -622,7 +651,7 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_poisson_kernel(const CdmSeg* 
     float m = 0.0f;
     for (long long p = first; p < n; p += stride) {
         float v[3];
-        poisson_point(in, rhs, p, n, w, wh, mode == 0, v);
+        poisson_point(in, rhs, p, n, w, wh, mode == 0, poisson_weight(S), v);
         out[3 * p] = v[0];
         out[3 * p + 1] = v[1];
         out[3 * p + 2] = v[2];
@@ -698,6 +727,48 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_accumulate_kernel(const CdmSe
     const float* __restrict__ cd = S.cur_d;
     float* __restrict__ out = S.tmp_d;
     const int w = D.w, wh = D.wh();
+    if (S.ndim == 2) {
+        // the 2-D form: bilinear sample of the mapping cur_d + (x, y); z stays 0
+        for (long long i = first; i < n; i += stride) {
+            float dx = nd[3 * i] * scale, dy = nd[3 * i + 1] * scale;
+            const int x = (int)(i % w), y = (int)(i / w);
+            bool ok = false;
+            if (dx != 0.0f || dy != 0.0f) {
+                dx += (float)x;
+                dy += (float)y;
+                Cell2 cl;
+                if (bilinear_cell(D, dx, dy, cl)) {
+                    const int b = cl.base, bx = b % w, by = b / w;
+                    const int off[4] = {0, 1, w, w + 1};
+                    const int ox[4] = {0, 1, 0, 1};
+                    const int oy[4] = {0, 0, 1, 1};
+                    float ax = 0.f, ay = 0.f;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const float* q = cd + 3LL * (b + off[k]);
+                        const float mx = q[0] + (float)(bx + ox[k]);
+                        const float my = q[1] + (float)(by + oy[k]);
+                        if (k == 0) {
+                            ax = mx * cl.r[0];
+                            ay = my * cl.r[0];
+                        } else {
+                            ax += mx * cl.r[k];
+                            ay += my * cl.r[k];
+                        }
+                    }
+                    out[3 * i] = ax - (float)x;
+                    out[3 * i + 1] = ay - (float)y;
+                    ok = true;
+                }
+            }
+            if (!ok) {
+                out[3 * i] = cd[3 * i];
+                out[3 * i + 1] = cd[3 * i + 1];
+            }
+            out[3 * i + 2] = 0.0f;
+        }
+        return;
+    }
     for (long long i = first; i < n; i += stride) {
         float dx = nd[3 * i] * scale, dy = nd[3 * i + 1] * scale, dz = nd[3 * i + 2] * scale;
         int x, y, z;
@@ -749,6 +820,7 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_accumulate_kernel(const CdmSe
 // ------------------------------------------------------------------ smooth
 // cdm_smooth (reg/cdm.hpp:302-366): cur_d = d*(1-s) + (s/6) * (d[+1] + d[-1] +
 // d[+w] + d[-w] + d[+wh] + d[-wh]) by flat index; s == 0 leaves cur_d as it is.
+// 2-D: s/4 and four neighbours (the +-wh taps of a d == 1 level fall outside).
 __global__ void __launch_bounds__(kCdmThreads) cdm_smooth_kernel(const CdmSeg* __restrict__ segs)
 {
     SEG_BEGIN
@@ -758,7 +830,7 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_smooth_kernel(const CdmSeg* _
     const float sm = c->cur_smoothing;
     if (sm == 0.0f)
         return;
-    const float w_6 = sm / (2.0f * 3.0f);
+    const float w_6 = sm / (2.0f * (S.ndim == 2 ? 2.0f : 3.0f));  // smoothing / (2 * dimension)
     const float w_1 = 1.0f - sm;
     const float* __restrict__ d = S.tmp_d;
     float* __restrict__ dd = S.cur_d;
@@ -871,11 +943,64 @@ __global__ void upsample_x2_kernel(const float* __restrict__ in, Dim3 di, float*
     }
 }
 
+// The 2-D form (vector<2> field of a d == 1 level): bilinear at (x, y) * 0.5; z is 0.
+__global__ void upsample_x2_2d_kernel(const float* __restrict__ in, Dim3 di, float* __restrict__ out, Dim3 dout)
+{
+    const long long n = dout.n();
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(o % dout.w), y = (int)(o / dout.w);
+        float vx = (float)x, vy = (float)y;
+        vx *= 0.5f;
+        vy *= 0.5f;
+        Cell2 c;
+        float2 v = make_float2(0.f, 0.f);
+        if (bilinear_cell(di, vx, vy, c)) {
+            const int w = di.w, b = c.base;
+            const int off[4] = {0, 1, w, w + 1};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const float* q = in + 3LL * (b + off[k]);
+                const float qx = q[0] * 2.0f, qy = q[1] * 2.0f;
+                if (k == 0) {
+                    v.x = qx * c.r[0];
+                    v.y = qy * c.r[0];
+                } else {
+                    v.x += qx * c.r[k];
+                    v.y += qy * c.r[k];
+                }
+            }
+        }
+        out[3 * o] = v.x;
+        out[3 * o + 1] = v.y;
+        out[3 * o + 2] = 0.0f;
+    }
+}
+
 cudaError_t launch_upsample_field_x2(const float* in, int iw, int ih, int id, float* out, int ow, int oh, int od,
-                                     cudaStream_t st)
+                                     cudaStream_t st, int ndim)
 {
     Dim3 di{iw, ih, id}, dout{ow, oh, od};
-    upsample_x2_kernel<<<cdm_blocks_for(dout.n()), kCdmThreads, 0, st>>>(in, di, out, dout);
+    if (ndim == 2)
+        upsample_x2_2d_kernel<<<cdm_blocks_for(dout.n()), kCdmThreads, 0, st>>>(in, di, out, dout);
+    else
+        upsample_x2_kernel<<<cdm_blocks_for(dout.n()), kCdmThreads, 0, st>>>(in, di, out, dout);
+    count_launch();
+    return cudaGetLastError();
+}
+
+__global__ void field_xy_kernel(const float* __restrict__ xyz, long long n, float* __restrict__ xy)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        xy[2 * i] = xyz[3 * i];
+        xy[2 * i + 1] = xyz[3 * i + 1];
+    }
+}
+
+cudaError_t launch_field_xy(const float* xyz, long long n, float* xy, cudaStream_t st)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    field_xy_kernel<<<cdm_blocks_for(n), kCdmThreads, 0, st>>>(xyz, n, xy);
     count_launch();
     return cudaGetLastError();
 }

@@ -31,8 +31,9 @@ struct CdmLevel {
     DevBuf<CdmSeg> d_seg;
     // It / Is: gtypes.size() modality pairs of one shape.  best is the level's in/out
     // field (starts as the upsampled coarser result).
+    // ndim 2: a level of a 2-D registration (d == 1).
     void init(const void* const* It, const void* const* Is, const std::string& gtypes, int w, int h, int d, int pix,
-              const regb_cdm_param& p, float* best, cudaStream_t st);
+              const regb_cdm_param& p, float* best, cudaStream_t st, int ndim = 3);
 };
 
 // One iteration of every segment in d_segs (reg/cdm.hpp:418-470); the segments

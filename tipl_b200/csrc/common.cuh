@@ -56,6 +56,31 @@ __device__ __forceinline__ bool trilinear_cell(const Dim3& D, float x, float y, 
     return true;
 }
 
+// Cell test and weights of interpolator::linear<2>::get_location
+// (numerical/interpolation.hpp:274-305): reject negative coordinates and cells
+// whose +1 neighbour leaves the image; weights n0*n1, p0*n1, n0*p1, p0*p1.
+struct Cell2 {
+    int base;
+    float r[4];
+};
+
+__device__ __forceinline__ bool bilinear_cell(const Dim3& D, float x, float y, Cell2& c)
+{
+    if (x < 0.0f || y < 0.0f)
+        return false;
+    if (!(x < (float)(D.w - 1)) || !(y < (float)(D.h - 1)))
+        return false;
+    const int ix = (int)x, iy = (int)y;
+    const float p0 = x - (float)ix, p1 = y - (float)iy;
+    const float n0 = 1.0f - p0, n1 = 1.0f - p1;
+    c.r[0] = n0 * n1;
+    c.r[1] = p0 * n1;
+    c.r[2] = n0 * p1;
+    c.r[3] = p0 * p1;
+    c.base = iy * D.w + ix;
+    return true;
+}
+
 template <typename T>
 __device__ __forceinline__ float ld_pix(const T* __restrict__ p, int i)
 {
@@ -75,6 +100,18 @@ __device__ __forceinline__ float cell_sum(const T* __restrict__ I, const Dim3& D
     acc += ld_pix(I, b + wh + 1) * c.r[5];
     acc += ld_pix(I, b + wh + w) * c.r[6];
     acc += ld_pix(I, b + wh + w + 1) * c.r[7];
+    return acc;
+}
+
+// weighted_sum over the 2-D cell (numerical/interpolation.hpp:61-73).
+template <typename T>
+__device__ __forceinline__ float cell_sum2(const T* __restrict__ I, const Dim3& D, const Cell2& c)
+{
+    const int w = D.w, b = c.base;
+    float acc = ld_pix(I, b) * c.r[0];
+    acc += ld_pix(I, b + 1) * c.r[1];
+    acc += ld_pix(I, b + w) * c.r[2];
+    acc += ld_pix(I, b + w + 1) * c.r[3];
     return acc;
 }
 

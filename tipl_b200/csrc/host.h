@@ -178,11 +178,13 @@ void runner_state_from_param(const int* fdim, const float* from_vs, const int* t
 // The CDM driver (reg/cdm.hpp:373-474) on device-resident images of nmod modality
 // pairs d_It[i] / d_Is[i] (one shape and pixel type); modality i uses gradient type
 // gtypes[i] ('r' / 'd'; 'r' past the string's end).  d_field receives the
-// full-resolution field.  Returns REGB_OK, REGB_FALSE or REGB_CANCELLED.
+// full-resolution field (xyz per voxel).  ndim 2: the images are 2-D (dim[2] == 1)
+// and the reference's dimension-2 instantiation is followed (the pyramid stops on
+// min(w, h); the field's z stays 0).  Returns REGB_OK, REGB_FALSE or REGB_CANCELLED.
 regb_status cdm_register_multi(const void* const* d_It, const void* const* d_Is, int nmod, const char* gtypes,
                                const int* dim, int pix, float* d_field, const regb_cdm_param& p,
                                volatile const int* terminated, cudaStream_t st, int* iterations = nullptr,
-                               CdmScheduler* sched = nullptr);
+                               CdmScheduler* sched = nullptr, int ndim = 3);
 // One modality pair with p.gradient_type.
 regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int pix, float* d_field,
                          const regb_cdm_param& p, volatile const int* terminated, cudaStream_t st,

@@ -77,6 +77,9 @@ struct CdmSeg {
     int nblk;         // blocks this segment uses (a function of its size only, so a
                       // job's reduction order does not depend on what it is batched with)
     int nmod;         // modality pairs (1 when 0)
+    int ndim;         // 2: a 2-D level (d == 1; tipl::image<2> and vector<2> math: bilinear
+                      // samples, the Poisson and smoothing weights of 4 neighbours; the
+                      // field's z stays 0); anything else: 3-D
     const void* It[kCdmMaxModalities];  // template (fixed) image of each modality at this level
     const void* Is[kCdmMaxModalities];  // subject (moving) image of each modality at this level
     void* Js;         // composed subject (scratch, pixel type)
@@ -132,7 +135,9 @@ cudaError_t launch_cdm_smooth(const CdmSeg* segs, int nseg, int blocks, cudaStre
 // Pyramid passes (single volume, device pointers).
 cudaError_t launch_downsample(const void* in, void* out, int w, int h, int d, int pix, cudaStream_t st);
 cudaError_t launch_upsample_field_x2(const float* in, int iw, int ih, int id, float* out, int ow, int oh, int od,
-                                     cudaStream_t st);
+                                     cudaStream_t st, int ndim = 3);
+// The x, y components of an xyz field (n voxels) as interleaved pairs (tipl::vector<2>).
+cudaError_t launch_field_xy(const float* xyz, long long n, float* xy, cudaStream_t st);
 // Sum of a segment's cost partials -> float mean (the reference's mean(cost_map)).
 cudaError_t launch_cost_mean(const CdmSeg* segs, int nseg, float* out, cudaStream_t st);
 int cdm_blocks_for(long long nvox);

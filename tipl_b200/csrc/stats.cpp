@@ -89,6 +89,14 @@ void KernelTimer::begin(cudaStream_t st, int k)
     cudaEventRecord(a, st);
 }
 
+void count_cdm_level(long long iterations, long long voxels, int pixel_bytes)
+{
+    std::lock_guard<std::mutex> g(g_m);
+    g_acc.cdm_iterations += iterations;
+    g_acc.cdm_voxel_iterations += (double)iterations * (double)voxels;
+    g_acc.cdm_model_bytes += (double)iterations * (double)voxels * (596.0 + 4.0 * pixel_bytes);
+}
+
 void KernelTimer::end(cudaStream_t st, long long tasks, double voxels, double bytes)
 {
     if (!on)
