@@ -230,8 +230,11 @@ def cdm_case(args):
     from tipl_b200 import phantom as ph
 
     t, m = ph.cdm_workload_pair(SHAPE)
-    It = torch.from_numpy(ph.normalize_to_u8(t)).cuda()
-    Is = torch.from_numpy(ph.normalize_to_u8(m)).cuda()
+    if args.pix == "f32":  # the float CDM (the serving workload's uint16 / float32 subjects)
+        It, Is = torch.from_numpy(t).cuda(), torch.from_numpy(m).cuda()
+    else:
+        It = torch.from_numpy(ph.normalize_to_u8(t)).cuda()
+        Is = torch.from_numpy(ph.normalize_to_u8(m)).cuda()
     p = tb.reg.cdm_param(min_dimension=32)
     field, ok = tb.reg.cdm(It, Is, p)  # warm-up
     L = _lib.lib()
@@ -244,9 +247,10 @@ def cdm_case(args):
     torch.cuda.synchronize()
     st = _lib.Stats()
     L.regb_stats_get(st)
-    line = {"kernel_case": "cdm", "ok": bool(ok), "ms": a.elapsed_time(b), "launches": st.launches,
+    line = {"kernel_case": "cdm", "pix": args.pix, "ok": bool(ok), "ms": a.elapsed_time(b), "launches": st.launches,
+            "iterations": st.cdm_iterations, "pass_model_gbs": st.cdm_model_bytes / (a.elapsed_time(b) / 1000.0) / 1e9,
             "field_rms": float(field.float().pow(2).sum(-1).sqrt().mean())}
-    if args.steps > 1:
+    if args.steps > 1 and args.pix == "u8":
         g = reference_gpu(It=It.cpu().numpy(), Is=Is.cpu().numpy(), min_dimension=np.int64(32))
         if g:
             line["reference_gpu_ms"] = 1000.0 * g["cdm_s"]
@@ -944,6 +948,7 @@ def main():
     ap.add_argument("--kernel-case", choices=["mi", "mi32", "corr", "cdm", "pre", "nifti"], default=None,
                     help="run only K-candidate cost batches of the full-size pair (for profiler captures)")
     ap.add_argument("--k", type=int, default=12)
+    ap.add_argument("--pix", choices=["u8", "f32"], default="u8", help="--kernel-case cdm: pixel type")
     ap.add_argument("--precision-report", action="store_true",
                     help="uint16 / BF16 storage: errors of the FP32 path against the FP64 oracle (config 4)")
     ap.add_argument("--ref-gpu-sample", default=None, help=argparse.SUPPRESS)

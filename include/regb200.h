@@ -94,6 +94,12 @@ const char* regb_last_error(void);   /* thread-local text of the last failure */
 regb_status regb_device_info(int* device, int* sm_count, size_t* free_bytes, size_t* total_bytes);
 /* Release every cached device buffer of this thread's context and every cached page-locked host block. */
 regb_status regb_release(void);
+/* Testing hook (no counterpart in the reference, which reports a failed CUDA call in
+ * cdm_cuda as `false`, reg/cdm.hpp:518-523): the next `count` device allocations of
+ * exactly `bytes` bytes made by this library fail as if the device were out of memory,
+ * so the call or engine job making them reports REGB_ERR_NOMEM; count 0 clears it.
+ * Lets a test fail one job of a running engine on the host, without touching the GPU. */
+regb_status regb_debug_fail_allocations(size_t bytes, int count);
 
 /* Launch accounting (no reference counterpart: instrumentation of this library).
  * launches counts every kernel this library launched since the last reset; with

@@ -223,3 +223,56 @@ def test_mm_reg_job_outputs_equal_plain_calls(orc):
     assert r["r_linear"] == r_lin and r["r_nonlinear"] == r_nl and r_nl > r_lin
     for got, want in ((out["f"], t2f), (out["rev"], f2t), (out["map"], to2from), (inv, from2to)):
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_failed_allocation_fails_only_its_job(data):
+    """Allocation failure injected on the host (regb_debug_fail_allocations fails the
+    next device allocation of one exact size): the job that makes it reports
+    REGB_ERR_NOMEM while the jobs running beside it give their alone results bit for
+    bit -- the reference's contract that a failed CUDA call ends only that call
+    (cdm_cuda returns false, reg/cdm.hpp:518-523).  Two places are hit: job B's affine
+    stage (the texture store of its moving volume, 44 x 46 rows of 40 halves at a pitch of
+    48, a size no other job allocates) while the others' probes share launches, and job D's
+    CDM stage (D registers to its own 36 x 40 x 38 fixed volume; the field of its second
+    pyramid level, 18 x 20 x 19 x 3 floats) after its coarsest level has iterated.  The
+    engine then runs the failed job again, unharmed."""
+    tmpl, movs = data
+    L = _lib.lib()
+    d_fixed = ph.normalize_to_u8(ph.class_phantom((38, 40, 36), np.random.default_rng(ph.seed_for(5, 9))))
+    jobs = [dict(mov=movs[0]), dict(mov=movs[2]), dict(mov=movs[3]), dict(mov=movs[1], fixed=d_fixed)]
+
+    def alone_job(j):
+        f = j.get("fixed", tmpl)
+        return alone(f, j["mov"], True)
+
+    ref = [alone_job(j) for j in jobs]
+    for target, size in ((1, 2 * 48 * 46 * 44), (3, 18 * 20 * 19 * 3 * 4)):
+        with tb.Engine(max_active=8) as eng:
+            tid = eng.add_template(tmpl)
+            fields = [np.zeros(j.get("fixed", tmpl).shape + (3,), np.float32) for j in jobs]
+            assert L.regb_debug_fail_allocations(size, 1) == 0
+            try:
+                ids = []
+                for j, f in zip(jobs, fields):
+                    if "fixed" in j:
+                        ids.append(eng.submit(j["mov"], fixed=j["fixed"], cdm=True, field_out=f))
+                    else:
+                        ids.append(eng.submit(j["mov"], template=tid, cdm=True, field_out=f))
+                res = [eng.wait(i) for i in ids]
+            finally:
+                L.regb_debug_fail_allocations(0, 0)
+            for k, (r, (cost, arg, evals, field), f) in enumerate(zip(res, ref, fields)):
+                if k == target:
+                    assert r["status"] == _lib.REGB_ERR_NOMEM
+                    continue
+                assert r["status"] == 0 and r["cdm_ok"]
+                assert np.float32(r["linear_cost"]) == np.float32(cost) and np.array_equal(r["arg"], arg)
+                assert np.array_equal(f.view(np.uint32), field.view(np.uint32))
+            # the failed job, run again on the same engine, gives its alone result
+            j = jobs[target]
+            f = np.zeros(j.get("fixed", tmpl).shape + (3,), np.float32)
+            if "fixed" in j:
+                r = eng.wait(eng.submit(j["mov"], fixed=j["fixed"], cdm=True, field_out=f))
+            else:
+                r = eng.wait(eng.submit(j["mov"], template=tid, cdm=True, field_out=f))
+            assert r["status"] == 0 and np.array_equal(f.view(np.uint32), ref[target][3].view(np.uint32))

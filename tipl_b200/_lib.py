@@ -149,6 +149,7 @@ _SIGS = {
     "regb_cdm_smooth": (C.c_int, [C.POINTER(Field), C.POINTER(Field), C.c_float, C.c_void_p]),
     "regb_cdm": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.POINTER(Field), C.POINTER(CdmParam),
                            C.c_void_p]),
+    "regb_debug_fail_allocations": (C.c_int, [C.c_size_t, C.c_int]),
     "regb_cdm_multi": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_int, C.POINTER(Field),
                                  C.POINTER(CdmParam), C.c_char_p, C.c_void_p]),
     "regb_cdm2d_multi": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_int, C.POINTER(Field),

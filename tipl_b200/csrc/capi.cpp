@@ -2,6 +2,7 @@
 // Every entry validates its views, stages host memory through device buffers when
 // a view lives on the host, and turns failures into regb_status codes.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -134,6 +135,20 @@ int pix_of(int dtype) { return dtype == REGB_F32 ? 1 : 0; }
 
 }  // namespace
 
+namespace regb {
+namespace {
+std::atomic<size_t> g_fail_bytes{0};
+std::atomic<int> g_fail_count{0};
+}  // namespace
+
+bool alloc_fault_injected(size_t bytes)
+{
+    if (g_fail_count.load(std::memory_order_relaxed) <= 0 || g_fail_bytes.load(std::memory_order_relaxed) != bytes)
+        return false;
+    return g_fail_count.fetch_sub(1) > 0;
+}
+}  // namespace regb
+
 extern "C" {
 
 void regb_linear_param_default(regb_linear_param* p)
@@ -176,6 +191,16 @@ regb_status regb_device_info(int* device, int* sm_count, size_t* free_bytes, siz
         if (total_bytes) *total_bytes = tot;
         return REGB_OK;
     });
+}
+
+regb_status regb_debug_fail_allocations(size_t bytes, int count)
+{
+    if (count < 0)
+        return REGB_ERR_ARG;
+    g_fail_count.store(0);
+    g_fail_bytes.store(bytes);
+    g_fail_count.store(count);
+    return REGB_OK;
 }
 
 regb_status regb_release(void)

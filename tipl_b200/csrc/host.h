@@ -37,6 +37,10 @@ void* pinned_get(size_t& bytes);
 void pinned_put(void* p, size_t bytes);
 void pinned_trim();
 
+// Allocation-failure injection (regb_debug_fail_allocations): true when this device
+// allocation of `bytes` bytes is one of those the hook was asked to fail.
+bool alloc_fault_injected(size_t bytes);
+
 // A device buffer from the stream-ordered pool (cudaMallocAsync); freed on the
 // same stream, so reuse is ordered without device-wide synchronisation.
 template <typename T>
@@ -68,6 +72,10 @@ struct DevBuf {
         st = s;
         n = count;
         if (count) {
+            if (alloc_fault_injected(count * sizeof(T))) {
+                n = 0;
+                throw Failure(REGB_ERR_NOMEM, "device allocation failed: injected by regb_debug_fail_allocations");
+            }
             cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), s);
             if (e != cudaSuccess) {
                 p = nullptr;
