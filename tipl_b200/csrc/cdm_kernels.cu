@@ -240,6 +240,26 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_gradient_kernel(const CdmSeg*
             const int xl = min(x, 2), yl = min(y, 2), zl = min(z, 2);
             const long long w = D.w, wh = D.wh();
             WindowAcc<T> acc;
+            // (float pixels only: the uint8 'r' gradient is the box-sum kernel below)
+            if (sizeof(T) == 4 && xu == 2 && xl == 2 && yu == 2 && yl == 2 && zu == 2 && zl == 2) {
+                // an interior voxel: the whole 5^3 window, visited in the same order
+                // with every offset known -- no loop bounds, no index arithmetic per tap
+                const T* __restrict__ pj = Js + i;
+                const T* __restrict__ pt = It + i;
+                constexpr int kOrd[5] = {0, 1, 2, -1, -2};
+#pragma unroll
+                for (int a = 0; a < 5; ++a) {
+#pragma unroll
+                    for (int b = 0; b < 5; ++b) {
+                        const long long row = kOrd[a] * wh + kOrd[b] * w;
+                        const T* __restrict__ rj = pj + row;
+                        const T* __restrict__ rt = pt + row;
+#pragma unroll
+                        for (int c = 0; c < 5; ++c)
+                            acc.add(rj[kOrd[c]], rt[kOrd[c]]);
+                    }
+                }
+            } else
             // iterate_xyz order (numerical/window.hpp:54-72)
             for (int pz = 0; pz < 2; ++pz) {
                 const int zc = pz ? zl : zu;
