@@ -748,7 +748,7 @@ def run_served(args, rank, world, dist):
     return t_dev, t_e2e, st, clocks, lat, costs, evals, estats, f8, subjects, plain, tuned
 
 
-def batch_result(args, n_subjects):
+def batch_result(args, n_subjects, plain_jobs=4):
     """A batch of --subjects registrations submitted at once: moving volumes of uneven
     shape (each dimension 96-256 voxels, isotropic voxel size U(0.8, 2.0) mm, uint16), each
     the 182x218x182 template phantom under its own random affine (resampled to its grid)
@@ -783,13 +783,15 @@ def batch_result(args, n_subjects):
         T = tb.affine_to_matrix(arg, SHAPE, VS, m.shape, vs)
         tb.reg.cdm(td, tb.resample(tb.widen_to_f32(m), SHAPE, T, allow_shift_copy=True), param=cdm_p)
 
-    plain(subjects[0], vss[0])  # warm-up
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for k in range(1, 5):
-        plain(subjects[k], vss[k])
-    torch.cuda.synchronize()
-    plain_rate = 4 / (time.perf_counter() - t0)
+    plain_rate = None
+    if plain_jobs:
+        plain(subjects[0], vss[0])  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(1, plain_jobs + 1):
+            plain(subjects[k], vss[k])
+        torch.cuda.synchronize()
+        plain_rate = plain_jobs / (time.perf_counter() - t0)
     with tb.Engine(hbm_budget_bytes=150 << 30, max_active=n_subjects) as eng:
         tid = eng.add_template(t)
         for k in range(2):  # warm-up
@@ -810,14 +812,15 @@ def batch_result(args, n_subjects):
             "ok": sum(int(r["status"] == 0 and r["cdm_ok"]) for r in res),
             "latency_ms": {"p50": pct(0.5), "p95": pct(0.95), "p99": pct(0.99)},
             "plain_sequential_registrations_per_s": plain_rate,
-            "batched_over_plain": (n_subjects / dt) / plain_rate,
+            "batched_over_plain": (n_subjects / dt) / plain_rate if plain_rate else None,
             "engine": {"affine_launches": est["affine_launches"], "affine_tasks": est["affine_tasks"],
-                       "cdm_rounds": est["cdm_rounds"]},
+                       "cdm_rounds": est["cdm_rounds"],
+                       "cdm_levels_per_round": est["cdm_round_segments"] / max(1, est["cdm_rounds"])},
             "data": "synthetic"}
 
 
 def batch_case(args):
-    print(json.dumps(batch_result(args, args.subjects)))
+    print(json.dumps(batch_result(args, args.subjects, args.batch_plain)))
     return 0
 
 
@@ -958,6 +961,8 @@ def main():
                     help="poisson: open-loop serving of affine+CDM jobs arriving as a Poisson stream; batch: "
                          "uneven-shape subjects submitted at once (affine + 3-level CDM)")
     ap.add_argument("--subjects", type=int, default=64, help="--workload batch: subjects in the batch")
+    ap.add_argument("--batch-plain", type=int, default=4,
+                    help="--workload batch: plain single-job registrations timed beside the batch (0 = none)")
     ap.add_argument("--rate", type=float, default=20.0, help="--workload poisson: arrivals per second")
     ap.add_argument("--duration", type=float, default=15.0, help="--workload poisson: seconds of arrivals")
     ap.add_argument("--max-active", type=int, default=32, help="--workload poisson: engine slots")

@@ -458,6 +458,8 @@ typedef struct {
     int queued, running;
     size_t used_bytes, budget_bytes;
     long long affine_launches, affine_tasks, cdm_rounds;
+    long long cdm_round_segments;  /* CDM levels summed over rounds: / cdm_rounds = the
+                                      levels that share one round's launches */
 } regb_engine_stats;
 
 void regb_engine_config_default(regb_engine_config* c);

@@ -201,6 +201,7 @@ public:
         s.affine_launches = batcher_.launches();
         s.affine_tasks = batcher_.tasks_evaluated();
         s.cdm_rounds = sched_.rounds();
+        s.cdm_round_segments = sched_.round_segments();
         return s;
     }
 

@@ -91,6 +91,7 @@ void CdmScheduler::loop()
             REGB_CK(cudaStreamSynchronize(st_));
             lk.lock();
             ++rounds_;
+            round_segments_ += n;
             for (int i = 0; i < n; ++i) {
                 Entry* e = cur[order[i]];
                 if (h_status_.p[i] || (e->term && *e->term)) {

@@ -23,6 +23,7 @@ public:
     // Iterates the level until its loop ends (or terminated is set); blocks the caller.
     void run(CdmLevel& lvl, volatile const int* terminated);
     long long rounds() const { return rounds_; }
+    long long round_segments() const { return round_segments_; }  // levels summed over rounds
 
 private:
     struct Entry {
@@ -37,6 +38,7 @@ private:
     bool stop_ = false;
     int iters_;
     long long rounds_ = 0;
+    long long round_segments_ = 0;
     cudaStream_t st_ = nullptr;
     DevBuf<CdmSeg> segs_;
     PinBuf<CdmSeg> h_segs_;
