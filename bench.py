@@ -696,7 +696,7 @@ def run_served(args, rank, world, dist):
     # the plain path's rate: registrations / total time, and from the median registration
     plain = {"mean_rate": len(plain_s) / sum(plain_s), "median_rate": 1.0 / float(np.median(plain_s)),
              "ms": sorted(round(1000.0 * t, 2) for t in plain_s)} if plain_s else None
-    tuned = tb.autotune()  # the cost kernels' block sizes for this device
+    tuned = tb.autotune_buckets("")  # the cost kernels' block sizes per grid-size bucket (cached on disk)
     eng = tb.Engine(max_active=max(args.batch, 1))
     tid = eng.add_template(torch.from_numpy(f8).cuda())
     lat, costs, evals = [], [], 0
@@ -776,6 +776,7 @@ def batch_result(args, n_subjects, plain_jobs=4):
         subjects.append(np.round(np.clip(ph.rician(m, rng), 0, 4095)).astype(np.uint16))
         vss.append((vs, vs, vs))
     cdm_p = tb.reg.cdm_param(min_dimension=32)
+    tb.autotune_buckets("")
 
     def plain(m, vs):
         q = tb.normalize_to_u8(m)[0]
@@ -851,6 +852,7 @@ def poisson_case(args):
         noisy = ph.rician(moved, rng)
         pool.append(np.round(np.clip(noisy, 0, 4095)).astype(np.uint16) if k % 2 == 0 else noisy.astype(np.float32))
     cdm_p = tb.reg.cdm_param()
+    tuned = tb.autotune_buckets("")
 
     def plain(t, m):
         q = lambda v: v if v.dtype == np.uint8 else tb.normalize_to_u8(v)[0]  # noqa: E731
@@ -929,6 +931,7 @@ def poisson_case(args):
                       "engine": {"affine_launches": est["affine_launches"], "affine_tasks": est["affine_tasks"],
                                  "cdm_rounds": est["cdm_rounds"]},
                       "plain_sequential_jobs_per_s": plain_rate,
+                      "autotuned_min_block_voxels": tuned["table"],
                       "template_shapes": [list(s) for s in tshapes], "data": "synthetic"}))
     return 0
 
@@ -1162,7 +1165,8 @@ def served_line(args, rank, world, dist, torch):
                            "plain_single_job_ms": plain["ms"] if plain else None,
                            "served_over_plain": (regs / t_dev / world) / plain["median_rate"] if plain else None,
                            "parallelism": f"replicas x{world}",
-                           "autotuned_min_block_voxels": tuned},
+                           "autotuned_min_block_voxels": tuned["table"],
+                           "autotune": {"seconds": tuned["seconds"], "from_cache": tuned["from_cache"]}},
                 "roofline": {"bound": "hbm",
                              "kernel": {"mi": "mi_kernel", "mi32": "mi32_kernel", "corr": "corr_kernel"}[args.cost],
                              "achieved": achieved, "peak": hbm,

@@ -125,15 +125,27 @@ regb_status regb_stats_reset(int timing);
 regb_status regb_stats_get(regb_stats* out);
 
 /* ---- launch-shape autotuner (no counterpart in the reference) ---------------------- */
-/* Times the batched affine cost kernels (correlation, MI, 32-bin MI) on a 182x218x182
- * pair with 12 candidate transforms for a few block sizes (minimum voxels per block) on
- * the current device, and keeps the fastest of each for the rest of the process.  The
- * choice only decides how voxels are split across blocks, so costs are identical under
- * every choice.  tuned (optional, indexed by regb_cost_type) receives the choices,
- * seconds (optional) the time the tuning took (about a second). */
+/* Times the batched affine cost kernels (correlation, MI, 32-bin MI) with 12 candidate
+ * transforms for a few block sizes (minimum voxels per block) on the current device, on
+ * one pair per size bucket (regb_autotune_buckets), and keeps the fastest of each for the
+ * rest of the process.  The choice only decides how voxels are split across blocks, so
+ * costs are identical under every choice.  tuned (optional, indexed by regb_cost_type)
+ * receives the choices for a 182x218x182 grid, seconds (optional) the time the tuning took. */
 regb_status regb_autotune(int tuned[3], double* seconds);
-/* The block sizes in use (the defaults until regb_autotune runs). */
+/* The block sizes in use for a 182x218x182 grid (the defaults until a tuner runs). */
 regb_status regb_tuning_get(int tuned[3]);
+/* The tuner per size bucket of the fixed grid: buckets 0..3 hold grids of up to
+ * 741,455 voxels, up to 3,890,000, up to 11,000,000, and more (around the 64^3, 128^3,
+ * 182x218x182 and 256^3 grids); each bucket is timed on a pair of its representative
+ * grid.  tuned (optional) receives the table, tuned[bucket * 3 + regb_cost_type].
+ * cache_path: NULL = no file; "" = the default file ($REGB_AUTOTUNE_CACHE, else
+ * $XDG_CACHE_HOME/tipl_b200/autotune.txt, else ~/.cache/tipl_b200/autotune.txt); a file
+ * that holds this device's table (keyed by device name and compute capability) is loaded
+ * instead of timing (*from_cache = 1), and a timed table is written to it.  regb_autotune
+ * is this call without a file. */
+regb_status regb_autotune_buckets(const char* cache_path, int tuned[12], double* seconds, int* from_cache);
+/* The block sizes in use, tuned[bucket * 3 + regb_cost_type]. */
+regb_status regb_tuning_get_buckets(int tuned[12]);
 
 /* ---- transform algebra (host) -------------------------------------------------- */
 /* transformation_matrix(affine_param, from, from_vs, to, to_vs)

@@ -35,7 +35,7 @@ from ._lib import CdmParam, Field, LinearParam, RegbError, Volume  # noqa: F401
 __all__ = ["affine_to_matrix", "affine_to_matrix_f64", "matrix_inverse", "resample", "mi_cost", "mi32_cost",
            "corr_cost", "nifti_info", "nifti_load", "nifti_save", "compose_displacement", "accumulate_displacement",
            "downsample", "upsample_field_x2", "cdm_gradient", "cdm_poisson", "cdm_max_length", "cdm_smooth", "reg",
-           "Engine", "RegbError", "version", "autotune", "tuning"]
+           "Engine", "RegbError", "version", "autotune", "tuning", "autotune_buckets", "tuning_buckets"]
 
 
 def version() -> str:
@@ -331,10 +331,33 @@ def autotune() -> dict:
 
 
 def tuning() -> dict:
-    """The block sizes in use (defaults until autotune runs)."""
+    """The block sizes in use for a 182x218x182 grid (defaults until autotune runs)."""
     tuned = np.zeros(3, np.int32)
     _lib.check(_lib.lib().regb_tuning_get(_fptr(tuned)))
     return {k: int(v) for k, v in zip(_COST_NAMES, tuned)}
+
+
+TUNE_BUCKETS = ("64^3", "128^3", "182x218x182", "256^3")
+
+
+def autotune_buckets(cache_path: str | None = "") -> dict:
+    """The autotuner per size bucket of the fixed grid (regb_autotune_buckets): returns
+    {bucket: {cost: minimum voxels per block}}, the seconds taken and whether the table
+    came from the cache file (cache_path None = no file, "" = the default file)."""
+    tuned = np.zeros(12, np.int32)
+    sec = C.c_double(0.0)
+    hit = C.c_int(0)
+    path = None if cache_path is None else str(cache_path).encode()
+    _lib.check(_lib.lib().regb_autotune_buckets(path, _fptr(tuned), C.byref(sec), C.byref(hit)))
+    table = {b: {k: int(tuned[3 * i + c]) for c, k in enumerate(_COST_NAMES)} for i, b in enumerate(TUNE_BUCKETS)}
+    return {"table": table, "seconds": sec.value, "from_cache": bool(hit.value)}
+
+
+def tuning_buckets() -> dict:
+    """The block sizes in use per size bucket."""
+    tuned = np.zeros(12, np.int32)
+    _lib.check(_lib.lib().regb_tuning_get_buckets(_fptr(tuned)))
+    return {b: {k: int(tuned[3 * i + c]) for c, k in enumerate(_COST_NAMES)} for i, b in enumerate(TUNE_BUCKETS)}
 
 
 # ---------------------------------------------------------------- NIfTI volumes (io/nifti.hpp)

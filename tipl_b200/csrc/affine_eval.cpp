@@ -6,7 +6,11 @@
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
+#include <cstdio>
+#include <sys/stat.h>
 #include <cstring>
+#include <string>
+#include <vector>
 
 namespace regb {
 
@@ -98,10 +102,21 @@ void TexVol::build(const uint8_t* v, Dim3 d, cudaStream_t st)
     }
 }
 
-// Minimum voxels per block of each cost kernel (index = cost type); the autotuner
-// replaces the defaults with the fastest measured choice.  Chunking only decides which
-// block counts which voxels, so every choice gives the same costs.
-static std::atomic<int> g_min_block_voxels[3] = {{32768}, {60000}, {60000}};
+// Minimum voxels per block of each cost kernel, per size bucket of the fixed grid
+// (index [bucket][cost type]); the autotuner replaces the defaults with the fastest
+// measured choice.  Chunking only decides which block counts which voxels, so every
+// choice gives the same costs.
+static std::atomic<int> g_min_block_voxels[kTuneBuckets][3] = {{{32768}, {60000}, {60000}},
+                                                                {{32768}, {60000}, {60000}},
+                                                                {{32768}, {60000}, {60000}},
+                                                                {{32768}, {60000}, {60000}}};
+
+int tune_bucket(long long voxels)
+{
+    // between the geometric means of the representative grids 64^3, 128^3,
+    // 182x218x182 and 256^3
+    return voxels <= 741455LL ? 0 : voxels <= 3890000LL ? 1 : voxels <= 11000000LL ? 2 : 3;
+}
 
 void check_mi_width(int fixed_width, const char* who)
 {
@@ -110,14 +125,14 @@ void check_mi_width(int fixed_width, const char* who)
                                                        "wide (16-bit per-block counters)");
 }
 
-int min_block_voxels(int cost_type) { return g_min_block_voxels[cost_type].load(); }
-void set_min_block_voxels(int cost_type, int v) { g_min_block_voxels[cost_type].store(v); }
+int min_block_voxels(int bucket, int cost_type) { return g_min_block_voxels[bucket][cost_type].load(); }
+void set_min_block_voxels(int bucket, int cost_type, int v) { g_min_block_voxels[bucket][cost_type].store(v); }
 
 void set_task_chunks(AffineTask& t, int cost_type)
 {
     // a chunk is a run of whole rows of the fixed grid
     const long long w = t.fd.w, rows = (long long)t.fd.h * t.fd.d;
-    const long long mv = g_min_block_voxels[cost_type].load();
+    const long long mv = g_min_block_voxels[tune_bucket(t.fd.n())][cost_type].load();
     long long rpc;
     if (cost_type == REGB_COST_MI) {
         // 16-bit per-block counters: at most 65535 voxels per block.  Blocks are made
@@ -137,70 +152,185 @@ void set_task_chunks(AffineTask& t, int cost_type)
     t.nchunk = (int)std::max<long long>(1, (rows + rpc - 1) / rpc);
 }
 
-double autotune_cost_kernels(cudaStream_t st, int* chosen)
+// Candidate minimum voxels per block, by cost type (MI: at most 65535, its 16-bit counters).
+static const int kTuneCand[3][5] = {{8192, 16384, 32768, 65536, 131072},  // correlation
+                                    {16384, 32768, 49152, 60000, 65535},  // MI
+                                    {8192, 16384, 32768, 60000, 131072}}; // MI32
+
+static bool tune_candidate(int cost_type, int v)
 {
-    const auto t_start = std::chrono::steady_clock::now();
-    // a 182 x 218 x 182 pair with smooth, many-valued content (the size of the affine
-    // workload's full-resolution level) and 12 small rigid candidates
-    const Dim3 d{182, 218, 182};
-    const size_t n = (size_t)d.n();
-    std::vector<uint8_t> hf(n), hm(n);
-    for (size_t i = 0; i < n; ++i) {
-        const int x = (int)(i % d.w), y = (int)((i / d.w) % d.h), z = (int)(i / d.wh());
-        hf[i] = (uint8_t)((x * 3 + y * 5 + z * 7) / 4 + ((x * y) >> 7));
-        hm[i] = (uint8_t)((x * 2 + y * 3 + z * 5) / 3 + ((y * z) >> 7));
+    for (int c : kTuneCand[cost_type])
+        if (c == v)
+            return true;
+    return false;
+}
+
+// The on-disk table: one line "<device name>|<bucket>|<cost type>|<voxels>" per choice.
+static std::string tune_key()
+{
+    int dev = 0;
+    cudaDeviceProp prop;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return "";
     }
-    DevBuf<uint8_t> f(n, st), m(n, st);
-    REGB_CK(cudaMemcpyAsync(f.p, hf.data(), n, cudaMemcpyHostToDevice, st));
-    REGB_CK(cudaMemcpyAsync(m.p, hm.data(), n, cudaMemcpyHostToDevice, st));
-    std::vector<float> T(12 * 12);
-    for (int k = 0; k < 12; ++k) {
-        const float a = 0.01f * (float)(k - 6), ca = std::cos(a), sa = std::sin(a);
-        const float R[9] = {ca, -sa, 0.0f, sa, ca, 0.0f, 0.0f, 0.0f, 1.0f};
-        const float c[3] = {d.w / 2.0f, d.h / 2.0f, d.d / 2.0f};
-        for (int r = 0; r < 3; ++r) {
-            float sh = c[r] + 0.3f * (float)(k % 3);
-            for (int j = 0; j < 3; ++j) {
-                T[12 * k + 3 * r + j] = R[3 * r + j];
-                sh -= R[3 * r + j] * c[j];
-            }
-            T[12 * k + 9 + r] = sh;
+    std::string k = prop.name;
+    for (char& c : k)
+        if (c == '|' || c == '\n')
+            c = ' ';
+    return k + " sm" + std::to_string(prop.major) + std::to_string(prop.minor);
+}
+
+static bool tune_load(const std::string& path, int* table)
+{
+    std::FILE* f = std::fopen(path.c_str(), "r");
+    if (!f)
+        return false;
+    const std::string key = tune_key();
+    int got = 0;
+    int tmp[kTuneBuckets * 3];
+    char line[512];
+    while (std::fgets(line, sizeof(line), f)) {
+        std::string l(line);
+        const size_t p1 = l.find('|');
+        if (p1 == std::string::npos || l.substr(0, p1) != key)
+            continue;
+        int b = -1, c = -1, v = 0;
+        if (std::sscanf(l.c_str() + p1 + 1, "%d|%d|%d", &b, &c, &v) == 3 && b >= 0 && b < kTuneBuckets && c >= 0 &&
+            c < 3 && tune_candidate(c, v)) {
+            tmp[b * 3 + c] = v;
+            got |= 1 << (b * 3 + c);
         }
     }
-    static const int cand[3][4] = {{16384, 32768, 65536, 131072},   // correlation
-                                   {32768, 49152, 60000, 65535},    // MI (16-bit counters)
-                                   {16384, 32768, 60000, 131072}};  // MI32
+    std::fclose(f);
+    if (got != (1 << (kTuneBuckets * 3)) - 1)
+        return false;  // not this device's complete table
+    std::memcpy(table, tmp, sizeof(tmp));
+    return true;
+}
+
+static void tune_store(const std::string& path, const int* table)
+{
+    // create the directories on the way (an existing one is fine)
+    for (size_t pos = path.find('/', 1); pos != std::string::npos; pos = path.find('/', pos + 1))
+        ::mkdir(path.substr(0, pos).c_str(), 0755);
+    // keep other devices' lines, replace this device's
+    const std::string key = tune_key();
+    std::vector<std::string> keep;
+    if (std::FILE* f = std::fopen(path.c_str(), "r")) {
+        char line[512];
+        while (std::fgets(line, sizeof(line), f)) {
+            std::string l(line);
+            if (l.compare(0, key.size() + 1, key + "|") != 0)
+                keep.push_back(l);
+        }
+        std::fclose(f);
+    }
+    const std::string tmp = path + ".tmp";
+    std::FILE* f = std::fopen(tmp.c_str(), "w");
+    if (!f)
+        return;  // an unwritable cache only costs the next process a tuning run
+    for (const auto& l : keep)
+        std::fputs(l.c_str(), f);
+    for (int b = 0; b < kTuneBuckets; ++b)
+        for (int c = 0; c < 3; ++c)
+            std::fprintf(f, "%s|%d|%d|%d\n", key.c_str(), b, c, table[b * 3 + c]);
+    std::fclose(f);
+    std::rename(tmp.c_str(), path.c_str());
+}
+
+std::string default_tune_cache()
+{
+    if (const char* e = std::getenv("REGB_AUTOTUNE_CACHE"))
+        return e;
+    if (const char* x = std::getenv("XDG_CACHE_HOME"))
+        return std::string(x) + "/tipl_b200/autotune.txt";
+    if (const char* h = std::getenv("HOME"))
+        return std::string(h) + "/.cache/tipl_b200/autotune.txt";
+    return "";
+}
+
+double autotune_cost_kernels(cudaStream_t st, int* chosen, const char* cache_path, int* from_cache)
+{
+    const auto t_start = std::chrono::steady_clock::now();
+    const std::string path = cache_path ? (cache_path[0] ? std::string(cache_path) : default_tune_cache()) : "";
+    int table[kTuneBuckets * 3];
+    if (from_cache)
+        *from_cache = 0;
+    if (!path.empty() && tune_load(path, table)) {
+        for (int b = 0; b < kTuneBuckets; ++b)
+            for (int c = 0; c < 3; ++c)
+                g_min_block_voxels[b][c].store(table[b * 3 + c]);
+        if (chosen)
+            std::memcpy(chosen, table, sizeof(table));
+        if (from_cache)
+            *from_cache = 1;
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    }
+    // one smooth, many-valued pair per bucket, of the bucket's representative grid, and
+    // 12 small rigid candidates (an optimiser's probe set)
+    static const Dim3 kRep[kTuneBuckets] = {{64, 64, 64}, {128, 128, 128}, {182, 218, 182}, {256, 256, 256}};
     cudaEvent_t a, b;
     REGB_CK(cudaEventCreate(&a));
     REGB_CK(cudaEventCreate(&b));
-    for (int ct = 0; ct < 3; ++ct) {
-        AffineEvaluator ev({AffineEvaluator::Pair{f.p, d, m.p, d}}, ct, st);
-        int best = g_min_block_voxels[ct].load();
-        float best_ms = 1e30f;
-        for (int v : cand[ct]) {
-            g_min_block_voxels[ct].store(v);
-            ev.eval(0, T.data(), 12);  // warm-up
-            float ms_min = 1e30f;
-            for (int rep = 0; rep < 3; ++rep) {
-                REGB_CK(cudaEventRecord(a, st));
-                ev.eval(0, T.data(), 12);
-                REGB_CK(cudaEventRecord(b, st));
-                REGB_CK(cudaEventSynchronize(b));
-                float ms = 0.0f;
-                REGB_CK(cudaEventElapsedTime(&ms, a, b));
-                ms_min = std::min(ms_min, ms);
-            }
-            if (ms_min < best_ms) {
-                best_ms = ms_min;
-                best = v;
+    for (int bk = 0; bk < kTuneBuckets; ++bk) {
+        const Dim3 d = kRep[bk];
+        const size_t n = (size_t)d.n();
+        std::vector<uint8_t> hf(n), hm(n);
+        for (size_t i = 0; i < n; ++i) {
+            const int x = (int)(i % d.w), y = (int)((i / d.w) % d.h), z = (int)(i / d.wh());
+            hf[i] = (uint8_t)((x * 3 + y * 5 + z * 7) / 4 + ((x * y) >> 7));
+            hm[i] = (uint8_t)((x * 2 + y * 3 + z * 5) / 3 + ((y * z) >> 7));
+        }
+        DevBuf<uint8_t> f(n, st), m(n, st);
+        REGB_CK(cudaMemcpyAsync(f.p, hf.data(), n, cudaMemcpyHostToDevice, st));
+        REGB_CK(cudaMemcpyAsync(m.p, hm.data(), n, cudaMemcpyHostToDevice, st));
+        std::vector<float> T(12 * 12);
+        for (int k = 0; k < 12; ++k) {
+            const float ang = 0.01f * (float)(k - 6), ca = std::cos(ang), sa = std::sin(ang);
+            const float R[9] = {ca, -sa, 0.0f, sa, ca, 0.0f, 0.0f, 0.0f, 1.0f};
+            const float c[3] = {d.w / 2.0f, d.h / 2.0f, d.d / 2.0f};
+            for (int r = 0; r < 3; ++r) {
+                float sh = c[r] + 0.3f * (float)(k % 3);
+                for (int j = 0; j < 3; ++j) {
+                    T[12 * k + 3 * r + j] = R[3 * r + j];
+                    sh -= R[3 * r + j] * c[j];
+                }
+                T[12 * k + 9 + r] = sh;
             }
         }
-        g_min_block_voxels[ct].store(best);
-        if (chosen)
-            chosen[ct] = best;
+        for (int ct = 0; ct < 3; ++ct) {
+            AffineEvaluator ev({AffineEvaluator::Pair{f.p, d, m.p, d}}, ct, st);
+            int best = g_min_block_voxels[bk][ct].load();
+            float best_ms = 1e30f;
+            for (int v : kTuneCand[ct]) {
+                g_min_block_voxels[bk][ct].store(v);
+                ev.eval(0, T.data(), 12);  // warm-up
+                float ms_min = 1e30f;
+                for (int rep = 0; rep < 3; ++rep) {
+                    REGB_CK(cudaEventRecord(a, st));
+                    ev.eval(0, T.data(), 12);
+                    REGB_CK(cudaEventRecord(b, st));
+                    REGB_CK(cudaEventSynchronize(b));
+                    float ms = 0.0f;
+                    REGB_CK(cudaEventElapsedTime(&ms, a, b));
+                    ms_min = std::min(ms_min, ms);
+                }
+                if (ms_min < best_ms) {
+                    best_ms = ms_min;
+                    best = v;
+                }
+            }
+            g_min_block_voxels[bk][ct].store(best);
+            table[bk * 3 + ct] = best;
+        }
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    if (chosen)
+        std::memcpy(chosen, table, sizeof(table));
+    if (!path.empty())
+        tune_store(path, table);
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
 }
 

@@ -2,6 +2,7 @@
 // pyramid level) in a single launch.  Also the task-level entry used by the
 // serving engine to put candidates of many jobs into one launch.
 #pragma once
+#include <string>
 #include <vector>
 #include "host.h"
 
@@ -65,13 +66,20 @@ void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, dou
 
 // Chunking of one task over its fixed-grid voxels.
 void set_task_chunks(AffineTask& t, int cost_type);
-// The chunking parameter per cost type (minimum voxels per block) and its autotuner:
-// times each cost kernel on a 182x218x182 pair with 12 candidates for a few block sizes
-// on the current device, keeps the fastest (results do not depend on the choice), writes
-// the choices to chosen[3] (optional) and returns the seconds it took.
-int min_block_voxels(int cost_type);
-void set_min_block_voxels(int cost_type, int v);
-double autotune_cost_kernels(cudaStream_t st, int* chosen);
+// The chunking parameter (minimum voxels per block) per size bucket of the fixed grid
+// and cost type, and its autotuner: for each bucket it times each cost kernel on a pair
+// of the bucket's representative grid (64^3, 128^3, 182x218x182, 256^3) with 12
+// candidates for a few block sizes on the current device and keeps the fastest
+// (results do not depend on the choice).  chosen (optional) receives the table
+// [bucket * 3 + cost type]; cache_path names a table file (NULL: none, "": the default
+// file), which is read instead of timing when it holds this device's table and written
+// after timing; from_cache (optional) tells which happened.  Returns the seconds taken.
+constexpr int kTuneBuckets = 4;
+int tune_bucket(long long voxels);
+int min_block_voxels(int bucket, int cost_type);
+void set_min_block_voxels(int bucket, int cost_type, int v);
+std::string default_tune_cache();
+double autotune_cost_kernels(cudaStream_t st, int* chosen, const char* cache_path, int* from_cache);
 
 class AffineEvaluator {
 public:

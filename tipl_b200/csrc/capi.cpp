@@ -217,12 +217,12 @@ regb_status regb_release(void)
     });
 }
 
-regb_status regb_autotune(int tuned[3], double* seconds)
+regb_status regb_autotune_buckets(const char* cache_path, int tuned[12], double* seconds, int* from_cache)
 {
     return guarded([&] {
         Stream s;
-        int chosen[3] = {0, 0, 0};
-        const double dt = autotune_cost_kernels(s.s, chosen);
+        int chosen[kTuneBuckets * 3] = {0};
+        const double dt = autotune_cost_kernels(s.s, chosen, cache_path, from_cache);
         s.sync();
         if (tuned)
             std::memcpy(tuned, chosen, sizeof(chosen));
@@ -232,12 +232,31 @@ regb_status regb_autotune(int tuned[3], double* seconds)
     });
 }
 
+regb_status regb_autotune(int tuned[3], double* seconds)
+{
+    int table[kTuneBuckets * 3];
+    const regb_status st = regb_autotune_buckets(nullptr, table, seconds, nullptr);
+    if (st == REGB_OK && tuned)
+        std::memcpy(tuned, table + 3 * tune_bucket(182LL * 218 * 182), 3 * sizeof(int));
+    return st;
+}
+
+regb_status regb_tuning_get_buckets(int tuned[12])
+{
+    if (!tuned)
+        return REGB_ERR_ARG;
+    for (int b = 0; b < kTuneBuckets; ++b)
+        for (int c = 0; c < 3; ++c)
+            tuned[b * 3 + c] = min_block_voxels(b, c);
+    return REGB_OK;
+}
+
 regb_status regb_tuning_get(int tuned[3])
 {
     if (!tuned)
         return REGB_ERR_ARG;
     for (int c = 0; c < 3; ++c)
-        tuned[c] = min_block_voxels(c);
+        tuned[c] = min_block_voxels(tune_bucket(182LL * 218 * 182), c);
     return REGB_OK;
 }
 
