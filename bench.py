@@ -697,7 +697,7 @@ def run_served(args, rank, world, dist):
     plain = {"mean_rate": len(plain_s) / sum(plain_s), "median_rate": 1.0 / float(np.median(plain_s)),
              "ms": sorted(round(1000.0 * t, 2) for t in plain_s)} if plain_s else None
     tuned = tb.autotune_buckets("")  # the cost kernels' block sizes per grid-size bucket (cached on disk)
-    eng = tb.Engine(max_active=max(args.batch, 1))
+    eng = tb.Engine(max_active=max(args.batch, 1), gather_us=args.gather_us)
     tid = eng.add_template(torch.from_numpy(f8).cuda())
     lat, costs, evals = [], [], 0
 
@@ -969,6 +969,8 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="--workload poisson: arrivals per second")
     ap.add_argument("--duration", type=float, default=15.0, help="--workload poisson: seconds of arrivals")
     ap.add_argument("--max-active", type=int, default=32, help="--workload poisson: engine slots")
+    ap.add_argument("--gather-us", type=int, default=30,
+                    help="served mode: how long a cost batch waits for more jobs once the device is free")
     args = ap.parse_args()
     # the affine cost: MI (the reference's linear() default) for the affine workloads,
     # correlation (the mm_reg class's default, reg/mm_reg.hpp:53) for the mm_reg pipeline
