@@ -450,6 +450,13 @@ typedef struct {
     float* field_rev_out;      /* optional: the reverse displacement (template dims x 3 floats) */
     float* mapping_out;        /* optional: template grid -> subject voxel mapping (template dims x 3) */
     float* inv_mapping_out;    /* optional: subject grid -> template voxel mapping (moving dims x 3) */
+    const float* prev_field;   /* mm_reg, optional, with prev_field_rev: the forward and reverse */
+    const float* prev_field_rev; /* fields of an earlier registration of this pair (template dims
+                                  x 3 floats, at field_location).  The new fields are accumulated
+                                  onto them (accumulate_displacement(previous_t2f, t2f_dis) and
+                                  (previous_f2t, f2t_dis), reg/mm_reg.hpp:408-412) before the
+                                  mappings and the nonlinear r; field_out / field_rev_out receive
+                                  the accumulated fields */
 } regb_job;
 
 typedef struct {

@@ -233,12 +233,12 @@ int orc_nifti_load(const char* path, int vol, float* out, long long cap, int* di
         case 64: v = (float)orc_f64(p, sw); break;
         case 1024: v = (float)orc_i64(p, sw); break;
         case 1280: v = (float)(uint64_t)orc_i64(p, sw); break;
-        default:
-            free(I);
-            if (data != f)
-                free(data);
-            free(f);
-            return 0;
+        case 128: /* tipl::rgb(r, g, b) as uint32: b low byte, alpha 0 (io/nifti.hpp:1113-1115) */
+            v = (float)(((uint32_t)p[0] << 16) | ((uint32_t)p[1] << 8) | (uint32_t)p[2]);
+            break;
+        default: /* no conversion in the reference's float read: the voxel stays 0 */
+            v = 0.0f;
+            break;
         }
         if (slope != 0.0f) {
             if (slope != 1.0f)

@@ -222,7 +222,7 @@ def nifti_bytes(data, datatype, bitpix, srow=None, pixdim=(1.0, 1.0, 1.0), qform
     import struct
 
     e = ">" if big else "<"
-    z, y, x = data.shape
+    z, y, x = data.shape[:3]  # an RGB array carries its 3 channels last
     dims = [3 + len(extra_dims), x, y, z] + list(extra_dims)
     dims += [1] * (8 - len(dims))
     pix = [1.0, *pixdim, 1.0, 1.0, 1.0, 1.0]
@@ -295,6 +295,9 @@ def nifti_cases():
          dict(srow=ras, extra_dims=(2,))),
         ("f32_mni", rng.random(sh).astype(np.float32), 16, 32,
          dict(srow=[-1.0, 0, 0, 90.0, 0, -1.0, 0, 126.0, 0, 0, 1.0, -72.0], sform_code=4)),
+        ("rgb_ras", rng.integers(0, 256, sh + (3,)).astype(np.uint8), 128, 24, dict(srow=ras)),
+        ("complex64_be_scaled", (rng.normal(0, 10, sh) + 1j * rng.normal(0, 10, sh)).astype(np.complex64), 32, 64,
+         dict(srow=lps, big=True, slope=2.0, inter=1.5)),
     ]
 
 

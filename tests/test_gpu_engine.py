@@ -225,6 +225,43 @@ def test_mm_reg_job_outputs_equal_plain_calls(orc):
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
+def test_mm_reg_job_continues_previous_fields():
+    """mm_reg with previous_t2f / previous_f2t (reg/mm_reg.hpp:408-412): the new forward
+    and reverse fields are accumulated onto the given ones before the mappings and the
+    nonlinear r; every output equals the plain calls (accumulate_displacement, then the
+    mappings) bit for bit."""
+    rng = np.random.default_rng(ph.seed_for(5, 11))
+    t = ph.class_phantom((36, 40, 34), rng)
+    s = (32, 44, 30)
+    T0 = ph.affine_matrix_f32(ph.random_affine(rng, rot_deg=6, trans_vox=2), s, (1, 1, 1), s, (1, 1, 1))
+    m = ph.rician(ph.apply_matrix(ph.class_phantom(s, rng), T0, s), rng)
+    prev = ph.smooth_field(t.shape, rng, 5.0, 1.5)
+    prev_rev = ph.smooth_field(t.shape, rng, 5.0, 1.5)
+    q_t, _ = tb.normalize_to_u8(t)
+    q_m = tb.subject_image_pre(m)
+    _, arg, _ = tb.reg.linear(q_t, (1, 1, 1), q_m, (1, 1, 1), param=tb.reg.linear_param(cost_type=tb.reg.CORR))
+    T = tb.affine_to_matrix(arg, t.shape, (1, 1, 1), m.shape, (1, 1, 1))
+    J = tb.resample(q_m, t.shape, T, allow_shift_copy=True)
+    It2 = tb.match_fov(q_t, T, m.shape)
+    t2f = tb.accumulate_displacement(prev, tb.reg.cdm(It2, J)[0])
+    f2t = tb.accumulate_displacement(prev_rev, tb.reg.cdm(J, It2)[0])
+    to2from = tb.displacement_to_mapping(t2f, T)
+    from2to = tb.inv_displacement_to_mapping(f2t, T, m.shape)
+    r_nl = tb.correlation(tb.compose_mapping(q_m, to2from), It2, masked=True)
+    out = {k: np.zeros(t.shape + (3,), np.float32) for k in ("f", "rev", "map")}
+    inv = np.zeros(m.shape + (3,), np.float32)
+    with tb.Engine() as eng:
+        tid = eng.add_template(t)
+        r = eng.wait(eng.submit(m, template=tid, cdm=True, subject_pre=True, mm_reg=True, field_out=out["f"],
+                                field_rev_out=out["rev"], mapping_out=out["map"], inv_mapping_out=inv,
+                                prev_field=prev, prev_field_rev=prev_rev))
+        with pytest.raises(_lib.RegbError):  # the pair goes together, with mm_reg
+            eng.submit(m, template=tid, cdm=True, prev_field=prev, prev_field_rev=prev_rev)
+    assert r["status"] == 0 and r["r_nonlinear"] == r_nl
+    for got, want in ((out["f"], t2f), (out["rev"], f2t), (out["map"], to2from), (inv, from2to)):
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
 def test_failed_allocation_fails_only_its_job(data):
     """Allocation failure injected on the host (regb_debug_fail_allocations fails the
     next device allocation of one exact size): the job that makes it reports

@@ -1,7 +1,8 @@
 """NIfTI volumes (io/nifti.hpp): the library's reader and writer against the
 reference's gz_nifti.
 
-Fixtures: tests/golden/nifti/ holds files of every datatype the reader takes, both
+Fixtures: tests/golden/nifti/ holds files of every datatype the reader takes (RGB as the
+reference's packed colour, complex left at 0 like the reference's float read), both
 byte orders, NIfTI-1 and -2, .nii / .nii.gz / .hdr+.img, sform and qform-only
 geometry, orientations that need flips and each kind of axis swap, scl_slope /
 scl_inter, a 4-D file and an MNI-space header; tests/golden/nifti.npz holds what the
@@ -183,8 +184,10 @@ def test_full_size_volume(orc, tmp_path):
 
 
 def test_reader_rejects_truncated_and_unsupported(tmp_path):
-    """A file shorter than its header says, and an RGB file, fail with an error before
-    any device work (so this runs without a GPU)."""
+    """A file shorter than its header says, a zero bitpix (the reference's own error,
+    io/nifti.hpp:1052-1057) and a converted datatype whose bitpix does not match its
+    element size fail with an error before any device work (so this runs without a
+    GPU)."""
     sys.path.insert(0, GOLDEN)
     from make_golden import nifti_bytes
 
@@ -195,7 +198,8 @@ def test_reader_rejects_truncated_and_unsupported(tmp_path):
     assert tb.nifti_info(str(short))["dim"] == (7, 6, 5)  # the header itself is fine
     with pytest.raises(tb.RegbError):
         tb.nifti_load(str(short))
-    rgb, _ = nifti_bytes(np.zeros((5, 6, 21), np.uint8), 128, 24)
-    (tmp_path / "rgb.nii").write_bytes(rgb)
-    with pytest.raises(tb.RegbError):
-        tb.nifti_load(str(tmp_path / "rgb.nii"))
+    for dt, bp in ((64, 0), (4, 8)):
+        bad, _ = nifti_bytes(np.zeros((5, 6, 7), np.uint8), dt, bp)
+        (tmp_path / "bad.nii").write_bytes(bad)
+        with pytest.raises(tb.RegbError):
+            tb.nifti_load(str(tmp_path / "bad.nii"))

@@ -589,7 +589,8 @@ class Engine:
     def submit(self, moving, moving_vs=(1.0, 1.0, 1.0), template=None, fixed=None, fixed_vs=(1.0, 1.0, 1.0),
                linear=True, linear_param: LinearParam | None = None, arg=None, cdm=False,
                cdm_param: CdmParam | None = None, field_out=None, subject_pre=False, mm_reg=False,
-               field_rev_out=None, mapping_out=None, inv_mapping_out=None) -> int:
+               field_rev_out=None, mapping_out=None, inv_mapping_out=None, prev_field=None,
+               prev_field_rev=None) -> int:
         L = _lib.lib()
         j = _lib.Job()
         L.regb_job_default(C.byref(j))
@@ -632,6 +633,13 @@ class Engine:
                 setattr(j, name, buf.data_ptr() if _is_dev(buf) else buf.ctypes.data)
                 if field_out is None:
                     j.field_location = _lib.DEVICE if _is_dev(buf) else _lib.HOST
+                keep.append(buf)
+        if prev_field is not None and prev_field_rev is not None:
+            # an earlier registration's fields, at field_out's location (mm_reg's previous_t2f / f2t)
+            for name, buf in (("prev_field", prev_field), ("prev_field_rev", prev_field_rev)):
+                if not _is_dev(buf):
+                    buf = np.ascontiguousarray(buf, np.float32)
+                setattr(j, name, buf.data_ptr() if _is_dev(buf) else buf.ctypes.data)
                 keep.append(buf)
         jid = C.c_uint64(0)
         _lib.check(L.regb_engine_submit(self._h, C.byref(j), C.byref(jid)))

@@ -74,7 +74,8 @@ class Job(C.Structure):
                 ("moving_vs", C.c_float * 3), ("run_linear", C.c_int), ("linear", LinearParam),
                 ("arg", C.c_float * 12), ("run_cdm", C.c_int), ("cdm", CdmParam), ("field_out", C.c_void_p),
                 ("field_location", C.c_int), ("subject_pre", C.c_int), ("mm_reg", C.c_int),
-                ("field_rev_out", C.c_void_p), ("mapping_out", C.c_void_p), ("inv_mapping_out", C.c_void_p)]
+                ("field_rev_out", C.c_void_p), ("mapping_out", C.c_void_p), ("inv_mapping_out", C.c_void_p),
+                ("prev_field", C.c_void_p), ("prev_field_rev", C.c_void_p)]
 
 
 class Result(C.Structure):

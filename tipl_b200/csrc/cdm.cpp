@@ -128,6 +128,33 @@ void launch_iteration(const CdmSeg* d_segs, int nseg, int blocks, int pix, const
     REGB_CK(launch_cdm_smooth(d_segs, nseg, blocks, st));
 }
 
+void accumulate_displacement_device(const float* dis, float* new_dis, const int* dim, cudaStream_t st)
+{
+    // the accumulate pass of a CDM iteration with speed / theta = 1 (an exact scaling)
+    const long long n = (long long)dim[0] * dim[1] * dim[2];
+    CdmSeg seg{};
+    seg.w = dim[0];
+    seg.h = dim[1];
+    seg.d = dim[2];
+    seg.nblk = cdm_blocks_for(n);
+    CdmCtl c;
+    std::memset(&c, 0, sizeof(c));
+    c.scale = 1.0f;
+    c.max_iter = 200;
+    DevBuf<float> out(3 * n, st);
+    DevBuf<CdmCtl> ctl(1, st);
+    DevBuf<CdmSeg> d_seg(1, st);
+    seg.cur_d = const_cast<float*>(dis);
+    seg.aux_d = new_dis;
+    seg.tmp_d = out.p;
+    seg.ctl = ctl.p;
+    REGB_CK(cudaMemcpyAsync(ctl.p, &c, sizeof(c), cudaMemcpyHostToDevice, st));
+    REGB_CK(cudaMemcpyAsync(d_seg.p, &seg, sizeof(seg), cudaMemcpyHostToDevice, st));
+    REGB_CK(launch_cdm_accumulate(d_seg.p, 1, seg.nblk, st));
+    REGB_CK(cudaMemcpyAsync(new_dis, out.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, st));
+    REGB_CK(cudaStreamSynchronize(st));  // c and seg are stack-staged
+}
+
 regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int pix, float* d_field,
                          const regb_cdm_param& p, volatile const int* terminated, cudaStream_t st, int* iterations,
                          CdmScheduler* sched)

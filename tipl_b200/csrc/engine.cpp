@@ -484,6 +484,18 @@ private:
                 r.status = REGB_CANCELLED;
             const cudaMemcpyKind kind =
                 s.field_location == REGB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+            if (mm && r.status != REGB_CANCELLED && s.prev_field && s.prev_field_rev) {
+                // continue an earlier registration (reg/mm_reg.hpp:408-412): the new
+                // fields are accumulated onto the previous ones
+                const cudaMemcpyKind in_kind =
+                    s.field_location == REGB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+                DevBuf<float> prev(3 * nf, st.s), prev_rev(3 * nf, st.s);
+                REGB_CK(cudaMemcpyAsync(prev.p, s.prev_field, sizeof(float) * 3 * nf, in_kind, st.s));
+                REGB_CK(cudaMemcpyAsync(prev_rev.p, s.prev_field_rev, sizeof(float) * 3 * nf, in_kind, st.s));
+                accumulate_displacement_device(prev.p, field.p, fdim, st.s);
+                accumulate_displacement_device(prev_rev.p, field_rev.p, fdim, st.s);
+                count_launch(2);
+            }
             if (s.field_out && cs != REGB_FALSE)
                 REGB_CK(cudaMemcpyAsync(s.field_out, field.p, sizeof(float) * 3 * nf, kind, st.s));
             if (mm && r.status != REGB_CANCELLED) {
@@ -633,6 +645,8 @@ regb_status regb_engine_submit(regb_engine* e, const regb_job* job, uint64_t* id
             throw Failure(REGB_ERR_ARG, "bad fixed/moving volume");
         if (job->mm_reg && !job->run_cdm)
             throw Failure(REGB_ERR_ARG, "mm_reg needs run_cdm");
+        if ((job->prev_field || job->prev_field_rev) && !(job->mm_reg && job->prev_field && job->prev_field_rev))
+            throw Failure(REGB_ERR_ARG, "prev_field and prev_field_rev go together, with mm_reg");
         const int ct = job->linear.cost_type;
         if (job->run_linear && ct != REGB_COST_CORR && ct != REGB_COST_MI && ct != REGB_COST_MI32)
             throw Failure(REGB_ERR_ARG, "cost_type must be MI, MI32 or CORR");

@@ -193,6 +193,9 @@ regb_status cdm_register_multi(const void* const* d_It, const void* const* d_Is,
                                const int* dim, int pix, float* d_field, const regb_cdm_param& p,
                                volatile const int* terminated, cudaStream_t st, int* iterations = nullptr,
                                CdmScheduler* sched = nullptr, int ndim = 3);
+// accumulate_displacement(dis, new_dis) (numerical/dif.hpp:166-186) on device fields of
+// one shape: new_dis <- dis composed with new_dis.
+void accumulate_displacement_device(const float* dis, float* new_dis, const int* dim, cudaStream_t st);
 // One modality pair with p.gradient_type.
 regb_status cdm_register(const void* d_It, const void* d_Is, const int* dim, int pix, float* d_field,
                          const regb_cdm_param& p, volatile const int* terminated, cudaStream_t st,

@@ -163,15 +163,21 @@ std::string img_path(const std::string& path)
 
 }  // namespace
 
-int nifti_bytes_per_voxel(int datatype)
+int nifti_bytes_per_voxel(int datatype, int bitpix)
 {
+    // the datatypes the reference's float read converts (io/nifti.hpp:1096-1131) keep
+    // their element size; every other code is read as bitpix / 8 bytes and left at 0
+    // (that read has no conversion for them: complex, float128, RGBA32, ...)
+    int size = 0;
     switch (datatype) {
-    case 2: case 256: return 1;
-    case 4: case 512: return 2;
-    case 8: case 16: case 768: return 4;
-    case 64: case 1024: case 1280: return 8;
-    default: return 0;
+    case 2: case 256: size = 1; break;
+    case 4: case 512: size = 2; break;
+    case 128: size = 3; break;  // RGB: r, g, b bytes
+    case 8: case 16: case 768: size = 4; break;
+    case 64: case 1024: case 1280: size = 8; break;
+    default: return bitpix >= 8 ? bitpix / 8 : 0;
     }
+    return bitpix == 8 * size ? size : 0;
 }
 
 NiftiFile nifti_open(const std::string& path)
@@ -250,8 +256,8 @@ NiftiFile nifti_open(const std::string& path)
 
 std::vector<uint8_t> nifti_read_voxels(const std::string& path, const NiftiFile& f, int vol)
 {
-    const int bpv = nifti_bytes_per_voxel(f.h.datatype);
-    if (bpv == 0 || f.h.bitpix != 8 * bpv)
+    const int bpv = nifti_bytes_per_voxel(f.h.datatype, f.h.bitpix);
+    if (bpv == 0)
         throw Failure(REGB_ERR_ARG, "unsupported NIfTI datatype " + std::to_string(f.h.datatype) + " / bitpix " +
                                         std::to_string(f.h.bitpix));
     const long long n = (long long)f.file_dim[1] * f.file_dim[2] * f.file_dim[3];

@@ -42,7 +42,7 @@ struct NiftiFile {
 NiftiFile nifti_open(const std::string& path);
 // Bytes of volume `vol` (the first three dims) exactly as stored; throws Failure.
 std::vector<uint8_t> nifti_read_voxels(const std::string& path, const NiftiFile& f, int vol);
-int nifti_bytes_per_voxel(int datatype);
+int nifti_bytes_per_voxel(int datatype, int bitpix);
 // Writes a NIfTI-1 file the way the reference's writer does (io/nifti.hpp:969-1020,
 // io/gz_stream.hpp:535-580): the 348-byte header, four zero bytes and the voxels, not
 // reoriented, through a gzip stream whatever the file name's extension.

@@ -60,7 +60,13 @@ __device__ __forceinline__ float element(const uint8_t* __restrict__ raw, long l
         unsigned long long v = reinterpret_cast<const unsigned long long*>(raw)[i];
         return __ull2float_rn(be ? bswap64(v) : v);
     }
-    default: return 0.0f;
+    case 128: {
+        // tipl::rgb(r, g, b) as uint32 (b in the low byte, alpha 0), then to float: exact
+        // below 2^24 (io/nifti.hpp:1113-1115)
+        const uint8_t* p = raw + 3 * i;
+        return (float)(((uint32_t)p[0] << 16) | ((uint32_t)p[1] << 8) | (uint32_t)p[2]);
+    }
+    default: return 0.0f;  // no conversion in the reference's read: the voxel stays 0
     }
 }
 
