@@ -1158,6 +1158,12 @@ def served_line(args, rank, world, dist, torch):
                            "mode": "served", "subjects_per_step": args.batch,
                            "cost": COST_DESC[args.cost], "l2": "flushed between timed steps (256 MB write)",
                            "final_cost_mean": float(np.mean(costs)) if costs else None,
+                           "final_cost_subject0": float(costs[0]) if costs else None,
+                           "final_cost_note": "subject 0 is the pair the cpu_baseline and reference_gpu samples "
+                                              "register; its device result equals the CPU replay of the same "
+                                              "search with the oracle's costs bit for bit, and the reference's "
+                                              "own CPU result varies from run to run (its line search races "
+                                              "L-BFGS in two threads)",
                            "cost_evals_per_registration": evals / max(1, len(costs)),
                            "latency_ms": {"p50": pct(0.50), "p95": pct(0.95), "p99": pct(0.99)},
                            "engine": {"affine_launches": estats["affine_launches"],
