@@ -311,6 +311,13 @@ regb_status regb_nifti_load(const char* path, int volume, regb_volume* out, regb
  * carries the int16 datatype code (its type table, io/nifti.hpp:286-290). */
 regb_status regb_nifti_save(const char* path, const regb_volume* vol, const float vs[3], const float srow[12],
                             int is_mni, const char* descrip);
+/* The displacement file of mm_reg::export_nonlinear (reg/mm_reg.hpp:418-441): a 4-D float
+ * NIfTI of dims (w, h, d, 6) -- volumes 0..2 the x, y, z components of f2t (the reverse
+ * field), volumes 3..5 those of t2f (the forward field) -- with the template's voxel
+ * size and srow rows (sform code 1), written as the reference's writer writes it (gzip).
+ * The export's volumes (I, It, J, JJ) are regb_nifti_save calls. */
+regb_status regb_mm_reg_export_fields(const char* path, const regb_field* f2t, const regb_field* t2f, const float vs[3],
+                                      const float srow[12]);
 
 /* downsample_with_padding (numerical/resampling.hpp:575-671); out dims (d+1)/2. */
 regb_status regb_downsample(const regb_volume* in, regb_volume* out, void* stream);

@@ -567,6 +567,13 @@ class Reference(_Lib):
         return bool(self.lib.tiplref_nifti_save(str(path).encode(), _ptr(v), int(v.dtype == np.uint8),
                                                 _ptr(_dims(v.shape)), _ptr(_f32(vs)), _ptr(_f32(srow)), int(is_mni)))
 
+    def nifti_save4(self, path, vol4, vs, srow):
+        """gz_nifti(path, out) << vs << T << I for a float32 array (t, z, y, x)."""
+        v = np.ascontiguousarray(vol4, np.float32)
+        t, z, y, x = v.shape
+        return bool(self.lib.tiplref_nifti_save4(str(path).encode(), _ptr(v), _ptr(np.array([x, y, z, t], np.int32)),
+                                                 _ptr(_f32(vs)), _ptr(_f32(srow))))
+
     def normalize_u16_to_u8(self, img, upper=255.999):
         out = np.zeros(img.shape, np.uint8)
         self.lib.tiplref_normalize_u16_to_u8(_ptr(np.ascontiguousarray(img, np.uint16)), _ptr(_dims(img.shape)),

@@ -493,4 +493,19 @@ int tiplref_nifti_save(const char* path, const void* data, int is_u8, const int*
     std::memcpy(I.data(), data, I.size() * sizeof(float));
     return (out << v << T << bool(is_mni) << I) ? 1 : 0;
 }
+// gz_nifti(path, out) << vs << T << I for a 4-D float image of dims (w, h, d, t):
+// mm_reg::export_nonlinear's dis file (reg/mm_reg.hpp:418-441).
+int tiplref_nifti_save4(const char* path, const float* data, const int* dim4, const float* vs, const float* srow)
+{
+    tipl::io::gz_nifti out(path, std::ios::out);
+    if (!out)
+        return 0;
+    tipl::matrix<4, 4> T;
+    T.identity();
+    std::copy_n(srow, 12, T.begin());
+    tipl::vector<3> v(vs[0], vs[1], vs[2]);
+    tipl::image<4, float> I(tipl::shape<4>(dim4[0], dim4[1], dim4[2], dim4[3]));
+    std::memcpy(I.data(), data, I.size() * sizeof(float));
+    return (out << v << T << I) ? 1 : 0;
+}
 }  // extern "C"

@@ -203,3 +203,24 @@ def test_reader_rejects_truncated_and_unsupported(tmp_path):
         (tmp_path / "bad.nii").write_bytes(bad)
         with pytest.raises(tb.RegbError):
             tb.nifti_load(str(tmp_path / "bad.nii"))
+
+
+def test_mm_reg_export_fields_equal_reference_writer(tmp_path):
+    """regb_mm_reg_export_fields writes mm_reg::export_nonlinear's dis file (a 4-D float
+    NIfTI of f2t's then t2f's x, y, z components, reg/mm_reg.hpp:418-441) byte for byte as
+    the reference's writer writes the same 4-D image."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    import oracle
+
+    if not os.path.exists(oracle.REF_SO):
+        pytest.skip("reference build (oracle/_ref) not present")
+    R = oracle.Reference()
+    rng = np.random.default_rng(9)
+    f2t = rng.normal(0, 2, (5, 6, 7, 3)).astype(np.float32)
+    t2f = rng.normal(0, 2, (5, 6, 7, 3)).astype(np.float32)
+    vs = np.array([1.5, 1.25, 2.0], np.float32)
+    srow = np.array([-1.5, 0, 0, 40, 0, -1.25, 0, 30, 0, 0, 2, -20], np.float32)
+    buf = np.concatenate([np.moveaxis(f2t, -1, 0), np.moveaxis(t2f, -1, 0)])  # (6, z, y, x)
+    assert R.nifti_save4(str(tmp_path / "ref_dis.nii.gz"), buf, vs, srow)
+    tb.mm_reg_export_fields(str(tmp_path / "our_dis.nii.gz"), f2t, t2f, vs, srow)
+    assert (tmp_path / "ref_dis.nii.gz").read_bytes() == (tmp_path / "our_dis.nii.gz").read_bytes()

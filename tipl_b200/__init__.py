@@ -35,7 +35,7 @@ from ._lib import CdmParam, Field, LinearParam, RegbError, Volume  # noqa: F401
 __all__ = ["affine_to_matrix", "affine_to_matrix_f64", "matrix_inverse", "resample", "mi_cost", "mi32_cost",
            "corr_cost", "nifti_info", "nifti_load", "nifti_save", "compose_displacement", "accumulate_displacement",
            "downsample", "upsample_field_x2", "cdm_gradient", "cdm_poisson", "cdm_max_length", "cdm_smooth", "reg",
-           "Engine", "RegbError", "version", "autotune", "tuning", "autotune_buckets", "tuning_buckets"]
+           "Engine", "RegbError", "version", "autotune", "tuning", "autotune_buckets", "tuning_buckets", "mm_reg_export_fields"]
 
 
 def version() -> str:
@@ -361,6 +361,16 @@ def tuning_buckets() -> dict:
 
 
 # ---------------------------------------------------------------- NIfTI volumes (io/nifti.hpp)
+def mm_reg_export_fields(path, f2t, t2f, vs, srow):
+    """mm_reg::export_nonlinear's displacement file (reg/mm_reg.hpp:418-441): a 4-D float
+    NIfTI (w, h, d, 6) of f2t's then t2f's x, y, z components, with the template's voxel
+    size and srow rows."""
+    _lib.check(_lib.lib().regb_mm_reg_export_fields(str(path).encode(), C.byref(_field(_host(f2t, np.float32))),
+                                                    C.byref(_field(_host(t2f, np.float32))),
+                                                    _fptr(np.asarray(vs, np.float32)),
+                                                    _fptr(np.asarray(srow, np.float32))))
+
+
 def nifti_info(path) -> dict:
     """The geometry tipl::io::gz_nifti reports for a .nii / .nii.gz / .hdr file after its
     LPS reorientation: dims (x, y, z), voxel size, srow rows, and the reorientation steps."""

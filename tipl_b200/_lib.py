@@ -153,6 +153,7 @@ _SIGS = {
     "regb_debug_fail_allocations": (C.c_int, [C.c_size_t, C.c_int]),
     "regb_autotune_buckets": (C.c_int, [C.c_char_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "regb_tuning_get_buckets": (C.c_int, [C.c_void_p]),
+    "regb_mm_reg_export_fields": (C.c_int, [C.c_char_p, C.POINTER(Field), C.POINTER(Field), C.c_void_p, C.c_void_p]),
     "regb_cdm_multi": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_int, C.POINTER(Field),
                                  C.POINTER(CdmParam), C.c_char_p, C.c_void_p]),
     "regb_cdm2d_multi": (C.c_int, [C.POINTER(Volume), C.POINTER(Volume), C.c_int, C.POINTER(Field),

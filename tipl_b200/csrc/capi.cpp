@@ -658,6 +658,40 @@ regb_status regb_nifti_save(const char* path, const regb_volume* vol, const floa
     });
 }
 
+regb_status regb_mm_reg_export_fields(const char* path, const regb_field* f2t, const regb_field* t2f, const float vs[3],
+                                      const float srow[12])
+{
+    return guarded([&] {
+        if (!path || !vs || !srow)
+            throw Failure(REGB_ERR_ARG, "null argument");
+        check_field(f2t, "f2t");
+        check_field(t2f, "t2f");
+        if (!same_dims(f2t->dim, t2f->dim))
+            throw Failure(REGB_ERR_ARG, "export: f2t and t2f shapes differ");
+        for (int i = 0; i < 3; ++i)
+            if (f2t->dim[i] > 32767)
+                throw Failure(REGB_ERR_ARG, "NIfTI-1 dims are at most 32767");
+        const size_t n = nvox(f2t->dim);
+        std::vector<float> a(3 * n), b(3 * n), buf(6 * n);
+        const regb_field* src[2] = {f2t, t2f};
+        std::vector<float>* dst[2] = {&a, &b};
+        for (int k = 0; k < 2; ++k) {
+            if (src[k]->location == REGB_DEVICE)
+                REGB_CK(cudaMemcpy(dst[k]->data(), src[k]->ptr, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost));
+            else
+                std::memcpy(dst[k]->data(), src[k]->ptr, sizeof(float) * 3 * n);
+        }
+        // volume c < 3 is f2t's component c, volume 3 + c is t2f's (reg/mm_reg.hpp:421-438)
+        for (int c = 0; c < 3; ++c)
+            for (size_t i = 0; i < n; ++i) {
+                buf[c * n + i] = a[3 * i + c];
+                buf[(3 + c) * n + i] = b[3 * i + c];
+            }
+        nifti_write(path, buf.data(), 16, 32, f2t->dim, vs, srow, 1, nullptr, 6);
+        return REGB_OK;
+    });
+}
+
 regb_status regb_compose_displacement(const regb_volume* from, const regb_field* dis, regb_volume* to, void* stream)
 {
     return guarded([&] {

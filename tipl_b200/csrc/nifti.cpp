@@ -278,14 +278,16 @@ std::vector<uint8_t> nifti_read_voxels(const std::string& path, const NiftiFile&
 }
 
 void nifti_write(const std::string& path, const void* data, int datatype, int bitpix, const int dim[3],
-                 const float vs[3], const float srow[12], int sform_code, const char* descrip)
+                 const float vs[3], const float srow[12], int sform_code, const char* descrip, int nvol)
 {
     uint8_t hdr[352];
     std::memset(hdr, 0, sizeof(hdr));
     auto put = [&](size_t off, const void* v, size_t n) { std::memcpy(hdr + off, v, n); };
     const int32_t sizeof_hdr = 348;
     put(0, &sizeof_hdr, 4);
-    int16_t d[8] = {3, (int16_t)dim[0], (int16_t)dim[1], (int16_t)dim[2], 1, 1, 1, 1};
+    // a 4-D image (nvol > 1) carries its volumes in dim[4] (set_dim, io/nifti.hpp:787-792)
+    int16_t d[8] = {(int16_t)(nvol > 1 ? 4 : 3), (int16_t)dim[0], (int16_t)dim[1], (int16_t)dim[2],
+                    (int16_t)(nvol > 1 ? nvol : 1), 1, 1, 1};
     put(40, d, 16);
     const int16_t dt = (int16_t)datatype, bp = (int16_t)bitpix;
     put(70, &dt, 2);
@@ -305,7 +307,7 @@ void nifti_write(const std::string& path, const void* data, int datatype, int bi
     put(280, srow, 48);
     const char magic[4] = {'n', '+', '1', 0};
     put(344, magic, 4);
-    const size_t bytes = (size_t)dim[0] * dim[1] * dim[2] * (size_t)(bitpix / 8);
+    const size_t bytes = (size_t)dim[0] * dim[1] * dim[2] * (size_t)(bitpix / 8) * (size_t)(nvol > 1 ? nvol : 1);
     // the reference's output stream is always gzip (io/gz_stream.hpp:535-580), whatever
     // the file name says; its reader and this one take either form
     GzFile g;

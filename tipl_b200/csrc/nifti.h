@@ -47,6 +47,6 @@ int nifti_bytes_per_voxel(int datatype, int bitpix);
 // io/gz_stream.hpp:535-580): the 348-byte header, four zero bytes and the voxels, not
 // reoriented, through a gzip stream whatever the file name's extension.
 void nifti_write(const std::string& path, const void* data, int datatype, int bitpix, const int dim[3],
-                 const float vs[3], const float srow[12], int sform_code, const char* descrip);
+                 const float vs[3], const float srow[12], int sform_code, const char* descrip, int nvol = 1);
 
 }  // namespace regb
