@@ -615,11 +615,18 @@ def kernel_case(args):
     import tipl_b200 as tb
     from tipl_b200 import phantom as ph
 
-    f8, m8, _ = make_pair(0)
+    if args.kernel_shape:
+        shape = tuple(int(v) for v in args.kernel_shape.lower().split("x"))[::-1]  # (d, h, w) array order
+        t, mv, _ = ph.affine_pair(shape, rng=np.random.default_rng(ph.seed_for(2, 0)))
+        f8, m8 = ph.normalize_to_u8(t), ph.normalize_to_u8(mv)
+        vs = (1.0, 1.0, 1.0)
+    else:
+        f8, m8, _ = make_pair(0)
+        shape, vs = SHAPE, VS
     fd = torch.from_numpy(f8).cuda()
     md = torch.from_numpy(m8).cuda()
     rng = np.random.default_rng(1)
-    Ts = np.array([tb.affine_to_matrix(ph.random_affine(rng, rot_deg=5, trans_vox=3), SHAPE, VS, SHAPE, VS)
+    Ts = np.array([tb.affine_to_matrix(ph.random_affine(rng, rot_deg=5, trans_vox=3), shape, vs, shape, vs)
                    for _ in range(args.k)], np.float32)
     fn = {"mi": tb.mi_cost, "mi32": tb.mi32_cost, "corr": tb.corr_cost}[args.kernel_case]
     is_mi = args.kernel_case != "corr"
@@ -637,7 +644,8 @@ def kernel_case(args):
     ms = (st.mi_ms / max(1, st.mi_launches)) if is_mi else (st.corr_ms / max(1, st.corr_launches))
     vox = (st.mi_voxels / max(1, st.mi_launches)) if is_mi else (
         st.corr_voxels / max(1, st.corr_launches))
-    print(json.dumps({"kernel_case": args.kernel_case, "k": args.k, "cost0": float(c[0]), "ms_per_launch": ms,
+    print(json.dumps({"kernel_case": args.kernel_case, "k": args.k, "shape_whd": list(f8.shape[::-1]),
+                      "cost0": float(c[0]), "ms_per_launch": ms,
                       "voxel_evals_per_s": vox / (ms / 1000.0)}))
     return 0
 
@@ -954,6 +962,9 @@ def main():
     ap.add_argument("--kernel-case", choices=["mi", "mi32", "corr", "cdm", "pre", "nifti"], default=None,
                     help="run only K-candidate cost batches of the full-size pair (for profiler captures)")
     ap.add_argument("--k", type=int, default=12)
+    ap.add_argument("--kernel-shape", default=None,
+                    help="--kernel-case mi/mi32/corr: WxHxD of a smaller pair (a coarse pyramid level), "
+                         "default the full-size pair")
     ap.add_argument("--pix", choices=["u8", "f32"], default="u8", help="--kernel-case cdm: pixel type")
     ap.add_argument("--precision-report", action="store_true",
                     help="uint16 / BF16 storage: errors of the FP32 path against the FP64 oracle (config 4)")

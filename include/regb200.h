@@ -125,11 +125,13 @@ regb_status regb_stats_reset(int timing);
 regb_status regb_stats_get(regb_stats* out);
 
 /* ---- launch-shape autotuner (no counterpart in the reference) ---------------------- */
-/* Times the batched affine cost kernels (correlation, MI, 32-bin MI) with 12 candidate
- * transforms for a few block sizes (minimum voxels per block) on the current device, on
- * one pair per size bucket (regb_autotune_buckets), and keeps the fastest of each for the
- * rest of the process.  The choice only decides how voxels are split across blocks, so
- * costs are identical under every choice.  tuned (optional, indexed by regb_cost_type)
+/* Times the batched affine cost kernels (correlation, MI, 32-bin MI) with 96 candidate
+ * transforms a launch (the size of the serving engine's gathered launches) for a few
+ * block sizes (minimum voxels per block) on the current device, on one pair per size
+ * bucket (regb_autotune_buckets), and keeps the fastest of each for the rest of the
+ * process.  A launch that fills less than half of one wave of resident blocks at the
+ * chosen size has its chunks split to fill it.  The choice only decides how voxels are
+ * split across blocks, so costs are identical under every choice.  tuned (optional, indexed by regb_cost_type)
  * receives the choices for a 182x218x182 grid, seconds (optional) the time the tuning took. */
 regb_status regb_autotune(int tuned[3], double* seconds);
 /* The block sizes in use for a 182x218x182 grid (the defaults until a tuner runs). */

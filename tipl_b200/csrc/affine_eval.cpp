@@ -152,6 +152,8 @@ void set_task_chunks(AffineTask& t, int cost_type)
     t.nchunk = (int)std::max<long long>(1, (rows + rpc - 1) / rpc);
 }
 
+constexpr int kTuneTasks = 96;  // candidates per timed launch
+
 // Candidate minimum voxels per block, by cost type (MI: at most 65535, its 16-bit counters).
 static const int kTuneCand[3][5] = {{8192, 16384, 32768, 65536, 131072},  // correlation
                                     {16384, 32768, 49152, 60000, 65535},  // MI
@@ -268,7 +270,9 @@ double autotune_cost_kernels(cudaStream_t st, int* chosen, const char* cache_pat
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     }
     // one smooth, many-valued pair per bucket, of the bucket's representative grid, and
-    // 12 small rigid candidates (an optimiser's probe set)
+    // kTuneTasks small rigid candidates: a launch of the serving engine's size (its
+    // launches gather about 90 to 160 candidates; smaller launches get their chunks
+    // split to fill one wave)
     static const Dim3 kRep[kTuneBuckets] = {{64, 64, 64}, {128, 128, 128}, {182, 218, 182}, {256, 256, 256}};
     cudaEvent_t a, b;
     REGB_CK(cudaEventCreate(&a));
@@ -285,9 +289,10 @@ double autotune_cost_kernels(cudaStream_t st, int* chosen, const char* cache_pat
         DevBuf<uint8_t> f(n, st), m(n, st);
         REGB_CK(cudaMemcpyAsync(f.p, hf.data(), n, cudaMemcpyHostToDevice, st));
         REGB_CK(cudaMemcpyAsync(m.p, hm.data(), n, cudaMemcpyHostToDevice, st));
-        std::vector<float> T(12 * 12);
-        for (int k = 0; k < 12; ++k) {
-            const float ang = 0.01f * (float)(k - 6), ca = std::cos(ang), sa = std::sin(ang);
+        std::vector<float> T(12 * kTuneTasks);
+        for (int k = 0; k < kTuneTasks; ++k) {
+            const float ang = 0.01f * (float)(k % 12 - 6) + 0.002f * (float)(k / 12), ca = std::cos(ang),
+                        sa = std::sin(ang);
             const float R[9] = {ca, -sa, 0.0f, sa, ca, 0.0f, 0.0f, 0.0f, 1.0f};
             const float c[3] = {d.w / 2.0f, d.h / 2.0f, d.d / 2.0f};
             for (int r = 0; r < 3; ++r) {
@@ -305,11 +310,11 @@ double autotune_cost_kernels(cudaStream_t st, int* chosen, const char* cache_pat
             float best_ms = 1e30f;
             for (int v : kTuneCand[ct]) {
                 g_min_block_voxels[bk][ct].store(v);
-                ev.eval(0, T.data(), 12);  // warm-up
+                ev.eval(0, T.data(), kTuneTasks);  // warm-up
                 float ms_min = 1e30f;
                 for (int rep = 0; rep < 3; ++rep) {
                     REGB_CK(cudaEventRecord(a, st));
-                    ev.eval(0, T.data(), 12);
+                    ev.eval(0, T.data(), kTuneTasks);
                     REGB_CK(cudaEventRecord(b, st));
                     REGB_CK(cudaEventSynchronize(b));
                     float ms = 0.0f;
@@ -334,8 +339,42 @@ double autotune_cost_kernels(cudaStream_t st, int* chosen, const char* cache_pat
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
 }
 
+// A launch of few tasks on small grids fills less than half of one wave of resident
+// blocks at the tuned chunk size, and then one block's serial share of voxels sets
+// its time.  Such a launch cuts every chunk into f pieces (never below
+// kFillMinVoxels voxels a block), f the largest factor that still fits one wave:
+// ceil(rows / ceil(rpc / f)) <= f * ceil(rows / rpc), so the launch stays within
+// f times its blocks.  Chunking only decides which block counts which voxels, so
+// the costs do not change.
+constexpr long long kFillMinVoxels = 2048;
+
+void fill_wave(AffineTask* t, int K, int cost_type)
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return;
+    }
+    long long blocks = 0;
+    for (int k = 0; k < K; ++k)
+        blocks += t[k].nchunk;
+    const long long slots = (long long)sms * cost_blocks_per_sm(cost_type == REGB_COST_CORR);
+    const long long f = slots / std::max<long long>(1, blocks);
+    if (f < 2)
+        return;
+    for (int k = 0; k < K; ++k) {
+        const long long w = t[k].fd.w, rows = (long long)t[k].fd.h * t[k].fd.d;
+        const long long floor_rows = std::max<long long>(1, (kFillMinVoxels + w - 1) / w);
+        const long long rpc = std::min<long long>(t[k].chunk, std::max(floor_rows, (t[k].chunk + f - 1) / f));
+        t[k].chunk = (int)rpc;
+        t[k].nchunk = (int)std::max<long long>(1, (rows + rpc - 1) / rpc);
+    }
+}
+
 void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, double* out)
 {
+    fill_wave(s.h_tasks.p, K, cost_type);
     int max_chunks = 1, max_chunks_tex = 1, ntex = 0;
     for (int k = 0; k < K; ++k) {
         AffineTask& t = s.h_tasks.p[k];

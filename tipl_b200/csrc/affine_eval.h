@@ -66,10 +66,13 @@ void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, dou
 
 // Chunking of one task over its fixed-grid voxels.
 void set_task_chunks(AffineTask& t, int cost_type);
+// Splits the chunks of a launch of K tasks that fills less than half of one wave of
+// resident blocks (costs unchanged: chunking only decides which block counts which voxels).
+void fill_wave(AffineTask* t, int K, int cost_type);
 // The chunking parameter (minimum voxels per block) per size bucket of the fixed grid
 // and cost type, and its autotuner: for each bucket it times each cost kernel on a pair
-// of the bucket's representative grid (64^3, 128^3, 182x218x182, 256^3) with 12
-// candidates for a few block sizes on the current device and keeps the fastest
+// of the bucket's representative grid (64^3, 128^3, 182x218x182, 256^3) with 96
+// candidates a launch for a few block sizes on the current device and keeps the fastest
 // (results do not depend on the choice).  chosen (optional) receives the table
 // [bucket * 3 + cost type]; cache_path names a table file (NULL: none, "": the default
 // file), which is read instead of timing when it holds this device's table and written

@@ -596,6 +596,23 @@ cudaError_t launch_corr_tex(const AffineTask* d_tasks, int ntask, int max_chunks
     return cudaGetLastError();
 }
 
+int cost_blocks_per_sm(bool is_corr)
+{
+    if (!is_corr)
+        return 1;  // __launch_bounds__(768, 1)
+    static std::atomic<int> occ{0};
+    int v = occ.load();
+    if (!v) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, corr_kernel<true>, kCorrThreads, 0) != cudaSuccess ||
+            v < 1) {
+            (void)cudaGetLastError();
+            v = 1;
+        }
+        occ.store(v);
+    }
+    return v;
+}
+
 // ---------------------------------------------------------------- template statistics
 // Row histogram of the fixed volume (histogram(from, 0, 255, 256), which for uint8
 // is the value count) and its exact sums for the correlation cost.

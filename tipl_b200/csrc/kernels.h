@@ -114,6 +114,9 @@ cudaError_t launch_mi32(const AffineTask* d_tasks, int ntask, int max_chunks, cu
 // texture (tex != 0; correlation tasks in integer-shift mode still read bytes).
 cudaError_t launch_mi32_tex(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
 cudaError_t launch_corr_tex(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st);
+// Blocks of a cost kernel resident on one SM (is_corr: the correlation kernel, else
+// either MI kernel, which launch one 768-thread block per SM).
+int cost_blocks_per_sm(bool is_corr);
 cudaError_t launch_fixed_stats(const uint8_t* f, long long n, int32_t* hist, unsigned long long* sums,
                                cudaStream_t st);
 

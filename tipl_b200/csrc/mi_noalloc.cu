@@ -121,8 +121,10 @@ extern "C" regb_status regb_mi_cost_noalloc(const uint8_t* fixed, const int fixe
             t.moments = s->moments + 3 * k;
             t.cost = cost + k;
             set_task_chunks(t, REGB_COST_MI);
-            max_chunks = t.nchunk > max_chunks ? t.nchunk : max_chunks;
         }
+        fill_wave(h, K, REGB_COST_MI);
+        for (int k = 0; k < K; ++k)
+            max_chunks = h[k].nchunk > max_chunks ? h[k].nchunk : max_chunks;
         REGB_CK(cudaMemcpyAsync(s->tasks, h, sizeof(AffineTask) * K, cudaMemcpyHostToDevice, st));
         REGB_CK(launch_mi(s->tasks, K, max_chunks, st));
         count_launch(2);  // the histogram and the reduction (launch_fixed_stats counts its own)
