@@ -129,8 +129,8 @@ regb_status regb_stats_get(regb_stats* out);
  * transforms a launch (the size of the serving engine's gathered launches) for a few
  * block sizes (minimum voxels per block) on the current device, on one pair per size
  * bucket (regb_autotune_buckets), and keeps the fastest of each for the rest of the
- * process.  A launch that fills less than half of one wave of resident blocks at the
- * chosen size has its chunks split to fill it.  The choice only decides how voxels are
+ * process.  Outside the serving engine, a launch that fills less than half of one wave
+ * of resident blocks at the chosen size has its chunks split to fill it.  The choice only decides how voxels are
  * split across blocks, so costs are identical under every choice.  tuned (optional, indexed by regb_cost_type)
  * receives the choices for a 182x218x182 grid, seconds (optional) the time the tuning took. */
 regb_status regb_autotune(int tuned[3], double* seconds);

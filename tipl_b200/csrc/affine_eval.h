@@ -61,8 +61,10 @@ constexpr int kMiMaxWidth = 65535;
 void check_mi_width(int fixed_width, const char* who);
 
 // Fills the scratch pointers of h_tasks[0..K), launches the MI or correlation
-// kernel for all of them, and copies the costs back (synchronises st).
-void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, double* out);
+// kernel for all of them, and copies the costs back (synchronises st).  fill: split
+// the chunks of a launch below half a wave (fill_wave); the serving engine's batcher
+// passes false.
+void run_affine_tasks(TaskScratch& s, int K, int cost_type, cudaStream_t st, double* out, bool fill = true);
 
 // Chunking of one task over its fixed-grid voxels.
 void set_task_chunks(AffineTask& t, int cost_type);

@@ -102,7 +102,7 @@ void AffineBatcher::loop(Worker& w)
                         k += r->n;
                     }
                 std::vector<double> c(total);
-                run_affine_tasks(s, total, ct, w.st, c.data());
+                run_affine_tasks(s, total, ct, w.st, c.data(), false);
                 k = 0;
                 for (Req* r : batch)
                     if (r->cost_type == ct) {
