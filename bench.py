@@ -891,6 +891,7 @@ def poisson_case(args):
             eng.wait(eng.submit(pool[ti], template=tids[ti], cdm=True, cdm_param=cdm_p))
         ids = [None] * len(arrivals)
         sub_t = [0.0] * len(arrivals)
+        est0 = eng.stats()
         start = time.perf_counter()
 
         def feed():
@@ -926,6 +927,9 @@ def poisson_case(args):
         by_t.setdefault(ti, []).append(l)
     lat_s = sorted(lat)
     pct = lambda q: lat_s[min(len(lat_s) - 1, int(q * len(lat_s)))]  # noqa: E731
+    # jobs in the system (submitted, not yet done) at every tenth of the span
+    marks = [sub_t[0] + span * k / 10.0 for k in range(11)]
+    in_system = [sum(1 for a, d in zip(sub_t, done_at) if a <= m < d) for m in marks]
     print(json.dumps({"workload": "poisson serving: affine + CDM, 4 resident templates, random-shape uint16/float32 "
                                   "subjects, 150 GB budget",
                       "metric": "registrations/s (open-loop Poisson arrivals) and latency",
@@ -933,9 +937,16 @@ def poisson_case(args):
                       "jobs": len(arrivals), "ok": ok,
                       "completed_per_s": len(arrivals) / span,
                       "latency_ms": {"p50": pct(0.50), "p95": pct(0.95), "p99": pct(0.99), "max": lat_s[-1]},
+                      "jobs_in_system_by_tenth_of_span": in_system,
                       "latency_p50_ms_by_template": {"x".join(str(v) for v in tshapes[ti][::-1]): float(np.median(v))
                                                      for ti, v in sorted(by_t.items())},
                       "mi_busy_fraction": st.mi_busy_ms / 1000.0 / span,
+                      # device time of the CDM rounds (their own stream, concurrent with the MI launches)
+                      "cdm_busy_fraction": (est["cdm_round_ms"] - est0["cdm_round_ms"]) / 1000.0 / span,
+                      "cdm_levels_per_round": (est["cdm_round_segments"] - est0["cdm_round_segments"]) /
+                      max(1, est["cdm_rounds"] - est0["cdm_rounds"]),
+                      "affine_tasks_per_launch": (est["affine_tasks"] - est0["affine_tasks"]) /
+                      max(1, est["affine_launches"] - est0["affine_launches"]),
                       "engine": {"affine_launches": est["affine_launches"], "affine_tasks": est["affine_tasks"],
                                  "cdm_rounds": est["cdm_rounds"]},
                       "plain_sequential_jobs_per_s": plain_rate,

@@ -488,6 +488,9 @@ typedef struct {
     long long affine_launches, affine_tasks, cdm_rounds;
     long long cdm_round_segments;  /* CDM levels summed over rounds: / cdm_rounds = the
                                       levels that share one round's launches */
+    double cdm_round_ms;           /* device time of the CDM rounds, summed (CUDA events on
+                                      the scheduler's stream, from the segment upload to the
+                                      status read-back) */
 } regb_engine_stats;
 
 void regb_engine_config_default(regb_engine_config* c);

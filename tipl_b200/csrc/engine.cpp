@@ -202,6 +202,7 @@ public:
         s.affine_tasks = batcher_.tasks_evaluated();
         s.cdm_rounds = sched_.rounds();
         s.cdm_round_segments = sched_.round_segments();
+        s.cdm_round_ms = sched_.round_ms();
         return s;
     }
 

@@ -7,7 +7,15 @@ namespace regb {
 
 CdmScheduler::CdmScheduler(int iters_per_round) : iters_(std::max(1, iters_per_round))
 {
-    REGB_CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    {
+        // the rounds are the serving engine's slower stage: their blocks go first when
+        // they and the affine cost launches (default priority) both wait for an SM
+        int lo = 0, hi = 0;
+        REGB_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        REGB_CK(cudaStreamCreateWithPriority(&st_, cudaStreamNonBlocking, hi));
+    }
+    REGB_CK(cudaEventCreate(&ev_[0]));
+    REGB_CK(cudaEventCreate(&ev_[1]));
     int dev = 0;
     REGB_CK(cudaGetDevice(&dev));
     th_ = std::thread([this, dev] {
@@ -31,6 +39,9 @@ CdmScheduler::~CdmScheduler()
         cudaStreamSynchronize(st_);
         cudaStreamDestroy(st_);
     }
+    for (cudaEvent_t e : ev_)
+        if (e)
+            cudaEventDestroy(e);
 }
 
 void CdmScheduler::run(CdmLevel& lvl, volatile const int* terminated)
@@ -72,6 +83,7 @@ void CdmScheduler::loop()
             std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
             for (int i = 0; i < n; ++i)
                 h_segs_.p[i] = cur[order[i]]->lvl->seg;
+            REGB_CK(cudaEventRecord(ev_[0], st_));
             REGB_CK(cudaMemcpyAsync(segs_.p, h_segs_.p, sizeof(CdmSeg) * n, cudaMemcpyHostToDevice, st_));
             for (int it = 0; it < iters_; ++it) {
                 for (int g0 = 0; g0 < n;) {
@@ -88,8 +100,12 @@ void CdmScheduler::loop()
             }
             REGB_CK(launch_cdm_status(segs_.p, n, status_.p, st_));
             REGB_CK(cudaMemcpyAsync(h_status_.p, status_.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
+            REGB_CK(cudaEventRecord(ev_[1], st_));
             REGB_CK(cudaStreamSynchronize(st_));
+            float ms = 0.0f;
+            REGB_CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
             lk.lock();
+            round_ms_ += ms;
             ++rounds_;
             round_segments_ += n;
             for (int i = 0; i < n; ++i) {

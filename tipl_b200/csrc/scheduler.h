@@ -22,8 +22,22 @@ public:
     CdmScheduler& operator=(const CdmScheduler&) = delete;
     // Iterates the level until its loop ends (or terminated is set); blocks the caller.
     void run(CdmLevel& lvl, volatile const int* terminated);
-    long long rounds() const { return rounds_; }
-    long long round_segments() const { return round_segments_; }  // levels summed over rounds
+    // counters, read under the scheduler's lock
+    long long rounds()
+    {
+        std::lock_guard<std::mutex> g(m_);
+        return rounds_;
+    }
+    long long round_segments()  // levels summed over rounds
+    {
+        std::lock_guard<std::mutex> g(m_);
+        return round_segments_;
+    }
+    double round_ms()  // device time of the rounds, summed
+    {
+        std::lock_guard<std::mutex> g(m_);
+        return round_ms_;
+    }
 
 private:
     struct Entry {
@@ -39,7 +53,9 @@ private:
     int iters_;
     long long rounds_ = 0;
     long long round_segments_ = 0;
+    double round_ms_ = 0.0;
     cudaStream_t st_ = nullptr;
+    cudaEvent_t ev_[2] = {nullptr, nullptr};
     DevBuf<CdmSeg> segs_;
     PinBuf<CdmSeg> h_segs_;
     DevBuf<int> status_;
