@@ -1,6 +1,7 @@
 // CDM nonlinear registration passes (reg/cdm.hpp) and the displacement algebra
-// they use (numerical/dif.hpp), as segment kernels: blockIdx.y selects a job
-// level (CdmSeg), blockIdx.x < seg.nblk strides over its voxels.
+// they use (numerical/dif.hpp), as segment kernels: a launch covers one or more job
+// levels (CdmSeg entries), each owning nblk consecutive blocks of a 1-D grid that
+// stride over its voxels.
 //
 // One iteration of a level (reg/cdm.hpp:418-470) is the launch sequence
 //   compose -> gradient (+ loop decisions in its last block) -> 12 Poisson sweeps
@@ -26,21 +27,44 @@ int cdm_blocks_for(long long nvox)
     return (int)(b < 1 ? 1 : b);
 }
 
+// The segment entry a block of a launch over nseg entries works on: the last one
+// whose blk0 <= blockIdx.x.  Every warp finds it on its own with one ballot per 32
+// entries (all lanes active: this runs first in each kernel); a launch of one entry
+// reads nothing to find it.
+__device__ __forceinline__ int seg_of_block(const CdmSeg* __restrict__ segs, int nseg)
+{
+    if (nseg <= 1)
+        return 0;
+    const int b = (int)blockIdx.x, lane = threadIdx.x & 31;
+    int k = 0;
+    for (int base = 0; base < nseg; base += 32) {
+        const int i = base + lane;
+        const unsigned m = __ballot_sync(0xffffffffu, i < nseg && segs[i].blk0 <= b);
+        k += __popc(m);
+        if (m != 0xffffffffu)
+            break;
+    }
+    return k - 1;
+}
+
+// MULTI: the kernel's instantiation for launches over several entries; a launch of one
+// entry takes the other, which has no lookup in its code at all.
 #define SEG_BEGIN                                                  \
-    const CdmSeg& S = segs[blockIdx.y];                            \
-    if ((int)blockIdx.x >= S.nblk)                                 \
+    const CdmSeg& S = segs[MULTI ? seg_of_block(segs, nseg) : 0];  \
+    const int blk = (int)blockIdx.x - (MULTI ? S.blk0 : 0);        \
+    if (blk >= S.nblk)                                             \
         return;                                                    \
     const Dim3 D{S.w, S.h, S.d};                                   \
     const long long n = D.n();                                     \
     const long long stride = (long long)S.nblk * blockDim.x;       \
-    const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long first = (long long)blk * blockDim.x + threadIdx.x;
 
 // ------------------------------------------------------------------ compose
 // compose_displacement (numerical/dif.hpp:90-107, 260-285): Js = Is[mod] where the
 // displacement is exactly zero, else the trilinear sample at x + d; failed
 // samples are 0.
-template <typename T>
-__global__ void __launch_bounds__(kCdmThreads) cdm_compose_kernel(const CdmSeg* __restrict__ segs, int mod)
+template <typename T, bool MULTI>
+__global__ void __launch_bounds__(kCdmThreads) cdm_compose_kernel(const CdmSeg* __restrict__ segs, int nseg, int mod)
 {
     SEG_BEGIN
     if (S.ctl->done || mod >= max(S.nmod, 1))
@@ -208,8 +232,8 @@ __device__ __forceinline__ void store_term(float* __restrict__ nd, long long i, 
 // cdm_get_gradient_r_imp / _d_imp (reg/cdm.hpp:46-78) of modality mod: the term is
 // 0 + gradient term; the cost of every voxel (0 where skipped) is summed per block in
 // double.
-template <typename T>
-__global__ void __launch_bounds__(kCdmThreads) cdm_gradient_kernel(const CdmSeg* __restrict__ segs, int gtype,
+template <typename T, bool MULTI>
+__global__ void __launch_bounds__(kCdmThreads) cdm_gradient_kernel(const CdmSeg* __restrict__ segs, int nseg, int gtype,
                                                                    int mod)
 {
     SEG_BEGIN
@@ -297,7 +321,7 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_gradient_kernel(const CdmSeg*
     __shared__ double red[32];
     csum = block_sum(csum, red);
     if (threadIdx.x == 0)
-        S.cost_part[blockIdx.x] = csum;
+        S.cost_part[blk] = csum;
     if (last_block_of_segment(S))
         control_block(S, mod);
 }
@@ -317,10 +341,13 @@ struct BoxSmem {
     int p2[5][kHZ][kTY][kTX];  // x,y-summed
 };
 
-__global__ void __launch_bounds__(kBoxThreads) cdm_gradient_box_u8_kernel(const CdmSeg* __restrict__ segs, int mod)
+template <bool MULTI>
+__global__ void __launch_bounds__(kBoxThreads) cdm_gradient_box_u8_kernel(const CdmSeg* __restrict__ segs, int nseg,
+                                                                                    int mod)
 {
-    const CdmSeg& S = segs[blockIdx.y];
-    if ((int)blockIdx.x >= S.nblk)
+    const CdmSeg& S = segs[MULTI ? seg_of_block(segs, nseg) : 0];
+    const int blk = (int)blockIdx.x - (MULTI ? S.blk0 : 0);
+    if (blk >= S.nblk)
         return;
     if (S.ctl->done || mod >= max(S.nmod, 1))
         return;
@@ -334,7 +361,7 @@ __global__ void __launch_bounds__(kBoxThreads) cdm_gradient_box_u8_kernel(const 
     const int ntiles = ntx * nty * ntz;
     const long long wl = D.w, whl = D.wh();
     double csum = 0.0;
-    for (int tile = blockIdx.x; tile < ntiles; tile += S.nblk) {
+    for (int tile = blk; tile < ntiles; tile += S.nblk) {
         const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
         const int x0 = tx * kTX, y0 = ty * kTY, z0 = tz * kTZ;
         __syncthreads();  // the previous tile's readers are done with the buffers
@@ -428,7 +455,7 @@ __global__ void __launch_bounds__(kBoxThreads) cdm_gradient_box_u8_kernel(const 
     __shared__ double red[32];
     csum = block_sum(csum, red);
     if (threadIdx.x == 0)
-        S.cost_part[blockIdx.x] = csum;
+        S.cost_part[blk] = csum;
     if (last_block_of_segment(S))
         control_block(S, mod);
 }
@@ -602,7 +629,8 @@ __device__ __forceinline__ float poisson_weight(const CdmSeg& S)
     return S.ndim == 2 ? -0.5f / 2.0f : -0.5f / 3.0f;
 }
 
-__global__ void __launch_bounds__(kCdmThreads) cdm_poisson_kernel(const CdmSeg* __restrict__ segs, int mode,
+template <bool MULTI>
+__global__ void __launch_bounds__(kCdmThreads) cdm_poisson_kernel(const CdmSeg* __restrict__ segs, int nseg, int mode,
                                                                   int parity)
 {
     SEG_BEGIN
@@ -702,7 +730,8 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_poisson_kernel(const CdmSeg* 
 // cdm_max_displacement_length (reg/cdm.hpp:260-295), only while theta == 0 (the
 // first iteration of a level); the last block sets theta and speed/theta, or
 // leaves the loop when theta is 0 (reg/cdm.hpp:463-467).
-__global__ void __launch_bounds__(kCdmThreads) cdm_theta_kernel(const CdmSeg* __restrict__ segs)
+template <bool MULTI>
+__global__ void __launch_bounds__(kCdmThreads) cdm_theta_kernel(const CdmSeg* __restrict__ segs, int nseg)
 {
     SEG_BEGIN
     CdmCtl* c = S.ctl;
@@ -736,7 +765,8 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_theta_kernel(const CdmSeg* __
 // (numerical/dif.hpp:166-186): out = (cur_d + id)(x + new_d) - x where new_d is
 // non-zero and the sample lands inside, else cur_d.  The mapping cur_d + id is
 // formed per corner exactly as displacement_to_mapping stores it.
-__global__ void __launch_bounds__(kCdmThreads) cdm_accumulate_kernel(const CdmSeg* __restrict__ segs)
+template <bool MULTI>
+__global__ void __launch_bounds__(kCdmThreads) cdm_accumulate_kernel(const CdmSeg* __restrict__ segs, int nseg)
 {
     SEG_BEGIN
     const CdmCtl* c = S.ctl;
@@ -841,7 +871,8 @@ __global__ void __launch_bounds__(kCdmThreads) cdm_accumulate_kernel(const CdmSe
 // cdm_smooth (reg/cdm.hpp:302-366): cur_d = d*(1-s) + (s/6) * (d[+1] + d[-1] +
 // d[+w] + d[-w] + d[+wh] + d[-wh]) by flat index; s == 0 leaves cur_d as it is.
 // 2-D: s/4 and four neighbours (the +-wh taps of a d == 1 level fall outside).
-__global__ void __launch_bounds__(kCdmThreads) cdm_smooth_kernel(const CdmSeg* __restrict__ segs)
+template <bool MULTI>
+__global__ void __launch_bounds__(kCdmThreads) cdm_smooth_kernel(const CdmSeg* __restrict__ segs, int nseg)
 {
     SEG_BEGIN
     const CdmCtl* c = S.ctl;
@@ -1057,16 +1088,25 @@ cudaError_t launch_cdm_status(const CdmSeg* segs, int nseg, int* out, cudaStream
 }
 
 // ------------------------------------------------------------------ launchers
-#define SEG_GRID dim3(blocks, nseg)
+// blocks: the launch's blocks, sum(nblk) over its nseg segment entries (their blk0 set
+// accordingly); one entry alone: its nblk.
+#define SEG_GRID dim3(blocks)
+#define SEG_LAUNCH(multi, single, threads, smem, ...)                                  \
+    do {                                                                               \
+        if (nseg > 1)                                                                  \
+            multi<<<SEG_GRID, threads, smem, st>>>(segs, nseg, ##__VA_ARGS__);         \
+        else                                                                           \
+            single<<<SEG_GRID, threads, smem, st>>>(segs, nseg, ##__VA_ARGS__);        \
+    } while (0)
 
 cudaError_t launch_cdm_compose(const CdmSeg* segs, int nseg, int blocks, int pix, cudaStream_t st, int mod)
 {
     if (mod < 0 || mod >= kCdmMaxModalities)
         return cudaErrorInvalidValue;
     if (pix == 0)
-        cdm_compose_kernel<uint8_t><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, mod);
+        SEG_LAUNCH((cdm_compose_kernel<uint8_t, true>), (cdm_compose_kernel<uint8_t, false>), kCdmThreads, 0, mod);
     else
-        cdm_compose_kernel<float><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, mod);
+        SEG_LAUNCH((cdm_compose_kernel<float, true>), (cdm_compose_kernel<float, false>), kCdmThreads, 0, mod);
     count_launch();
     return cudaGetLastError();
 }
@@ -1084,17 +1124,23 @@ cudaError_t launch_cdm_gradient(const CdmSeg* segs, int nseg, int blocks, int pi
             return e;
         const unsigned long long bit = 1ull << (dev & 63);
         if (!(attr_set.load() & bit)) {
-            e = cudaFuncSetAttribute(cdm_gradient_box_u8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            e = cudaFuncSetAttribute(cdm_gradient_box_u8_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(BoxSmem));
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(cdm_gradient_box_u8_kernel<false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BoxSmem));
             if (e != cudaSuccess)
                 return e;
             attr_set.fetch_or(bit);
         }
-        cdm_gradient_box_u8_kernel<<<SEG_GRID, kBoxThreads, sizeof(BoxSmem), st>>>(segs, mod);
+        SEG_LAUNCH(cdm_gradient_box_u8_kernel<true>, cdm_gradient_box_u8_kernel<false>, kBoxThreads,
+                   sizeof(BoxSmem), mod);
     } else if (pix == 0)
-        cdm_gradient_kernel<uint8_t><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, gradient_type, mod);
+        SEG_LAUNCH((cdm_gradient_kernel<uint8_t, true>), (cdm_gradient_kernel<uint8_t, false>), kCdmThreads, 0,
+                   gradient_type, mod);
     else
-        cdm_gradient_kernel<float><<<SEG_GRID, kCdmThreads, 0, st>>>(segs, gradient_type, mod);
+        SEG_LAUNCH((cdm_gradient_kernel<float, true>), (cdm_gradient_kernel<float, false>), kCdmThreads, 0,
+                   gradient_type, mod);
     count_launch();
     return cudaGetLastError();
 }
@@ -1102,31 +1148,31 @@ cudaError_t launch_cdm_gradient(const CdmSeg* segs, int nseg, int blocks, int pi
 cudaError_t launch_cdm_poisson(const CdmSeg* segs, int nseg, int blocks, int sweeps, cudaStream_t st)
 {
     // sweeps is 12 (reg/cdm.hpp:165): first (B), 10 middle (B->A, A->B, ...), last (B->A)
-    cdm_poisson_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs, 0, 0);
+    SEG_LAUNCH(cdm_poisson_kernel<true>, cdm_poisson_kernel<false>, kCdmThreads, 0, 0, 0);
     for (int k = 1; k < sweeps - 1; ++k)
-        cdm_poisson_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs, 1, k & 1);
-    cdm_poisson_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs, 2, 1);
+        SEG_LAUNCH(cdm_poisson_kernel<true>, cdm_poisson_kernel<false>, kCdmThreads, 0, 1, k & 1);
+    SEG_LAUNCH(cdm_poisson_kernel<true>, cdm_poisson_kernel<false>, kCdmThreads, 0, 2, 1);
     count_launch(sweeps);
     return cudaGetLastError();
 }
 
 cudaError_t launch_cdm_theta(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st)
 {
-    cdm_theta_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+    SEG_LAUNCH(cdm_theta_kernel<true>, cdm_theta_kernel<false>, kCdmThreads, 0);
     count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_cdm_accumulate(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st)
 {
-    cdm_accumulate_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+    SEG_LAUNCH(cdm_accumulate_kernel<true>, cdm_accumulate_kernel<false>, kCdmThreads, 0);
     count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_cdm_smooth(const CdmSeg* segs, int nseg, int blocks, cudaStream_t st)
 {
-    cdm_smooth_kernel<<<SEG_GRID, kCdmThreads, 0, st>>>(segs);
+    SEG_LAUNCH(cdm_smooth_kernel<true>, cdm_smooth_kernel<false>, kCdmThreads, 0);
     count_launch();
     return cudaGetLastError();
 }

@@ -38,6 +38,8 @@ struct CdmLevel {
 
 // One iteration of every segment in d_segs (reg/cdm.hpp:418-470); the segments
 // share pix and the gradient types of their modalities (gtypes, one char each).
+// blocks: sum(nblk) over the nseg entries, whose blk0 number them (one entry
+// alone: its nblk, blk0 0).
 void launch_iteration(const CdmSeg* d_segs, int nseg, int blocks, int pix, const std::string& gtypes,
                       cudaStream_t st);
 

@@ -90,6 +90,10 @@ struct CdmSeg {
     float* tmp_d;     // Poisson iterate B / accumulated field (scratch)
     double* cost_part;  // per-block partial cost sums (nblk entries)
     CdmCtl* ctl;
+    // A launch over several segments (their entries back to back) has sum(nblk) blocks:
+    // this segment owns blocks [blk0, blk0 + nblk), blk0 ascending along the entries
+    // (0 for a launch of this segment alone).
+    int blk0;
 };
 
 template <typename T>

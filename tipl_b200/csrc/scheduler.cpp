@@ -83,21 +83,29 @@ void CdmScheduler::loop()
             std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
             for (int i = 0; i < n; ++i)
                 h_segs_.p[i] = cur[order[i]]->lvl->seg;
+            // one launch per group over exactly its blocks: each entry's blk0 counts the
+            // blocks of the group's entries before it
+            struct Group {
+                int g0, g1, blocks;
+            };
+            std::vector<Group> groups;
+            for (int g0 = 0; g0 < n;) {
+                int g1 = g0, blocks = 0;
+                while (g1 < n && key(order[g1]) == key(order[g0])) {
+                    h_segs_.p[g1].blk0 = blocks;
+                    blocks += h_segs_.p[g1].nblk;
+                    ++g1;
+                }
+                groups.push_back({g0, g1, blocks});
+                g0 = g1;
+            }
             REGB_CK(cudaEventRecord(ev_[0], st_));
             REGB_CK(cudaMemcpyAsync(segs_.p, h_segs_.p, sizeof(CdmSeg) * n, cudaMemcpyHostToDevice, st_));
-            for (int it = 0; it < iters_; ++it) {
-                for (int g0 = 0; g0 < n;) {
-                    int g1 = g0;
-                    int blocks = 1;
-                    while (g1 < n && key(order[g1]) == key(order[g0])) {
-                        blocks = std::max(blocks, h_segs_.p[g1].nblk);
-                        ++g1;
-                    }
-                    const Entry* e = cur[order[g0]];
-                    launch_iteration(segs_.p + g0, g1 - g0, blocks, e->lvl->pix, e->lvl->gtypes, st_);
-                    g0 = g1;
+            for (int it = 0; it < iters_; ++it)
+                for (const Group& g : groups) {
+                    const Entry* e = cur[order[g.g0]];
+                    launch_iteration(segs_.p + g.g0, g.g1 - g.g0, g.blocks, e->lvl->pix, e->lvl->gtypes, st_);
                 }
-            }
             REGB_CK(launch_cdm_status(segs_.p, n, status_.p, st_));
             REGB_CK(cudaMemcpyAsync(h_status_.p, status_.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
             REGB_CK(cudaEventRecord(ev_[1], st_));
