@@ -885,7 +885,8 @@ def poisson_case(args):
         if t > args.duration:
             break
         arrivals.append((t, int(rng.integers(0, 4)), int(rng.integers(0, len(pool)))))
-    with tb.Engine(hbm_budget_bytes=150 << 30, max_active=args.max_active) as eng:
+    with tb.Engine(hbm_budget_bytes=150 << 30, max_active=args.max_active,
+                   cdm_iters_per_round=args.cdm_iters_per_round) as eng:
         tids = [eng.add_template(tm) for tm in templates]
         for ti in range(4):  # warm-up: one job per template
             eng.wait(eng.submit(pool[ti], template=tids[ti], cdm=True, cdm_param=cdm_p))
@@ -934,6 +935,7 @@ def poisson_case(args):
                                   "subjects, 150 GB budget",
                       "metric": "registrations/s (open-loop Poisson arrivals) and latency",
                       "rate_per_s": args.rate, "duration_s": args.duration, "max_active": args.max_active,
+                      "cdm_iters_per_round": args.cdm_iters_per_round,
                       "jobs": len(arrivals), "ok": ok,
                       "completed_per_s": len(arrivals) / span,
                       "latency_ms": {"p50": pct(0.50), "p95": pct(0.95), "p99": pct(0.99), "max": lat_s[-1]},
@@ -991,6 +993,9 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="--workload poisson: arrivals per second")
     ap.add_argument("--duration", type=float, default=15.0, help="--workload poisson: seconds of arrivals")
     ap.add_argument("--max-active", type=int, default=32, help="--workload poisson: engine slots")
+    ap.add_argument("--cdm-iters-per-round", type=int, default=4,
+                    help="--workload poisson: CDM iterations the engine launches between two reads of the levels' "
+                         "done flags")
     ap.add_argument("--gather-us", type=int, default=30,
                     help="served mode: how long a cost batch waits for more jobs once the device is free")
     args = ap.parse_args()
