@@ -233,14 +233,14 @@ regb_status regb_mi32_cost(const regb_volume* fixed, const regb_volume* moving, 
  * is a DEVICE array of K doubles.  Nothing is allocated: all scratch lives in one
  * file-scope device array (4 MiB of joint histograms plus about 25 KiB), so K <= 16 and
  * larger K is rejected with REGB_ERR_ARG, as is a fixed width above 65535.  The first
- * call on a device looks up that array's device address, so make that first call
- * before any stream capture; it is also the call on which the CUDA runtime, which
- * loads device code lazily, brings this library's kernels and the array (about 4 MiB
- * plus code) into device memory, so make it during initialisation, where allocation
- * is still allowed.  Every call shares the array: calls that overlap on the GPU
- * (different streams or host threads without ordering) race and give wrong costs.
- * The call synchronises the stream before it returns, so the costs are written when
- * it returns. */
+ * call on a device looks up that array's device address; it is also the call on which
+ * the CUDA runtime, which loads device code lazily, brings this library's kernels and
+ * the array (about 4 MiB plus code) into device memory, so make it during
+ * initialisation, where allocation is still allowed.  Every call shares the array:
+ * calls that overlap on the GPU (different streams or host threads without ordering)
+ * race and give wrong costs.  The call is synchronous: it synchronises the stream
+ * before it returns, so the costs are written when it returns, and it cannot be part
+ * of a CUDA graph -- a call while the stream is being captured returns REGB_ERR_ARG. */
 regb_status regb_mi_cost_noalloc(const uint8_t* fixed, const int fixed_dim[3], const uint8_t* moving,
                                  const int moving_dim[3], const float* T, int K, double* cost, void* stream);
 /* correlation::operator() (reg/linear.hpp:23-78) for K transforms: 1 - r^2 with the

@@ -46,3 +46,35 @@ def test_noalloc_matches_mi_cost_twice():
                                 Ts.ctypes.data_as(C.c_void_p), 17, C.c_void_p(out.data_ptr()), None)
     assert st == _lib.REGB_ERR_ARG
     assert b"16" in L.regb_last_error()
+
+
+def test_noalloc_refuses_stream_capture():
+    """The call synchronises its stream, which a CUDA graph capture cannot hold: made while
+    its stream is being captured, it returns REGB_ERR_ARG before any work and the capture
+    ends normally."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from tipl_b200 import _lib, build
+
+    build.build()
+    L = _lib.lib()
+    dims = np.array([16, 16, 16], np.int32)
+    vol = torch.zeros(16 * 16 * 16, dtype=torch.uint8, device="cuda")
+    Ts = np.zeros((4, 12), np.float32)
+    Ts[:, [0, 4, 8]] = 1.0
+    out = torch.zeros(4, dtype=torch.float64, device="cuda")
+    side = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=side):
+        out.add_(1.0)
+        st = L.regb_mi_cost_noalloc(C.c_void_p(vol.data_ptr()), dims.ctypes.data_as(C.c_void_p),
+                                    C.c_void_p(vol.data_ptr()), dims.ctypes.data_as(C.c_void_p),
+                                    Ts.ctypes.data_as(C.c_void_p), 4, C.c_void_p(out.data_ptr()),
+                                    C.c_void_p(side.cuda_stream))
+    assert st == _lib.REGB_ERR_ARG
+    assert b"captured" in L.regb_last_error()
+    g.replay()
+    torch.cuda.synchronize()
+    assert float(out[0]) == 1.0

@@ -96,6 +96,12 @@ extern "C" regb_status regb_mi_cost_noalloc(const uint8_t* fixed, const int fixe
         if (K == 0)
             return REGB_OK;
         cudaStream_t st = (cudaStream_t)stream;
+        // the call ends with a stream synchronisation, which a capture cannot hold
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        REGB_CK(cudaStreamIsCapturing(st, &cap));
+        if (cap != cudaStreamCaptureStatusNone)
+            throw Failure(REGB_ERR_ARG, "regb_mi_cost_noalloc: the call is synchronous and cannot be made while "
+                                        "its stream is being captured");
         NoAllocScratch* s = scratch_on_current_device();
         // counters the kernels expect at zero; the array keeps whatever the last call left
         REGB_CK(cudaMemsetAsync(s->hist, 0, sizeof(uint32_t) * 65536 * K, st));
