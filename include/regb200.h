@@ -233,9 +233,10 @@ regb_status regb_mi32_cost(const regb_volume* fixed, const regb_volume* moving, 
  * is a DEVICE array of K doubles.  Nothing is allocated: all scratch lives in one
  * file-scope device array (4 MiB of joint histograms plus about 25 KiB), so K <= 16 and
  * larger K is rejected with REGB_ERR_ARG, as is a fixed width above 65535.  The first
- * call on a device looks up that array's device address; it is also the call on which
+ * call on a device looks up that array's device address and fills the MI reduction's
+ * n*ln(n) table (another static device array, 512 KiB); it is also the call on which
  * the CUDA runtime, which loads device code lazily, brings this library's kernels and
- * the array (about 4 MiB plus code) into device memory, so make it during
+ * both arrays (about 4.5 MiB, plus code) into device memory, so make it during
  * initialisation, where allocation is still allowed.  Every call shares the array:
  * calls that overlap on the GPU (different streams or host threads without ordering)
  * race and give wrong costs.  The call is synchronous: it synchronises the stream

@@ -12,6 +12,7 @@
 // The last block of a task (ticket counter) reduces that task's counts to its
 // cost and clears the task's scratch, so the next launch finds it zeroed.
 #include <atomic>
+#include <mutex>
 #include <cuda_fp16.h>
 #include "common.cuh"
 #include "stats.h"
@@ -105,8 +106,28 @@ __device__ __forceinline__ void mi_count(uint32_t* sh, uint32_t bin)
 // of the task adds the partial sums in block order, writes -sum/65536, and clears
 // the column sums and the ticket.  The order of every sum is fixed, so a task's cost
 // does not depend on what it is batched with.
+//
+// Each term is formed as n*ln(n) - n*(ln(row) + ln(col)): n*ln(n) from a table for
+// n < 65536 (g_nlogn, filled once per device), ln(row) and ln(col) once per block.
+// Against n*ln(n/row/col) with its two divisions and a logarithm per bin, that is a
+// few FP64 operations a bin (the reduction was FP64-throughput bound); each term
+// moves by rounding only, ~1e-16 of its size, against the ~1e-16 * sqrt(bins) the
+// block-parallel summation order already allows.
 constexpr int kMiReduceThreads = 256;
 constexpr int kMiReduceRows = 256 / kMiReduceBlocks;
+constexpr int kNlognTable = 65536;
+__device__ double g_nlogn[kNlognTable];  // n * ln(n); 0 for n = 0
+
+__global__ void nlogn_table_kernel()
+{
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < kNlognTable; n += gridDim.x * blockDim.x)
+        g_nlogn[n] = n ? (double)n * log((double)n) : 0.0;
+}
+
+__device__ __forceinline__ double nlogn(uint32_t n)
+{
+    return n < (uint32_t)kNlognTable ? g_nlogn[n] : (double)n * log((double)n);
+}
 
 __global__ void __launch_bounds__(kMiReduceThreads) mi_reduce_kernel(const AffineTask* __restrict__ tasks)
 {
@@ -123,14 +144,19 @@ __global__ void __launch_bounds__(kMiReduceThreads) mi_reduce_kernel(const Affin
     // every voxel is in one bin: the uncounted background bin is the remainder
     const unsigned long long tot = block_sum((unsigned long long)c, red64);
     __shared__ uint32_t n00_s;
+    __shared__ double lrow[kMiReduceRows];
     if (t == 0) {
         n00_s = (uint32_t)(tk.fd.n() - (long long)tot);
         col[0] += n00_s;
     }
+    if (t < kMiReduceRows) {
+        const int32_t rh = tk.row_hist[blockIdx.x * kMiReduceRows + t];
+        lrow[t] = rh > 0 ? log((double)rh) : 0.0;  // a row with no template voxels has no counts
+    }
     __syncthreads();
     const uint32_t n00 = n00_s;
     uint32_t* __restrict__ hist = tk.hist;
-    const double cd = (double)col[t];
+    const double lcol = col[t] ? log((double)col[t]) : 0.0;
     double acc = 0.0;
 #pragma unroll
     for (int k = 0; k < kMiReduceRows; ++k) {
@@ -138,8 +164,7 @@ __global__ void __launch_bounds__(kMiReduceThreads) mi_reduce_kernel(const Affin
         const int b = row * 256 + t;
         const uint32_t n = (b == 0) ? n00 : __ldcg(hist + b);
         if (n) {
-            const double mu = (double)n;
-            acc += mu * log(mu / (double)tk.row_hist[row] / cd);
+            acc += nlogn(n) - (double)n * (lrow[k] + lcol);
             hist[b] = 0u;
         }
     }
@@ -255,6 +280,29 @@ __global__ void __launch_bounds__(kMiThreads, 1) mi_kernel(const AffineTask* __r
         atomicAdd(tk.col + threadIdx.x, colp[threadIdx.x]);
 }
 
+// g_nlogn of the current device, filled before its first reduction launch on any stream
+// (the fill is synchronised before the device counts as ready, so a launch on another
+// stream never reads the table half written).
+static cudaError_t ensure_nlogn_table(int dev, cudaStream_t st)
+{
+    static std::atomic<unsigned long long> ready{0};  // one bit per device
+    static std::mutex m;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (ready.load() & bit)
+        return cudaSuccess;
+    std::lock_guard<std::mutex> g(m);
+    if (ready.load() & bit)
+        return cudaSuccess;
+    nlogn_table_kernel<<<64, 256, 0, st>>>();
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess)
+        ready.fetch_or(bit);
+    return e;
+}
+
 template <bool TEX>
 static cudaError_t launch_mi_impl(const AffineTask* d_tasks, int ntask, int max_chunks, cudaStream_t st)
 {
@@ -270,6 +318,9 @@ static cudaError_t launch_mi_impl(const AffineTask* d_tasks, int ntask, int max_
             return e;
         attr_set.fetch_or(bit);
     }
+    e = ensure_nlogn_table(dev, st);
+    if (e != cudaSuccess)
+        return e;
     dim3 grid(max_chunks, ntask);
     mi_kernel<TEX><<<grid, kMiThreads, kMiSmemWords * 4, st>>>(d_tasks);
     e = cudaGetLastError();
