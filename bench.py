@@ -705,7 +705,7 @@ def run_served(args, rank, world, dist):
     plain = {"mean_rate": len(plain_s) / sum(plain_s), "median_rate": 1.0 / float(np.median(plain_s)),
              "ms": sorted(round(1000.0 * t, 2) for t in plain_s)} if plain_s else None
     tuned = tb.autotune_buckets("")  # the cost kernels' block sizes per grid-size bucket (cached on disk)
-    eng = tb.Engine(max_active=max(args.batch, 1), gather_us=args.gather_us)
+    eng = tb.Engine(max_active=max(args.batch, 1), gather_us=args.gather_us, affine_workers=args.affine_workers)
     tid = eng.add_template(torch.from_numpy(f8).cuda())
     lat, costs, evals = [], [], 0
 
@@ -801,7 +801,8 @@ def batch_result(args, n_subjects, plain_jobs=4):
             plain(subjects[k], vss[k])
         torch.cuda.synchronize()
         plain_rate = plain_jobs / (time.perf_counter() - t0)
-    with tb.Engine(hbm_budget_bytes=150 << 30, max_active=n_subjects) as eng:
+    with tb.Engine(hbm_budget_bytes=150 << 30, max_active=n_subjects, gather_us=args.gather_us,
+                   affine_workers=args.affine_workers) as eng:
         tid = eng.add_template(t)
         for k in range(2):  # warm-up
             eng.wait(eng.submit(subjects[k], vss[k], template=tid, cdm=True, cdm_param=cdm_p))
@@ -886,7 +887,8 @@ def poisson_case(args):
             break
         arrivals.append((t, int(rng.integers(0, 4)), int(rng.integers(0, len(pool)))))
     with tb.Engine(hbm_budget_bytes=150 << 30, max_active=args.max_active,
-                   cdm_iters_per_round=args.cdm_iters_per_round) as eng:
+                   cdm_iters_per_round=args.cdm_iters_per_round, gather_us=args.gather_us,
+                   affine_workers=args.affine_workers) as eng:
         tids = [eng.add_template(tm) for tm in templates]
         for ti in range(4):  # warm-up: one job per template
             eng.wait(eng.submit(pool[ti], template=tids[ti], cdm=True, cdm_param=cdm_p))
@@ -996,6 +998,8 @@ def main():
     ap.add_argument("--cdm-iters-per-round", type=int, default=4,
                     help="--workload poisson: CDM iterations the engine launches between two reads of the levels' "
                          "done flags")
+    ap.add_argument("--affine-workers", type=int, default=2,
+                    help="served mode: affine cost launches the engine keeps in flight at once")
     ap.add_argument("--gather-us", type=int, default=30,
                     help="served mode: how long a cost batch waits for more jobs once the device is free")
     args = ap.parse_args()
@@ -1194,7 +1198,8 @@ def served_line(args, rank, world, dist, torch):
                            "cost_evals_per_registration": evals / max(1, len(costs)),
                            "latency_ms": {"p50": pct(0.50), "p95": pct(0.95), "p99": pct(0.99)},
                            "engine": {"affine_launches": estats["affine_launches"],
-                                      "affine_tasks": estats["affine_tasks"]},
+                                      "affine_tasks": estats["affine_tasks"],
+                                      "affine_workers": args.affine_workers, "gather_us": args.gather_us},
                            "plain_single_job_registrations_per_s": plain["mean_rate"] if plain else None,
                            "plain_single_job_median_registrations_per_s": plain["median_rate"] if plain else None,
                            "plain_single_job_ms": plain["ms"] if plain else None,

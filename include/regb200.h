@@ -427,6 +427,8 @@ typedef struct {
                                   more jobs to join; 0 = 30 us */
     int cdm_iters_per_round;   /* CDM iterations launched between two reads of the done
                                   flags; 0 = 4 */
+    int affine_workers;        /* affine cost launches in flight at once (each worker its own
+                                  stream and scratch), 1..4 (larger values are clamped); 0 = 2 */
 } regb_engine_config;
 
 /* One registration: affine (tipl::reg::linear) of moving to the template, then

@@ -574,7 +574,7 @@ class Engine:
     levels iterate together.  Host arrays passed to submit() are kept alive here
     until the job is released."""
 
-    def __init__(self, hbm_budget_bytes=0, max_active=64, gather_us=30, cdm_iters_per_round=4):
+    def __init__(self, hbm_budget_bytes=0, max_active=64, gather_us=30, cdm_iters_per_round=4, affine_workers=2):
         L = _lib.lib()
         cfg = _lib.EngineConfig()
         L.regb_engine_config_default(C.byref(cfg))
@@ -582,6 +582,7 @@ class Engine:
         cfg.max_active = int(max_active)
         cfg.gather_us = int(gather_us)
         cfg.cdm_iters_per_round = int(cdm_iters_per_round)
+        cfg.affine_workers = int(affine_workers)
         h = C.c_void_p()
         _lib.check(L.regb_engine_create(C.byref(cfg), C.byref(h)))
         self._h = h

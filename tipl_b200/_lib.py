@@ -59,7 +59,7 @@ class RunnerState(C.Structure):
 
 class EngineConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_active", C.c_int), ("gather_us", C.c_int),
-                ("cdm_iters_per_round", C.c_int)]
+                ("cdm_iters_per_round", C.c_int), ("affine_workers", C.c_int)]
 
 
 class NiftiInfo(C.Structure):

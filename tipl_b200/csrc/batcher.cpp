@@ -1,20 +1,24 @@
 #include "batcher.h"
 #include <chrono>
+#include <algorithm>
 #include <cstring>
 
 namespace regb {
 
-AffineBatcher::AffineBatcher(int gather_us) : gather_us_(gather_us)
+AffineBatcher::AffineBatcher(int gather_us, int workers)
+    : nworkers_(std::min(std::max(workers, 1), kMaxWorkers)), gather_us_(gather_us)
 {
     int dev = 0;
     REGB_CK(cudaGetDevice(&dev));
-    for (Worker& w : workers_)
-        REGB_CK(cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking));
-    for (Worker& w : workers_)
+    for (int i = 0; i < nworkers_; ++i)
+        REGB_CK(cudaStreamCreateWithFlags(&workers_[i].st, cudaStreamNonBlocking));
+    for (int i = 0; i < nworkers_; ++i) {
+        Worker& w = workers_[i];
         w.th = std::thread([this, dev, &w] {
             cudaSetDevice(dev);
             loop(w);
         });
+    }
 }
 
 AffineBatcher::~AffineBatcher()

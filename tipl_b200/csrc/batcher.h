@@ -20,7 +20,8 @@ constexpr int kCostTypes = 3;  // REGB_COST_CORR, REGB_COST_MI, REGB_COST_MI32
 // whatever it is batched with.
 class AffineBatcher {
 public:
-    explicit AffineBatcher(int gather_us);
+    // workers: concurrent launches (1..kMaxWorkers)
+    AffineBatcher(int gather_us, int workers);
     ~AffineBatcher();
     AffineBatcher(const AffineBatcher&) = delete;
     AffineBatcher& operator=(const AffineBatcher&) = delete;
@@ -44,10 +45,11 @@ private:
         bool done = false;
         std::exception_ptr err;
     };
-    // Two workers, each with its own stream and scratch: while one batch runs on the
-    // device, the jobs it does not hold can form the next batch, which the other worker
-    // launches at once instead of after the first batch's results are back.
-    static constexpr int kWorkers = 2;
+    // Workers, each with its own stream and scratch: while one batch runs on the device,
+    // the jobs it does not hold can form the next batch, which another worker launches at
+    // once instead of after the first batch's results are back.
+    static constexpr int kMaxWorkers = 4;
+    int nworkers_;
     struct Worker {
         TaskScratch scratch[kCostTypes];  // one per cost type (REGB_COST_CORR, _MI, _MI32)
         cudaStream_t st = nullptr;
@@ -62,7 +64,7 @@ private:
     bool stop_ = false;
     int gather_us_;
     std::atomic<long long> launches_{0}, tasks_{0};
-    Worker workers_[kWorkers];
+    Worker workers_[kMaxWorkers];
 };
 
 }  // namespace regb

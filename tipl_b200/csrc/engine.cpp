@@ -80,7 +80,7 @@ struct EngineJob {
 class Engine {
 public:
     explicit Engine(const regb_engine_config& c)
-        : cfg_(c), batcher_(c.gather_us > 0 ? c.gather_us : 30), sched_(c.cdm_iters_per_round > 0 ? c.cdm_iters_per_round : 4)
+        : cfg_(c), batcher_(c.gather_us > 0 ? c.gather_us : 30, c.affine_workers > 0 ? c.affine_workers : 2), sched_(c.cdm_iters_per_round > 0 ? c.cdm_iters_per_round : 4)
     {
         REGB_CK(cudaGetDevice(&dev_));
         if (cfg_.max_active <= 0)
@@ -583,6 +583,7 @@ void regb_engine_config_default(regb_engine_config* c)
     c->max_active = 64;
     c->gather_us = 30;
     c->cdm_iters_per_round = 4;
+    c->affine_workers = 2;
 }
 
 void regb_job_default(regb_job* j)
