@@ -998,9 +998,9 @@ def main():
     ap.add_argument("--cdm-iters-per-round", type=int, default=4,
                     help="--workload poisson: CDM iterations the engine launches between two reads of the levels' "
                          "done flags")
-    ap.add_argument("--affine-workers", type=int, default=2,
+    ap.add_argument("--affine-workers", type=int, default=3,
                     help="served mode: affine cost launches the engine keeps in flight at once")
-    ap.add_argument("--gather-us", type=int, default=30,
+    ap.add_argument("--gather-us", type=int, default=10,
                     help="served mode: how long a cost batch waits for more jobs once the device is free")
     args = ap.parse_args()
     # the affine cost: MI (the reference's linear() default) for the affine workloads,
@@ -1145,7 +1145,7 @@ def served_line(args, rank, world, dist, torch):
     t_e2e = replicas.max_over_ranks(t_e2e, dist)
     regs = args.steps * args.batch * world
     hbm, hbm_kind = peaks()
-    # the engine keeps up to two MI launches in flight on two streams, so the kernel's
+    # the engine keeps several MI launches in flight on as many streams, so the kernel's
     # rate is its algorithmic bytes over the union of its launches' device intervals
     # (the correlation kernel's launches have no union record: their summed times)
     if args.cost == "corr":

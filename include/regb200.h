@@ -424,11 +424,11 @@ typedef struct {
     size_t hbm_budget_bytes;   /* admission budget for running jobs; 0 = 80% of free memory */
     int max_active;            /* concurrent jobs; 0 = 64 */
     int gather_us;             /* once the device is free, how long a cost batch waits for
-                                  more jobs to join; 0 = 30 us */
+                                  more jobs to join; 0 = 10 us */
     int cdm_iters_per_round;   /* CDM iterations launched between two reads of the done
                                   flags; 0 = 4 */
     int affine_workers;        /* affine cost launches in flight at once (each worker its own
-                                  stream and scratch), 1..4 (larger values are clamped); 0 = 2 */
+                                  stream and scratch), 1..4 (larger values are clamped); 0 = 3 */
 } regb_engine_config;
 
 /* One registration: affine (tipl::reg::linear) of moving to the template, then

@@ -574,7 +574,7 @@ class Engine:
     levels iterate together.  Host arrays passed to submit() are kept alive here
     until the job is released."""
 
-    def __init__(self, hbm_budget_bytes=0, max_active=64, gather_us=30, cdm_iters_per_round=4, affine_workers=2):
+    def __init__(self, hbm_budget_bytes=0, max_active=64, gather_us=10, cdm_iters_per_round=4, affine_workers=3):
         L = _lib.lib()
         cfg = _lib.EngineConfig()
         L.regb_engine_config_default(C.byref(cfg))

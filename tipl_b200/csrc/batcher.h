@@ -14,7 +14,8 @@ namespace regb {
 constexpr int kCostTypes = 3;  // REGB_COST_CORR, REGB_COST_MI, REGB_COST_MI32
 
 // Collects cost-evaluation requests from many jobs and evaluates all pending ones
-// of a cost type in one launch (two launches may be in flight, on two streams).
+// of a cost type in one launch (one launch per worker may be in flight, each worker
+// on its own stream).
 // A request's tasks carry their own volumes, so requests of different jobs, shapes
 // and pyramid levels mix freely; every task's cost depends only on its own inputs,
 // whatever it is batched with.

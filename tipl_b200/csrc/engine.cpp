@@ -80,7 +80,7 @@ struct EngineJob {
 class Engine {
 public:
     explicit Engine(const regb_engine_config& c)
-        : cfg_(c), batcher_(c.gather_us > 0 ? c.gather_us : 30, c.affine_workers > 0 ? c.affine_workers : 2), sched_(c.cdm_iters_per_round > 0 ? c.cdm_iters_per_round : 4)
+        : cfg_(c), batcher_(c.gather_us > 0 ? c.gather_us : 10, c.affine_workers > 0 ? c.affine_workers : 3), sched_(c.cdm_iters_per_round > 0 ? c.cdm_iters_per_round : 4)
     {
         REGB_CK(cudaGetDevice(&dev_));
         if (cfg_.max_active <= 0)
@@ -581,9 +581,9 @@ void regb_engine_config_default(regb_engine_config* c)
         return;
     c->hbm_budget_bytes = 0;
     c->max_active = 64;
-    c->gather_us = 30;
+    c->gather_us = 10;
     c->cdm_iters_per_round = 4;
-    c->affine_workers = 2;
+    c->affine_workers = 3;
 }
 
 void regb_job_default(regb_job* j)
