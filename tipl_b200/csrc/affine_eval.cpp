@@ -270,9 +270,9 @@ double autotune_cost_kernels(cudaStream_t st, int* chosen, const char* cache_pat
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     }
     // one smooth, many-valued pair per bucket, of the bucket's representative grid, and
-    // kTuneTasks small rigid candidates: a launch of the serving engine's size (its
-    // launches gather about 90 to 160 candidates; smaller launches get their chunks
-    // split to fill one wave)
+    // kTuneTasks small rigid candidates: a launch of the order of the serving engine's
+    // (its launches gather about 50 to 160 candidates; smaller launches outside the
+    // engine get their chunks split to fill one wave)
     static const Dim3 kRep[kTuneBuckets] = {{64, 64, 64}, {128, 128, 128}, {182, 218, 182}, {256, 256, 256}};
     cudaEvent_t a, b;
     REGB_CK(cudaEventCreate(&a));
