@@ -84,6 +84,22 @@ def test_param_defaults(L):
     assert abs(q.speed - 0.3) < 1e-7 and abs(q.smoothing - 0.05) < 1e-7
 
 
+def test_engine_config_defaults_match_python(L):
+    """regb_engine_config_default (host only) and the Python Engine's keyword defaults agree:
+    slots, gather window, affine workers and CDM iterations per round."""
+    import inspect
+
+    import tipl_b200 as tb
+
+    c = _lib.EngineConfig()
+    L.regb_engine_config_default(C.byref(c))
+    assert (c.hbm_budget_bytes, c.max_active, c.gather_us, c.cdm_iters_per_round, c.affine_workers) == \
+        (0, 64, 10, 4, 3)
+    sig = inspect.signature(tb.Engine.__init__).parameters
+    assert (sig["max_active"].default, sig["gather_us"].default, sig["cdm_iters_per_round"].default,
+            sig["affine_workers"].default) == (c.max_active, c.gather_us, c.cdm_iters_per_round, c.affine_workers)
+
+
 def test_runner_state_from_param(L):
     """The runner state of tipl::reg::linear for an affine MI registration: the four DOF
     stages, bounds around the identity from reg_bound (reg/linear.hpp:258-263, 370-420)."""
