@@ -494,6 +494,7 @@ typedef struct {
     double cdm_round_ms;           /* device time of the CDM rounds, summed (CUDA events on
                                       the scheduler's stream, from the segment upload to the
                                       status read-back) */
+    int cdm_max_round_segments;    /* the most CDM levels one round has carried */
 } regb_engine_stats;
 
 void regb_engine_config_default(regb_engine_config* c);

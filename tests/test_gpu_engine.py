@@ -313,3 +313,37 @@ def test_failed_allocation_fails_only_its_job(data):
             else:
                 r = eng.wait(eng.submit(j["mov"], template=tid, cdm=True, field_out=f))
             assert r["status"] == 0 and np.array_equal(f.view(np.uint32), ref[target][3].view(np.uint32))
+
+
+def test_many_levels_in_one_round_equal_plain():
+    """More CDM levels in one scheduler round than a warp's ballot covers (each block of a
+    launch over many levels finds its level 32 entries at a time), in two launch groups
+    (float and uint8 pixels): every job's field equals the plain single-job CDM call
+    bit for bit."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    p = tb.reg.cdm_param(resolution=1.0, min_dimension=8)
+    cases = []
+    for k in range(46):
+        s = (24 + k % 9, 26 + (3 * k) % 7, 22 + (5 * k) % 8)
+        t, m = ph.cdm_class_pair(s, seed=ph.seed_for(5, 300 + k))
+        if k >= 40:
+            t, m = ph.normalize_to_u8(t), ph.normalize_to_u8(m)
+        cases.append((t, m))
+    outs = [np.zeros(t.shape + (3,), np.float32) for t, _ in cases]
+    with tb.Engine(max_active=64) as eng:
+        ids = [eng.submit(m, fixed=t, linear=False, cdm=True, cdm_param=p, field_out=o)
+               for (t, m), o in zip(cases, outs)]
+        res = [eng.wait(i) for i in ids]
+        st = eng.stats()
+    assert st["cdm_max_round_segments"] > 32, st
+    moving = 0
+    for (t, m), o, r in zip(cases, outs, res):
+        assert r["status"] == 0
+        f, ok = tb.reg.cdm(t, m, param=p)
+        assert bool(r["cdm_ok"]) == bool(ok)
+        assert np.array_equal(np.asarray(f, np.float32).view(np.uint32), o.view(np.uint32))
+        moving += int(float(np.abs(o).max()) > 0.1)
+    assert moving >= 10

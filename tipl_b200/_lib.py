@@ -89,7 +89,7 @@ class EngineStats(C.Structure):
     _fields_ = [("queued", C.c_int), ("running", C.c_int), ("used_bytes", C.c_size_t),
                 ("budget_bytes", C.c_size_t), ("affine_launches", C.c_longlong), ("affine_tasks", C.c_longlong),
                 ("cdm_rounds", C.c_longlong), ("cdm_round_segments", C.c_longlong),
-                ("cdm_round_ms", C.c_double)]
+                ("cdm_round_ms", C.c_double), ("cdm_max_round_segments", C.c_int)]
 
 
 class RegbError(RuntimeError):

@@ -203,6 +203,7 @@ public:
         s.cdm_rounds = sched_.rounds();
         s.cdm_round_segments = sched_.round_segments();
         s.cdm_round_ms = sched_.round_ms();
+        s.cdm_max_round_segments = sched_.max_round_segments();
         return s;
     }
 

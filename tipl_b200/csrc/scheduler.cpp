@@ -116,6 +116,7 @@ void CdmScheduler::loop()
             round_ms_ += ms;
             ++rounds_;
             round_segments_ += n;
+            max_round_segments_ = std::max(max_round_segments_, n);
             for (int i = 0; i < n; ++i) {
                 Entry* e = cur[order[i]];
                 if (h_status_.p[i] || (e->term && *e->term)) {

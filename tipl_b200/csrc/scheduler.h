@@ -38,6 +38,11 @@ public:
         std::lock_guard<std::mutex> g(m_);
         return round_ms_;
     }
+    int max_round_segments()  // the most levels one round has carried
+    {
+        std::lock_guard<std::mutex> g(m_);
+        return max_round_segments_;
+    }
 
 private:
     struct Entry {
@@ -54,6 +59,7 @@ private:
     long long rounds_ = 0;
     long long round_segments_ = 0;
     double round_ms_ = 0.0;
+    int max_round_segments_ = 0;
     cudaStream_t st_ = nullptr;
     cudaEvent_t ev_[2] = {nullptr, nullptr};
     DevBuf<CdmSeg> segs_;
