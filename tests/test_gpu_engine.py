@@ -43,11 +43,13 @@ def alone(tmpl, mov, with_cdm):
     return cost, arg, evals, field
 
 
-@pytest.mark.parametrize("with_cdm", [False, True])
-def test_alone_vs_in_the_mix(data, with_cdm):
+@pytest.mark.parametrize("with_cdm,workers", [(False, 3), (True, 3), (False, 1), (False, 4)])
+def test_alone_vs_in_the_mix(data, with_cdm, workers):
+    """workers: the engine's affine cost launches in flight (affine_workers); how the
+    jobs' probe sets are gathered into launches must not change any result."""
     tmpl, movs = data
     ref = [alone(tmpl, m, with_cdm) for m in movs]
-    with tb.Engine(max_active=8) as eng:
+    with tb.Engine(max_active=8, affine_workers=workers) as eng:
         tid = eng.add_template(tmpl)
         fields = [np.zeros(tmpl.shape + (3,), np.float32) for _ in movs]
         ids = [eng.submit(m, template=tid, cdm=with_cdm, field_out=f if with_cdm else None)
