@@ -147,3 +147,35 @@ def test_mi_rejects_rows_wider_than_16_bit_counters(L):
                                 buf.ctypes.data_as(C.c_void_p), md.ctypes.data_as(C.c_void_p),
                                 T.ctypes.data_as(C.c_void_p), 1, cost.ctypes.data_as(C.c_void_p), None)
     assert st == _lib.REGB_ERR_ARG and b"65535" in L.regb_last_error()
+
+
+# The ctypes mirrors of the header's structs: every field at the header's offset and
+# every struct of the header's size, so a field added on one side only cannot go unnoticed.
+MIRRORED = {"Volume": "regb_volume", "Field": "regb_field", "LinearParam": "regb_linear_param",
+            "CdmParam": "regb_cdm_param", "Stats": "regb_stats", "RunnerState": "regb_runner_state",
+            "EngineConfig": "regb_engine_config", "NiftiInfo": "regb_nifti_info", "Job": "regb_job",
+            "Result": "regb_result", "EngineStats": "regb_engine_stats"}
+
+
+def test_ctypes_structs_match_header(tmp_path):
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "regb200.h"', "int main(void) {"]
+    expect = []
+    for py, c in MIRRORED.items():
+        cls = getattr(_lib, py)
+        lines.append(f'printf("%zu\\n", sizeof({c}));')
+        expect.append(C.sizeof(cls))
+        for name, _ in cls._fields_:
+            lines.append(f'printf("%zu\\n", offsetof({c}, {name}));')
+            expect.append(getattr(cls, name).offset)
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    got = [int(v) for v in subprocess.check_output([str(exe)]).split()]
+    assert got == expect
