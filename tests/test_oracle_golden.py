@@ -197,3 +197,42 @@ def test_oracle_cdm2d_matches_reference(orc, golden):
         assert int(ok) == int(g[f"c{k}_ok"]), k
         if ok:
             assert hashlib.sha256(d.tobytes()).hexdigest() == str(g[f"c{k}_sha256"]), k
+
+
+def mi_from_terms(hist, from_hist):
+    """The MI reduction's arithmetic (affine_kernels.cu, mi_reduce_kernel): each non-zero
+    bin adds n*ln(n) - n*(ln(row) + ln(col)) in double, a block of 8 rows x 256 columns per
+    partial sum, the 32 partials added in block order; the cost is -sum / 65536."""
+    h = np.asarray(hist, np.int64).reshape(256, 256)
+    col = h.sum(axis=0).astype(np.float64)
+    row = np.asarray(from_hist, np.float64)
+    lcol = np.where(col > 0, np.log(np.where(col > 0, col, 1.0)), 0.0)
+    lrow = np.where(row > 0, np.log(np.where(row > 0, row, 1.0)), 0.0)
+    n = h.astype(np.float64)
+    nz = h > 0
+    terms = np.where(nz, n * np.log(np.where(nz, n, 1.0)) - n * (lrow[:, None] + lcol[None, :]), 0.0)
+    parts = [float(np.sum(terms[8 * b:8 * b + 8])) for b in range(32)]
+    s = 0.0
+    for p in parts:
+        s += p
+    return -(s / 65536.0)
+
+
+def test_mi_term_form_within_tolerance(orc, golden):
+    """The reduction forms each term as n ln n - n (ln row + ln col) instead of the
+    reference's n ln(n / row / col): only rounding differs, and the cost stays within the
+    1e-12 relative tolerance of the reference's own costs (fixtures) and of the oracle on a
+    full-size 182x218x182 histogram."""
+    from tipl_b200 import phantom as ph
+
+    g = golden("affine_costs")
+    for h, mi in zip(g["hist"], g["mi"]):
+        assert mi_from_terms(h, g["from_hist"]) == pytest.approx(mi, rel=1e-12)
+    rng = np.random.default_rng(ph.seed_for(2, 0))
+    shape = (182, 218, 182)
+    t, m, _ = ph.affine_pair(shape, rng=rng)
+    f8, m8 = ph.normalize_to_u8(t), ph.normalize_to_u8(m)
+    T = np.array([1, 0.02, 0, -0.02, 1, 0, 0, 0, 1, 1.5, -2.0, 0.7], np.float32)
+    h = orc.mi_hist(f8, m8, T)
+    fh = orc.histogram(f8)
+    assert mi_from_terms(h, fh) == pytest.approx(orc.mi_cost_from_hist(h, fh), rel=1e-12)
